@@ -1,0 +1,751 @@
+// frw_api.cpp -- the extern "C" boundary (include/frw.h) over the CUDA kernels.
+//
+// Host responsibilities only: argument checking, the reference's layout
+// reader and bounds rule, device buffers and streams, and turning the
+// device accumulators into the estimator's rows.  Every compute step runs on
+// the device; there is no CPU path to fall back to.
+#include <math.h>
+#include <stdio.h>
+
+#include <cmath>
+#include <string.h>
+#include <time.h>
+
+#include <algorithm>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "frw_internal.h"
+#include "layout_io.h"
+
+struct frw_layout {
+    int device = 0;
+    int64_t n = 0;
+    std::vector<double> rects;  // layer order, as given
+    double bounds[4] = {0, 0, 0, 0};
+    frw::TreeBuffers T;
+    frw::DevLayout dl{};
+    float build_ms = 0.f;
+    int leaf_max = frw::kDefaultLeafMax;
+};
+
+namespace frw {
+namespace {
+
+thread_local std::string g_err;
+
+struct DeviceCtx {
+    bool ready = false;
+    int sms = 0;
+    int cc_major = 0, cc_minor = 0;
+    double *tables = nullptr;  // intg[201] | wx[200] | wy[200]
+};
+std::mutex g_mu;
+std::map<int, DeviceCtx> g_ctx;
+
+// Keeps the caller's current device.
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+frw_status device_ctx(int dev, DeviceCtx **out) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    DeviceCtx &c = g_ctx[dev];
+    if (!c.ready) {
+        int ndev = 0;
+        cudaError_t e = cudaGetDeviceCount(&ndev);
+        if (e != cudaSuccess || ndev <= dev || dev < 0) {
+            set_error("no CUDA device " + std::to_string(dev) +
+                      (e != cudaSuccess ? std::string(": ") + cudaGetErrorString(e) : std::string()));
+            return FRW_E_DEVICE;
+        }
+        cudaDeviceProp p;
+        FRW_CK(cudaGetDeviceProperties(&p, dev));
+        if (p.major != 10) {
+            set_error("device " + std::to_string(dev) + " is sm_" + std::to_string(p.major) +
+                      std::to_string(p.minor) + "; this library is built for sm_100a only");
+            return FRW_E_DEVICE;
+        }
+        c.sms = p.multiProcessorCount;
+        c.cc_major = p.major;
+        c.cc_minor = p.minor;
+        DeviceGuard g(dev);
+        double h[FRW_NSAMPLE + 1 + 2 * FRW_NSAMPLE];
+        green_tables(nullptr, h, h + FRW_NSAMPLE + 1, h + 2 * FRW_NSAMPLE + 1);
+        FRW_CK(cudaMalloc(&c.tables, sizeof(h)));
+        FRW_CK(cudaMemcpy(c.tables, h, sizeof(h), cudaMemcpyHostToDevice));
+        // keep stream-ordered allocations pooled between calls
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            uint64_t thr = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        }
+        c.ready = true;
+    }
+    *out = &c;
+    return FRW_OK;
+}
+
+// Reads the kernel status word (after the stream has drained).
+frw_status check_status(const uint32_t *d_status, cudaStream_t st) {
+    uint32_t h = 0;
+    FRW_CK(cudaMemcpyAsync(&h, d_status, 4, cudaMemcpyDeviceToHost, st));
+    FRW_CK(cudaStreamSynchronize(st));
+    if (h) {
+        std::string m = "kernel reported:";
+        if (h & kStCandOverflow) m += " near-tie candidate list overflow;";
+        if (h & kStStackOverflow) m += " traversal stack overflow;";
+        if (h & kStReplayCap) m += " bisection replay iteration bound exceeded;";
+        if (h & kStBadInput) m += " invalid input;";
+        set_error(m);
+        return FRW_E_KERNEL;
+    }
+    return FRW_OK;
+}
+
+bool fp32_exact(double v) { return (double)(float)v == v && fabs(v) < 16777216.0; }
+
+frw_status validate_opts(const frw_opts *o) {
+    if (!o) return FRW_OK;
+    if (o->struct_size != sizeof(frw_opts)) {
+        set_error("frw_opts.struct_size mismatch (call frw_opts_default)");
+        return FRW_E_ARG;
+    }
+    if (o->gauss_mode != FRW_GAUSS_SCALE && o->gauss_mode != FRW_GAUSS_OFFSET) {
+        set_error("frw_opts.gauss_mode");
+        return FRW_E_ARG;
+    }
+    if (o->start_mode != FRW_START_GREEN && o->start_mode != FRW_START_UNIFORM) {
+        set_error("frw_opts.start_mode");
+        return FRW_E_ARG;
+    }
+    if (!(o->gauss_param >= 0) || o->hop_cap < 1) {
+        set_error("frw_opts.gauss_param / hop_cap");
+        return FRW_E_ARG;
+    }
+    return FRW_OK;
+}
+
+// Device scratch owned by one call, released on the stream at scope exit.
+struct Scratch {
+    cudaStream_t st;
+    std::vector<void *> ptrs;
+    explicit Scratch(cudaStream_t s) : st(s) {}
+    template <typename T>
+    cudaError_t get(T **p, size_t bytes) {
+        cudaError_t e = cudaMallocAsync((void **)p, bytes ? bytes : 16, st);
+        if (e == cudaSuccess) ptrs.push_back(*p);
+        return e;
+    }
+    ~Scratch() {
+        for (void *p : ptrs) cudaFreeAsync(p, st);
+    }
+};
+
+struct WalkRun {
+    // outputs
+    uint64_t escaped = 0, aborted = 0, hops = 0, done = 0;
+    double gauss[4] = {0, 0, 0, 0};
+    float kernel_ms = 0.f;
+    std::vector<int64_t> row;
+    std::vector<unsigned long long> n;
+    std::vector<double> s, s2;
+};
+
+// One job on one layout; records optional; host results optional.
+frw_status run_walks(const frw_layout *lay, int64_t target, uint64_t first_walk, uint64_t walks,
+                     uint64_t seed, const frw_opts &o, cudaStream_t st, int64_t *rec_end, int32_t *rec_hops,
+                     int32_t *rec_bin, double *rec_w, WalkRun *out) {
+    DeviceCtx *ctx;
+    frw_status rc = device_ctx(lay->device, &ctx);
+    if (rc) return rc;
+    if (target < 0 || target >= lay->n) {
+        set_error("target conductor index out of range");
+        return FRW_E_ARG;
+    }
+    Scratch S(st);
+    double4 *d_tgt, *d_gauss;
+    uint32_t *d_status;
+    unsigned long long *d_counter, *d_stats, *d_acc_n;
+    double *d_acc_s, *d_acc_s2;
+    const int64_t rows = lay->n;  // the kernel flushes every conductor it reaches
+    FRW_CK(S.get(&d_tgt, sizeof(double4)));
+    FRW_CK(S.get(&d_gauss, sizeof(double4)));
+    FRW_CK(S.get(&d_status, 4));
+    FRW_CK(S.get(&d_counter, 8));
+    FRW_CK(S.get(&d_stats, 4 * 8));
+    FRW_CK(S.get(&d_acc_n, (size_t)std::max<int64_t>(rows, 1) * 8));
+    FRW_CK(S.get(&d_acc_s, (size_t)std::max<int64_t>(rows, 1) * 8));
+    FRW_CK(S.get(&d_acc_s2, (size_t)std::max<int64_t>(rows, 1) * 8));
+    const double *r = lay->rects.data() + 4 * target;
+    const double tg[4] = {r[0], r[1], r[2], r[3]};
+    FRW_CK(cudaMemcpyAsync(d_tgt, tg, sizeof(tg), cudaMemcpyHostToDevice, st));
+    FRW_CK(cudaMemsetAsync(d_status, 0, 4, st));
+    FRW_CK(cudaMemsetAsync(d_counter, 0, 8, st));
+    FRW_CK(cudaMemsetAsync(d_stats, 0, 32, st));
+    if (rows) {
+        FRW_CK(cudaMemsetAsync(d_acc_n, 0, rows * 8, st));
+        FRW_CK(cudaMemsetAsync(d_acc_s, 0, rows * 8, st));
+        FRW_CK(cudaMemsetAsync(d_acc_s2, 0, rows * 8, st));
+    }
+    rc = launch_gauss(lay->dl, (const double *)d_tgt, 1, o.gauss_mode, o.gauss_param, (double *)d_gauss,
+                      d_status, st);
+    if (rc) return rc;
+
+    WalkParams P{};
+    P.job0.L = lay->dl;
+    P.job0.target = target;
+    P.job0.walk_begin = 0;
+    P.job0.walks = walks;
+    P.job0.first_walk = first_walk;
+    P.job0.acc_base = 0;
+    P.job0.stream_id = o.stream_id;
+    P.jobs = nullptr;
+    P.gauss = d_gauss;
+    P.njobs = 1;
+    P.start_mode = o.start_mode;
+    P.exact_perimeter = o.exact_perimeter;
+    P.refill_min = o.refill_min > 0 ? o.refill_min : 1;
+    P.hop_cap = o.hop_cap;
+    P.permittivity = o.permittivity;
+    P.seed = seed;
+    P.total_walks = walks;
+    P.counter = d_counter;
+    P.acc_n = d_acc_n;
+    P.acc_s = d_acc_s;
+    P.acc_s2 = d_acc_s2;
+    P.job_stats = d_stats;
+    P.status = d_status;
+    P.rec_end = rec_end;
+    P.rec_hops = rec_hops;
+    P.rec_bin = rec_bin;
+    P.rec_w = rec_w;
+    P.intg = ctx->tables;
+    P.wx = ctx->tables + FRW_NSAMPLE + 1;
+    P.wy = ctx->tables + 2 * FRW_NSAMPLE + 1;
+    const int threads = 256;
+    int bps = o.blocks_per_sm > 0 ? o.blocks_per_sm : walk_max_blocks_per_sm(threads, false);
+    if (bps < 1) bps = 1;
+    int blocks = ctx->sms * bps;
+    const uint64_t need = (walks + threads - 1) / threads;
+    if ((uint64_t)blocks > need) blocks = (int)std::max<uint64_t>(need, 1);
+
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (out) {
+        FRW_CK(cudaEventCreate(&e0));
+        FRW_CK(cudaEventCreate(&e1));
+        FRW_CK(cudaEventRecord(e0, st));
+    }
+    if (walks > 0) {
+        rc = launch_walk(P, threads, blocks, st);
+        if (rc) return rc;
+    }
+    if (!out) {
+        // stream-ordered call: report kernel limits only when the caller syncs;
+        // the status word is checked here synchronously to keep errors loud.
+        return check_status(d_status, st);
+    }
+    FRW_CK(cudaEventRecord(e1, st));
+    // compact nonzero rows
+    int64_t *d_row;
+    unsigned long long *d_cn, *d_cnt;
+    double *d_cs, *d_cs2;
+    FRW_CK(S.get(&d_row, (size_t)std::max<int64_t>(rows, 1) * 8));
+    FRW_CK(S.get(&d_cn, (size_t)std::max<int64_t>(rows, 1) * 8));
+    FRW_CK(S.get(&d_cs, (size_t)std::max<int64_t>(rows, 1) * 8));
+    FRW_CK(S.get(&d_cs2, (size_t)std::max<int64_t>(rows, 1) * 8));
+    FRW_CK(S.get(&d_cnt, 8));
+    FRW_CK(cudaMemsetAsync(d_cnt, 0, 8, st));
+    rc = launch_compact(d_acc_n, d_acc_s, d_acc_s2, rows, d_row, d_cn, d_cs, d_cs2, d_cnt, st);
+    if (rc) return rc;
+    unsigned long long h_cnt = 0, h_stats[4];
+    FRW_CK(cudaMemcpyAsync(&h_cnt, d_cnt, 8, cudaMemcpyDeviceToHost, st));
+    FRW_CK(cudaMemcpyAsync(h_stats, d_stats, 32, cudaMemcpyDeviceToHost, st));
+    FRW_CK(cudaMemcpyAsync(out->gauss, d_gauss, 32, cudaMemcpyDeviceToHost, st));
+    rc = check_status(d_status, st);
+    if (rc) return rc;
+    out->row.resize(h_cnt);
+    out->n.resize(h_cnt);
+    out->s.resize(h_cnt);
+    out->s2.resize(h_cnt);
+    if (h_cnt) {
+        FRW_CK(cudaMemcpyAsync(out->row.data(), d_row, h_cnt * 8, cudaMemcpyDeviceToHost, st));
+        FRW_CK(cudaMemcpyAsync(out->n.data(), d_cn, h_cnt * 8, cudaMemcpyDeviceToHost, st));
+        FRW_CK(cudaMemcpyAsync(out->s.data(), d_cs, h_cnt * 8, cudaMemcpyDeviceToHost, st));
+        FRW_CK(cudaMemcpyAsync(out->s2.data(), d_cs2, h_cnt * 8, cudaMemcpyDeviceToHost, st));
+        FRW_CK(cudaStreamSynchronize(st));
+    }
+    out->escaped = h_stats[0];
+    out->aborted = h_stats[1];
+    out->hops = h_stats[2];
+    out->done = h_stats[3];
+    cudaEventElapsedTime(&out->kernel_ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (out->done != walks) {
+        set_error("walk kernel finished " + std::to_string(out->done) + " of " + std::to_string(walks) +
+                  " walks");
+        return FRW_E_KERNEL;
+    }
+    return FRW_OK;
+}
+
+}  // namespace
+
+void set_error(const std::string &msg) { g_err = msg; }
+
+frw_status cuda_fail(cudaError_t e, const char *what) {
+    g_err = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    if (e == cudaErrorMemoryAllocation) return FRW_E_OOM;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver || e == cudaErrorInvalidDevice)
+        return FRW_E_DEVICE;
+    return FRW_E_CUDA;
+}
+
+}  // namespace frw
+
+using namespace frw;
+
+extern "C" {
+
+const char *frw_version(void) { return "frw-b200 0.1 (sm_100a)"; }
+
+const char *frw_last_error(void) { return g_err.c_str(); }
+
+frw_status frw_device_check(int device) {
+    DeviceCtx *c;
+    return device_ctx(device, &c);
+}
+
+frw_status frw_green_table(double *g, double *intg) {
+    green_tables(g, intg, nullptr, nullptr);
+    return FRW_OK;
+}
+
+void frw_opts_default(frw_opts *o) {
+    memset(o, 0, sizeof(*o));
+    o->struct_size = sizeof(frw_opts);
+    o->gauss_mode = FRW_GAUSS_SCALE;
+    o->gauss_param = 1.5;
+    o->start_mode = FRW_START_GREEN;
+    o->exact_perimeter = 0;
+    o->hop_cap = 100000;
+    o->permittivity = 8.854187817620e-12;
+    o->stream_id = 0;
+    o->threads_per_block = 256;
+    o->blocks_per_sm = 0;
+    o->refill_min = 1;
+}
+
+frw_status frw_layout_create(const float *rects, int64_t n, const double *bounds, int device, void *stream,
+                             frw_layout **out) {
+    if (!out || !rects || n <= 0) {
+        set_error("frw_layout_create: null pointer or empty layout");
+        return FRW_E_ARG;
+    }
+    *out = nullptr;
+    if (n >= (1ll << 26)) {
+        set_error("frw_layout_create: at most 2^26-1 rects per layout");
+        return FRW_E_ARG;
+    }
+    DeviceCtx *ctx;
+    frw_status rc = device_ctx(device, &ctx);
+    if (rc) return rc;
+    std::vector<double> h((size_t)n * 4);
+    for (int64_t i = 0; i < n; i++) {
+        const float *q = rects + 4 * i;
+        for (int k = 0; k < 4; k++) {
+            if (!std::isfinite(q[k]) || fabsf(q[k]) >= 16777216.0f) {
+                set_error("rect " + std::to_string(i) + ": coordinate not finite or |c| >= 2^24");
+                return FRW_E_ARG;
+            }
+            h[4 * i + k] = q[k];
+        }
+        if (!(q[0] <= q[2] && q[1] <= q[3])) {
+            set_error("rect " + std::to_string(i) + ": inverted (need x0 <= x1 and y0 <= y1)");
+            return FRW_E_ARG;
+        }
+    }
+    frw_layout *L = new frw_layout();
+    L->device = device;
+    L->n = n;
+    L->rects.swap(h);
+    if (bounds) memcpy(L->bounds, bounds, sizeof(L->bounds));
+    else reference_bounds(L->rects.data(), n, L->bounds);
+    const double *b = L->bounds;
+    if (!(b[0] <= b[2] && b[1] <= b[3]) || !std::isfinite(b[0]) || !std::isfinite(b[1]) ||
+        !std::isfinite(b[2]) || !std::isfinite(b[3])) {
+        set_error("bounds invalid");
+        delete L;
+        return FRW_E_ARG;
+    }
+    for (int64_t i = 0; i < n; i++) {
+        const double *q = L->rects.data() + 4 * i;
+        if (!(q[1] >= b[1] && q[0] >= b[0] && q[3] <= b[3] && q[2] <= b[2])) {
+            set_error("rect " + std::to_string(i) + " lies outside the bounds");
+            delete L;
+            return FRW_E_ARG;
+        }
+    }
+    DeviceGuard g(device);
+    cudaStream_t st = (cudaStream_t)stream;
+    float4 *d_in = nullptr;
+    auto fail = [&](frw_status r) {
+        if (d_in) cudaFree(d_in);
+        free_tree(&L->T);
+        delete L;
+        return r;
+    };
+    cudaError_t e = cudaMalloc(&d_in, (size_t)n * 16);
+    if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc rects"));
+    e = cudaMemcpyAsync(d_in, rects, (size_t)n * 16, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return fail(cuda_fail(e, "upload rects"));
+    rc = build_tree(d_in, (int32_t)n, L->bounds, L->leaf_max, st, &L->T, &L->build_ms);
+    if (rc) return fail(rc);
+    cudaFree(d_in);
+    d_in = nullptr;
+    DevLayout &dl = L->dl;
+    dl.rects = L->T.rects;
+    dl.ids = L->T.ids;
+    dl.nbox = L->T.nbox;
+    dl.nref = L->T.nref;
+    dl.bx0 = b[0];
+    dl.by0 = b[1];
+    dl.bx1 = b[2];
+    dl.by1 = b[3];
+    {
+        // drawBiggestSquareAtPoint: dist = (H > W ? H : W) * 0.05
+        const double bw = b[2] - b[0], bh = b[3] - b[1];
+        double dist = (bh > bw) ? bh : bw;
+        dist *= 0.05;
+        dl.dist0 = dist;
+        // tie window: every box of a replay has coordinates below
+        // M = 4 * max(|bounds|, W, H) + 16 after <= 256 roundings of at most
+        // M * 2^-53 each, i.e. within M * 2^-45; delta = M * 2^-40 leaves 32x.
+        double M = std::max(std::max(fabs(b[0]), fabs(b[1])), std::max(fabs(b[2]), fabs(b[3])));
+        M = 4.0 * std::max(M, std::max(bw, bh)) + 16.0;
+        dl.delta = ldexp(M, -40);
+    }
+    dl.n = (int32_t)n;
+    dl.nodes = L->T.nodes;
+    *out = L;
+    return FRW_OK;
+}
+
+frw_status frw_layout_from_file(const char *path, int layer, int device, frw_layout **out) {
+    if (!path || !out) {
+        set_error("frw_layout_from_file: null argument");
+        return FRW_E_ARG;
+    }
+    std::vector<double> r;
+    frw_status rc = parse_layout_file(path, layer, &r, nullptr);
+    if (rc) return rc;
+    const int64_t n = (int64_t)r.size() / 4;
+    if (n == 0) {
+        set_error(std::string(path) + ": layer " + std::to_string(layer) + " has no rects");
+        return FRW_E_ARG;
+    }
+    std::vector<float> f(r.size());
+    for (size_t i = 0; i < r.size(); i++) {
+        if (!fp32_exact(r[i])) {
+            set_error(std::string(path) + ": coordinate " + std::to_string(r[i]) +
+                      " is not exactly representable in FP32 (|c| < 2^24 required)");
+            return FRW_E_ARG;
+        }
+        f[i] = (float)r[i];
+    }
+    double b[4];
+    reference_bounds(r.data(), n, b);
+    return frw_layout_create(f.data(), n, b, device, nullptr, out);
+}
+
+frw_status frw_layout_destroy(frw_layout *L) {
+    if (!L) return FRW_OK;
+    DeviceGuard g(L->device);
+    free_tree(&L->T);
+    delete L;
+    return FRW_OK;
+}
+
+frw_status frw_layout_info_get(const frw_layout *L, frw_layout_info *info) {
+    if (!L || !info) {
+        set_error("null argument");
+        return FRW_E_ARG;
+    }
+    info->n_rects = L->n;
+    info->n_nodes = L->T.nodes;
+    info->depth = L->T.depth;
+    info->leaf_max = L->leaf_max;
+    memcpy(info->bounds, L->bounds, sizeof(info->bounds));
+    info->device_bytes = L->T.bytes;
+    info->device = L->device;
+    info->build_ms = L->build_ms;
+    return FRW_OK;
+}
+
+frw_status frw_layout_rects(const frw_layout *L, double *out) {
+    if (!L || !out) {
+        set_error("null argument");
+        return FRW_E_ARG;
+    }
+    memcpy(out, L->rects.data(), L->rects.size() * sizeof(double));
+    return FRW_OK;
+}
+
+frw_status frw_query_batch(const frw_layout *L, const double *pts, int64_t n, double *sq, int64_t *hit, int mem,
+                           void *stream) {
+    if (!L || (n > 0 && (!pts || !sq || !hit)) || n < 0) {
+        set_error("frw_query_batch: bad arguments");
+        return FRW_E_ARG;
+    }
+    if (n == 0) return FRW_OK;
+    if (mem == FRW_MEM_DEVICE && (((uintptr_t)pts & 15) || ((uintptr_t)sq & 31) || ((uintptr_t)hit & 7))) {
+        set_error("frw_query_batch: device buffers must be aligned (points 16 B, squares 32 B, hits 8 B)");
+        return FRW_E_ARG;
+    }
+    DeviceGuard g(L->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    Scratch S(st);
+    uint32_t *d_status;
+    FRW_CK(S.get(&d_status, 4));
+    FRW_CK(cudaMemsetAsync(d_status, 0, 4, st));
+    const double *dp = pts;
+    double *ds = sq;
+    int64_t *dh = hit;
+    if (mem == FRW_MEM_HOST) {
+        double *a, *b;
+        int64_t *c;
+        FRW_CK(S.get(&a, n * 16));
+        FRW_CK(S.get(&b, n * 32));
+        FRW_CK(S.get(&c, n * 8));
+        FRW_CK(cudaMemcpyAsync(a, pts, n * 16, cudaMemcpyHostToDevice, st));
+        dp = a;
+        ds = b;
+        dh = c;
+    }
+    frw_status rc = launch_query(L->dl, dp, n, ds, dh, d_status, st);
+    if (rc) return rc;
+    if (mem == FRW_MEM_HOST) {
+        FRW_CK(cudaMemcpyAsync(sq, ds, n * 32, cudaMemcpyDeviceToHost, st));
+        FRW_CK(cudaMemcpyAsync(hit, dh, n * 8, cudaMemcpyDeviceToHost, st));
+    }
+    return check_status(d_status, st);
+}
+
+frw_status frw_box_collides_batch(const frw_layout *L, const double *boxes, int64_t n, const double *ignore,
+                                  uint8_t *out, int mem, void *stream) {
+    if (!L || (n > 0 && (!boxes || !out)) || n < 0) {
+        set_error("frw_box_collides_batch: bad arguments");
+        return FRW_E_ARG;
+    }
+    if (n == 0) return FRW_OK;
+    if (mem == FRW_MEM_DEVICE && ((uintptr_t)boxes & 31)) {
+        set_error("frw_box_collides_batch: device boxes must be 32-byte aligned");
+        return FRW_E_ARG;
+    }
+    DeviceGuard g(L->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    Scratch S(st);
+    uint32_t *d_status;
+    FRW_CK(S.get(&d_status, 4));
+    FRW_CK(cudaMemsetAsync(d_status, 0, 4, st));
+    const double *db = boxes;
+    uint8_t *dout = out;
+    if (mem == FRW_MEM_HOST) {
+        double *a;
+        uint8_t *c;
+        FRW_CK(S.get(&a, n * 32));
+        FRW_CK(S.get(&c, n));
+        FRW_CK(cudaMemcpyAsync(a, boxes, n * 32, cudaMemcpyHostToDevice, st));
+        db = a;
+        dout = c;
+    }
+    frw_status rc = launch_box_collides(L->dl, db, n, ignore != nullptr, ignore, dout, d_status, st);
+    if (rc) return rc;
+    if (mem == FRW_MEM_HOST) FRW_CK(cudaMemcpyAsync(out, dout, n, cudaMemcpyDeviceToHost, st));
+    return check_status(d_status, st);
+}
+
+frw_status frw_gauss_surface(const frw_layout *L, int64_t target, const frw_opts *opts, double out[4],
+                             void *stream) {
+    frw_opts o;
+    frw_opts_default(&o);
+    if (opts) o = *opts;
+    frw_status rc = validate_opts(&o);
+    if (rc) return rc;
+    if (!L || !out || target < 0 || target >= L->n) {
+        set_error("frw_gauss_surface: bad arguments");
+        return FRW_E_ARG;
+    }
+    DeviceGuard g(L->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    Scratch S(st);
+    double *d_t, *d_o;
+    uint32_t *d_status;
+    FRW_CK(S.get(&d_t, 32));
+    FRW_CK(S.get(&d_o, 32));
+    FRW_CK(S.get(&d_status, 4));
+    FRW_CK(cudaMemsetAsync(d_status, 0, 4, st));
+    FRW_CK(cudaMemcpyAsync(d_t, L->rects.data() + 4 * target, 32, cudaMemcpyHostToDevice, st));
+    rc = launch_gauss(L->dl, d_t, 1, o.gauss_mode, o.gauss_param, d_o, d_status, st);
+    if (rc) return rc;
+    FRW_CK(cudaMemcpyAsync(out, d_o, 32, cudaMemcpyDeviceToHost, st));
+    return check_status(d_status, st);
+}
+
+frw_status frw_walk(const frw_layout *L, int64_t target, uint64_t walks, uint64_t seed, const frw_opts *opts,
+                    frw_result *res, void *stream) {
+    frw_opts o;
+    frw_opts_default(&o);
+    if (opts) o = *opts;
+    frw_status rc = validate_opts(&o);
+    if (rc) return rc;
+    if (!L || !res) {
+        set_error("frw_walk: null argument");
+        return FRW_E_ARG;
+    }
+    DeviceGuard g(L->device);
+    WalkRun R;
+    rc = run_walks(L, target, 0, walks, seed, o, (cudaStream_t)stream, nullptr, nullptr, nullptr, nullptr, &R);
+    if (rc) return rc;
+    res->walks = walks;
+    res->escaped = R.escaped;
+    res->aborted = R.aborted;
+    res->hops_total = R.hops;
+    memcpy(res->gauss, R.gauss, sizeof(res->gauss));
+    res->kernel_ms = R.kernel_ms;
+    std::vector<size_t> ord(R.row.size());
+    for (size_t i = 0; i < ord.size(); i++) ord[i] = i;
+    std::sort(ord.begin(), ord.end(), [&](size_t a, size_t b) { return R.row[a] < R.row[b]; });
+    uint64_t on_target = 0;
+    res->n_entries = (int64_t)ord.size();
+    const double N = (double)walks;
+    for (size_t k = 0; k < ord.size(); k++) {
+        const size_t i = ord[k];
+        if (R.row[i] == target) on_target = R.n[i];
+        if ((int64_t)k >= res->capacity) continue;
+        const double mean = R.s[i] / N;
+        const double var = walks > 1 ? std::max(R.s2[i] / N - mean * mean, 0.0) * N / (N - 1.0) : 0.0;
+        if (res->conductor) res->conductor[k] = R.row[i];
+        if (res->hits) res->hits[k] = R.n[i];
+        if (res->cap) res->cap[k] = mean;
+        if (res->cap_se) res->cap_se[k] = sqrt(var / N);
+    }
+    res->fraction_other = walks ? (double)(walks - on_target) / N : 0.0;
+    return FRW_OK;
+}
+
+frw_status frw_walk_trace(const frw_layout *L, int64_t target, uint64_t first_walk, uint64_t walks, uint64_t seed,
+                          const frw_opts *opts, int64_t *end, int32_t *hops, int32_t *bin1, double *weight,
+                          int mem, void *stream) {
+    frw_opts o;
+    frw_opts_default(&o);
+    if (opts) o = *opts;
+    frw_status rc = validate_opts(&o);
+    if (rc) return rc;
+    if (!L) {
+        set_error("frw_walk_trace: null layout");
+        return FRW_E_ARG;
+    }
+    DeviceGuard g(L->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    Scratch S(st);
+    int64_t *de;
+    int32_t *dh, *db;
+    double *dw;
+    // the kernel writes all four records; absent ones go to scratch
+    const bool host = mem == FRW_MEM_HOST;
+    if (host || !end) FRW_CK(S.get(&de, walks * 8)); else de = end;
+    if (host || !hops) FRW_CK(S.get(&dh, walks * 4)); else dh = hops;
+    if (host || !bin1) FRW_CK(S.get(&db, walks * 4)); else db = bin1;
+    if (host || !weight) FRW_CK(S.get(&dw, walks * 8)); else dw = weight;
+    rc = run_walks(L, target, first_walk, walks, seed, o, st, de, dh, db, dw, nullptr);
+    if (rc) return rc;
+    if (host) {
+        if (end) FRW_CK(cudaMemcpyAsync(end, de, walks * 8, cudaMemcpyDeviceToHost, st));
+        if (hops) FRW_CK(cudaMemcpyAsync(hops, dh, walks * 4, cudaMemcpyDeviceToHost, st));
+        if (bin1) FRW_CK(cudaMemcpyAsync(bin1, db, walks * 4, cudaMemcpyDeviceToHost, st));
+        if (weight) FRW_CK(cudaMemcpyAsync(weight, dw, walks * 8, cudaMemcpyDeviceToHost, st));
+        FRW_CK(cudaStreamSynchronize(st));
+    }
+    return FRW_OK;
+}
+
+frw_status frw_avg_path_len(const char *path, int64_t iter_num, int64_t rect_id, int layer, uint64_t seed,
+                            int device, const char *hist_path, double *fraction) {
+    if (iter_num <= 0 || !fraction) {
+        set_error("frw_avg_path_len: iter_num must be positive");
+        return FRW_E_ARG;
+    }
+    frw_layout *L = nullptr;
+    frw_status rc = frw_layout_from_file(path, layer, device, &L);
+    if (rc) return rc;
+    if (rect_id < 0 || rect_id >= L->n) {
+        frw_layout_destroy(L);
+        set_error("rect id out of range");
+        return FRW_E_ARG;
+    }
+    frw_opts o;
+    frw_opts_default(&o);  // reference start and Gaussian surface
+    std::vector<int64_t> cond(L->n);
+    std::vector<uint64_t> hits(L->n);
+    frw_result r{};
+    r.capacity = L->n;
+    r.conductor = cond.data();
+    r.hits = hits.data();
+    rc = frw_walk(L, rect_id, (uint64_t)iter_num, seed, &o, &r, nullptr);
+    if (rc == FRW_OK) {
+        *fraction = r.fraction_other;
+        if (hist_path) {
+            // the reference's "<ts>wyniki.txt" layout (Cuda/getAvgPathLenCUDA.cu:23-48):
+            // one line per rect reached, then the escaped share
+            FILE *f = fopen(hist_path, "w");
+            if (!f) {
+                set_error(std::string("cannot write ") + hist_path);
+                rc = FRW_E_IO;
+            } else {
+                fprintf(f, "[GPU]\n");
+                if (r.escaped)
+                    fprintf(f, "Ile scie\xc5\xbc" "ek wysz\xc5\x82o poza granice warstwy: %g%%\n",
+                            (float)r.escaped / (float)iter_num * 100);
+                for (int64_t k = 0; k < std::min(r.n_entries, r.capacity); k++) {
+                    const double *q = L->rects.data() + 4 * cond[k];
+                    fprintf(f, "%g %g %g %g: %g%%\n", q[0], q[1], q[2], q[3],
+                            ((float)hits[k] / (float)iter_num) * 100);
+                }
+                fclose(f);
+            }
+        }
+    }
+    frw_layout_destroy(L);
+    return rc;
+}
+
+frw_status frw_generate_layout(uint64_t seed, int64_t n, double domain, int32_t wmin, int32_t wmax, double gap,
+                               float *out) {
+    if (!out) {
+        set_error("null output");
+        return FRW_E_ARG;
+    }
+    return generate_layout(seed, n, domain, wmin, wmax, gap, out);
+}
+
+frw_status frw_write_layout(const char *path, const float *rects, int64_t n, const char *name) {
+    if (!path || !rects || n <= 0) {
+        set_error("frw_write_layout: bad arguments");
+        return FRW_E_ARG;
+    }
+    return write_layout(path, rects, n, name);
+}
+
+}  // extern "C"

@@ -1,0 +1,143 @@
+// frw_cli.cpp -- command-line front end with the reference's flags
+// (randomWalk/main.cpp:25-126, defines.h:30-40):
+//   -S/--source <file>  -I/--iterations <n>  -O/--object <id>  -L/--layer <k>
+//   -G/--GPU (accepted; the device path is the only path)  -M/--measure  --help
+// Extra flags: --seed <u64>, --device <k>, --uniform (uniform start and
+// capacitance weights), --offset <d> (Gaussian surface = target grown by d),
+// --scale <f> (reference scaled surface, default 1.5), --exact-perimeter,
+// --cap (print the capacitance row), --hist <file> (histogram file name;
+// default "<unixtime>wyniki.txt" as the reference writes).
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+#include <chrono>
+#include <string>
+#include <vector>
+
+#include "../../include/frw.h"
+
+static const char *kHelp =
+    "\t-S\t--source\t\tlayout file\n"
+    "\t-M\t--measure\t\tprint timings\n"
+    "\t-O\t--object\t\ttarget rect id\n"
+    "\t-I\t--iterations\t\tnumber of walks\n"
+    "\t-G\t--GPU\t\t\t(accepted; walks always run on the GPU)\n"
+    "\t-L\t--layer\t\t\tlayer number\n"
+    "\t\t--seed <u64> --device <k> --uniform --offset <d> --scale <f>\n"
+    "\t\t--exact-perimeter --cap --hist <file>\n"
+    "\t\t--help\t\t\tthis text\n"
+    "\tDefaults: -I 1000 -O 10 -S ../tests/test -L 0\n";
+
+int main(int argc, char **argv) {
+    std::string path = "../tests/test", hist;
+    long long iters = 1000, object = 10;
+    int layer = 0, device = 0;
+    bool measure = false, uniform = false, cap = false, exact = false;
+    unsigned long long seed = (unsigned long long)time(nullptr);
+    double offset = -1.0, scale = 1.5;
+    for (int i = 1; i < argc; i++) {
+        std::string a = argv[i];
+        auto val = [&](const char *what) -> const char * {
+            if (i + 1 >= argc) {
+                fprintf(stderr, "%s needs a value\n", what);
+                exit(2);
+            }
+            return argv[++i];
+        };
+        if (a == "-S" || a == "--source") path = val("-S");
+        else if (a == "-I" || a == "--iterations") iters = atoll(val("-I"));
+        else if (a == "-O" || a == "--object") object = atoll(val("-O"));
+        else if (a == "-L" || a == "--layer") layer = atoi(val("-L"));
+        else if (a == "-G" || a == "--GPU") {
+        } else if (a == "-M" || a == "--measure") measure = true;
+        else if (a == "--seed") seed = strtoull(val("--seed"), nullptr, 0);
+        else if (a == "--device") device = atoi(val("--device"));
+        else if (a == "--uniform") uniform = true;
+        else if (a == "--offset") offset = atof(val("--offset"));
+        else if (a == "--scale") scale = atof(val("--scale"));
+        else if (a == "--exact-perimeter") exact = true;
+        else if (a == "--cap") cap = true;
+        else if (a == "--hist") hist = val("--hist");
+        else if (a == "--help" || a == "-h") {
+            printf("%s", kHelp);
+            return 0;
+        } else {
+            fprintf(stderr, "unknown argument %s\n%s", a.c_str(), kHelp);
+            return 2;
+        }
+    }
+    if (iters <= 0) {
+        fprintf(stderr, "Incorrect args!\n");
+        return 2;
+    }
+    auto t0 = std::chrono::steady_clock::now();
+    frw_layout *L = nullptr;
+    if (frw_layout_from_file(path.c_str(), layer, device, &L) != FRW_OK) {
+        fprintf(stderr, "error: %s\n", frw_last_error());
+        return 1;
+    }
+    frw_layout_info info;
+    frw_layout_info_get(L, &info);
+    if (object < 0 || object >= info.n_rects) {
+        fprintf(stderr, "Incorrect args! (object %lld of %lld rects)\n", object, (long long)info.n_rects);
+        frw_layout_destroy(L);
+        return 2;
+    }
+    frw_opts o;
+    frw_opts_default(&o);
+    if (offset >= 0) {
+        o.gauss_mode = FRW_GAUSS_OFFSET;
+        o.gauss_param = offset;
+    } else {
+        o.gauss_param = scale;
+    }
+    o.start_mode = uniform ? FRW_START_UNIFORM : FRW_START_GREEN;
+    o.exact_perimeter = exact ? 1 : 0;
+    std::vector<int64_t> cond(info.n_rects);
+    std::vector<uint64_t> hits(info.n_rects);
+    std::vector<double> c(info.n_rects), se(info.n_rects);
+    frw_result r{};
+    r.capacity = info.n_rects;
+    r.conductor = cond.data();
+    r.hits = hits.data();
+    r.cap = c.data();
+    r.cap_se = se.data();
+    if (frw_walk(L, object, (uint64_t)iters, seed, &o, &r, nullptr) != FRW_OK) {
+        fprintf(stderr, "error: %s\n", frw_last_error());
+        frw_layout_destroy(L);
+        return 1;
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    if (hist.empty()) hist = std::to_string((unsigned long)time(nullptr)) + "wyniki.txt";
+    FILE *f = fopen(hist.c_str(), "w");
+    if (f) {
+        fprintf(f, "[GPU]\n");
+        if (r.escaped)
+            fprintf(f, "Ile scie\xc5\xbc" "ek wysz\xc5\x82o poza granice warstwy: %g%%\n",
+                    (float)r.escaped / (float)iters * 100);
+        std::vector<double> q(4 * info.n_rects);
+        frw_layout_rects(L, q.data());
+        for (int64_t k = 0; k < r.n_entries && k < r.capacity; k++)
+            fprintf(f, "%g %g %g %g: %g%%\n", q[4 * cond[k]], q[4 * cond[k] + 1], q[4 * cond[k] + 2],
+                    q[4 * cond[k] + 3], ((float)hits[k] / (float)iters) * 100);
+        fclose(f);
+        printf("Wynik zapisany do %s\n", hist.c_str());
+    }
+    printf("[GPU] Ile sciezek trafi\xc5\x82o do innego elementu: %f%%\n", r.fraction_other * 100.);
+    printf("Czas wykonania: %lld ms\n",
+           (long long)std::chrono::duration_cast<std::chrono::milliseconds>(t1 - t0).count());
+    if (measure)
+        printf("tree build %.3f ms (%lld nodes, depth %d); walk kernel %.3f ms; %.1f hops/walk; "
+               "%.3e walks/s\n",
+               info.build_ms, (long long)info.n_nodes, info.depth, r.kernel_ms,
+               (double)r.hops_total / (double)iters, iters / (r.kernel_ms * 1e-3));
+    if (cap && uniform) {
+        printf("capacitance row of conductor %lld (F/m), %llu walks:\n", object, (unsigned long long)iters);
+        for (int64_t k = 0; k < r.n_entries && k < r.capacity; k++)
+            printf("  C[%lld,%lld] = %.6e +- %.2e\n", object, (long long)cond[k], c[k], se[k]);
+    }
+    frw_layout_destroy(L);
+    return 0;
+}

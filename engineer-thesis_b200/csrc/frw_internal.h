@@ -1,0 +1,140 @@
+// frw_internal.h -- shared declarations of the FRW library (host + device).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/frw.h"
+
+namespace frw {
+
+// ---- quadtree layout in HBM --------------------------------------------------
+// Rects are stored Morton-sorted as float4 (x0,y0,x1,y1): 16-byte vector
+// loads, exact because every accepted coordinate is FP32-representable.
+// Each internal node holds the boxes of its four children (4 x float4 = 64 B,
+// 64-byte aligned) in `nbox` and their references (int4) in `nref`:
+//   ref >= 0         internal node index
+//   ref == -1        empty quadrant
+//   ref <= -2        leaf: -2 - ((first_rect << 5) | count), count <= 31
+constexpr int kLeafBits = 5;
+constexpr int kLeafCountMax = (1 << kLeafBits) - 1;
+constexpr int kRefEmpty = -1;
+constexpr int kDefaultLeafMax = 8;
+
+#if defined(__CUDACC__)
+#define FRW_HD __host__ __device__ inline
+#else
+#define FRW_HD inline
+#endif
+FRW_HD int leaf_ref(int first, int count) { return -2 - ((first << kLeafBits) | count); }
+FRW_HD int leaf_first(int ref) { return (-2 - ref) >> kLeafBits; }
+FRW_HD int leaf_count(int ref) { return (-2 - ref) & kLeafCountMax; }
+
+struct DevLayout {
+    const float4 *rects;  // [n] Morton order
+    const int32_t *ids;   // [n] Morton position -> layer index
+    const float4 *nbox;   // [4 * nodes]
+    const int4 *nref;     // [nodes]
+    double bx0, by0, bx1, by1;  // layer bounds (reference getLayerSize)
+    double dist0;               // 0.05 * max(W, H): drawBiggestSquareAtPoint's first step
+    double delta;               // tie window of the clearance replay (see query.cuh)
+    int32_t n, nodes;
+};
+
+// ---- device status word (atomicOr'ed by kernels, read back by the host) ----
+enum : uint32_t {
+    kStCandOverflow = 1u,   // more near-tied rects than the candidate list holds
+    kStStackOverflow = 2u,  // traversal stack overflow
+    kStReplayCap = 4u,      // bisection replay exceeded its iteration bound
+    kStBadInput = 8u,       // a kernel met an input outside its contract
+};
+
+// ---- walk jobs ----------------------------------------------------------------
+struct WalkJob {
+    DevLayout L;
+    int64_t target;       // layer index
+    uint64_t walk_begin;  // first global walk index of this job
+    uint64_t walks;       // walks of this job
+    uint64_t first_walk;  // Philox walk index of the job's first walk
+    int64_t acc_base;     // accumulator offset (per-conductor rows)
+    uint32_t stream_id;
+    int32_t pad;
+};
+
+struct WalkParams {
+    WalkJob job0;          // the job of a single-job launch (read from parameter space)
+    const WalkJob *jobs;   // [njobs] for a multi-job launch
+    const double4 *gauss;  // [njobs] Gaussian surfaces (written on the device by launch_gauss)
+    int32_t njobs;
+    int32_t start_mode;
+    int32_t exact_perimeter;
+    int32_t refill_min;
+    int64_t hop_cap;
+    double permittivity;
+    uint64_t seed;
+    uint64_t total_walks;
+    unsigned long long *counter;  // global walk counter (refill)
+    // per-conductor accumulators (dense rows, acc_base + layer index)
+    unsigned long long *acc_n;
+    double *acc_s;
+    double *acc_s2;
+    // per-job scalars [njobs][4]: escaped, aborted, hops, done
+    unsigned long long *job_stats;
+    uint32_t *status;
+    // optional per-walk records (indexed by global walk index)
+    int64_t *rec_end;
+    int32_t *rec_hops;
+    int32_t *rec_bin;
+    double *rec_w;
+    // tables
+    const double *intg;  // [201]
+    const double *wx;    // [200]
+    const double *wy;    // [200]
+};
+
+// ---- host helpers ----------------------------------------------------------
+void set_error(const std::string &msg);
+frw_status cuda_fail(cudaError_t e, const char *what);
+
+#define FRW_CK(call)                                          \
+    do {                                                      \
+        cudaError_t e__ = (call);                             \
+        if (e__ != cudaSuccess) return cuda_fail(e__, #call); \
+    } while (0)
+
+// tree_build.cu
+struct TreeBuffers {
+    float4 *rects = nullptr;
+    int32_t *ids = nullptr;
+    float4 *nbox = nullptr;
+    int4 *nref = nullptr;
+    int32_t nodes = 0, depth = 0;
+    int64_t bytes = 0;
+};
+frw_status build_tree(const float4 *d_rects_in, int32_t n, const double bounds[4], int leaf_max,
+                      cudaStream_t stream, TreeBuffers *out, float *build_ms);
+void free_tree(TreeBuffers *t);
+
+// query.cu
+frw_status launch_query(const DevLayout &L, const double *d_pts, int64_t n, double *d_sq,
+                        int64_t *d_hit, uint32_t *d_status, cudaStream_t stream);
+frw_status launch_box_collides(const DevLayout &L, const double *d_boxes, int64_t n, bool has_ignore,
+                               const double ignore[4], uint8_t *d_out, uint32_t *d_status,
+                               cudaStream_t stream);
+frw_status launch_gauss(const DevLayout &L, const double *d_targets /*[n][4]*/, int n, int mode,
+                        double param, double *d_out, uint32_t *d_status, cudaStream_t stream);
+
+// walk.cu
+frw_status launch_walk(const WalkParams &P, int threads, int blocks, cudaStream_t stream);
+int walk_max_blocks_per_sm(int threads, bool multi);
+// Compacts the nonzero accumulator rows: returns their count through *d_count.
+frw_status launch_compact(const unsigned long long *acc_n, const double *acc_s, const double *acc_s2,
+                          int64_t rows, int64_t *out_row, unsigned long long *out_n, double *out_s,
+                          double *out_s2, unsigned long long *d_count, cudaStream_t stream);
+
+// host_green.cpp
+void green_tables(double *g, double *intg, double *wx, double *wy);
+
+}  // namespace frw

@@ -1,0 +1,284 @@
+// query.cuh -- device-side collision queries on the flat Morton quadtree.
+//
+// The reference answers drawBiggestSquareAtPoint (CPU/quadTree.cpp:264-312,
+// Cuda/d_quadTree.cu:86-134) with 17-26 full tree traversals per point: one
+// checkCollisions(box) per step of an expand/bisect loop.  Here ONE traversal
+// per point computes the L-infinity clearance
+//     d* = min( distance to the layer bounds, min_R gap(R, p) ),
+//     gap(R, p) = max(R.x0 - p.x, p.x - R.x1, R.y0 - p.y, p.y - R.y1),
+// and the short list of rects whose gap lies within 2*delta of d*; the loop is
+// then replayed on scalars with the reference's own FP64 operations.  Every
+// box of the loop is p +- h up to the rounding of its four coordinates
+// (each within eps of the others, eps << delta), so a rect outside the list
+// can only touch such a box when the box's smallest extent already exceeds d*
+// + delta, and then the nearest rect (in the list) touches it too.  Hence
+//     collides(box) = outside(bounds) || any(listed rect touches box)
+// exactly, and the returned square is bit-identical to the reference's.
+// The point query (checkCollisons(point), CPU/quadTree.cpp:240-262) falls out
+// of the same traversal: rects with gap <= 0 contain p (closed intervals).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "frw_internal.h"
+
+namespace frw {
+
+constexpr int kStackMax = 64;
+constexpr int kCandMax = 8;
+constexpr int kReplayCap = 256;
+constexpr int kNoHit = 0x7FFFFFFF;
+constexpr double kMinDist = (double).095f;  // drawBiggestSquareAtPoint MIN_DIST
+
+struct Cands {
+    int idx[kCandMax];  // Morton positions of the near-tied rects
+    float g[kCandMax];  // their gaps, rounded down (keeping extra entries is harmless)
+    int n;
+};
+
+__device__ __forceinline__ double lb_box(const float4 b, double px, double py) {
+    double d = fmax(fmax((double)b.x - px, px - (double)b.z), fmax((double)b.y - py, py - (double)b.w));
+    return fmax(d, 0.0);
+}
+
+// One depth-first, nearest-child-first traversal.  Returns status bits.
+__device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, double py, Cands &C,
+                                              int &hit, double &best) {
+    uint32_t st = 0;
+    const double r2 = 2.0 * L.delta;
+    best = fmin(fmin(px - L.bx0, L.bx1 - px), fmin(py - L.by0, L.by1 - py));
+    hit = kNoHit;
+    C.n = 0;
+    int stk_node[kStackMax];
+    float stk_lb[kStackMax];
+    int sp = 1;
+    stk_node[0] = 0;
+    stk_lb[0] = 0.f;
+    while (sp > 0) {
+        --sp;
+        const int nd = stk_node[sp];
+        if ((double)stk_lb[sp] > fmax(best, 0.0) + r2) continue;
+        const float4 *bp = L.nbox + 4 * nd;
+        float4 b[4];
+        b[0] = __ldg(bp);
+        b[1] = __ldg(bp + 1);
+        b[2] = __ldg(bp + 2);
+        b[3] = __ldg(bp + 3);
+        const int4 rf = __ldg(L.nref + nd);
+        const int ref[4] = {rf.x, rf.y, rf.z, rf.w};
+        double lb[4];
+#pragma unroll
+        for (int c = 0; c < 4; c++) lb[c] = ref[c] == kRefEmpty ? 1e300 : lb_box(b[c], px, py);
+        // leaves of this node first: they tighten `best` before children are pushed
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            if (ref[c] > kRefEmpty || ref[c] == kRefEmpty) continue;
+            if (lb[c] > fmax(best, 0.0) + r2) continue;
+            const int f = leaf_first(ref[c]), m = leaf_count(ref[c]);
+            for (int k = f; k < f + m; k++) {
+                const float4 r = __ldg(L.rects + k);
+                const double x0 = r.x, y0 = r.y, x1 = r.z, y1 = r.w;
+                const double g = fmax(fmax(x0 - px, px - x1), fmax(y0 - py, py - y1));
+                if (g <= 0.0 && px >= x0 && py >= y0 && px <= x1 && py <= y1) {
+                    const int id = __ldg(L.ids + k);
+                    hit = id < hit ? id : hit;
+                }
+                if (g < best) {
+                    best = g;
+                    int j = 0;
+                    for (int q = 0; q < C.n; q++)
+                        if ((double)C.g[q] <= best + r2) {
+                            C.idx[j] = C.idx[q];
+                            C.g[j] = C.g[q];
+                            j++;
+                        }
+                    C.n = j;
+                }
+                if (g <= best + r2) {
+                    if (C.n < kCandMax) {
+                        C.idx[C.n] = k;
+                        C.g[C.n] = __double2float_rd(g);
+                        C.n++;
+                    } else {
+                        st |= kStCandOverflow;
+                    }
+                }
+            }
+        }
+        // internal children, farthest pushed first so the nearest is popped next
+        const double lim = fmax(best, 0.0) + r2;
+        int ord[4] = {0, 1, 2, 3};
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+            for (int c = 0; c < 3 - a; c++)
+                if (lb[ord[c]] < lb[ord[c + 1]]) {
+                    int t = ord[c];
+                    ord[c] = ord[c + 1];
+                    ord[c + 1] = t;
+                }
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int q = ord[c];
+            if (ref[q] < 0 || lb[q] > lim) continue;
+            if (sp < kStackMax) {
+                stk_node[sp] = ref[q];
+                stk_lb[sp] = __double2float_rd(lb[q]);
+                sp++;
+            } else {
+                st |= kStStackOverflow;
+            }
+        }
+    }
+    return st;
+}
+
+// Tree::checkCollisions(box) restricted to the near-tie list (exact for the
+// boxes of the replay, see the file comment).
+__device__ __forceinline__ bool collides_listed(const DevLayout &L, const Cands &C, const double o[4]) {
+    if (!(o[1] >= L.by0 && o[0] >= L.bx0 && o[3] <= L.by1 && o[2] <= L.bx1)) return true;
+    for (int q = 0; q < C.n; q++) {
+        const float4 r = __ldg(L.rects + C.idx[q]);
+        if ((double)r.z >= o[0] && o[2] >= (double)r.x && (double)r.w >= o[1] && o[3] >= (double)r.y)
+            return true;
+    }
+    return false;
+}
+
+// drawBiggestSquareAtPoint replayed on scalars: same operations, same order,
+// explicit round-to-nearest intrinsics (no contraction).
+__device__ __forceinline__ uint32_t replay_square(const DevLayout &L, const Cands &C, double px,
+                                                  double py, double sq[4]) {
+    double o[4] = {__dsub_rn(px, 1.0), __dsub_rn(py, 1.0), __dadd_rn(px, 1.0), __dadd_rn(py, 1.0)};
+    if (collides_listed(L, C, o)) {
+        sq[0] = o[0]; sq[1] = o[1]; sq[2] = o[2]; sq[3] = o[3];
+        return 0;
+    }
+    const double in2[4] = {__dsub_rn(px, 2.0), __dsub_rn(py, 2.0), __dadd_rn(px, 2.0),
+                           __dadd_rn(py, 2.0)};
+    if (collides_listed(L, C, in2)) {
+        sq[0] = in2[0]; sq[1] = in2[1]; sq[2] = in2[2]; sq[3] = in2[3];
+        return 0;
+    }
+    double dist = L.dist0;
+    bool maxReached = false, isc;
+    uint32_t st = 0;
+    int it = 0;
+    while ((isc = collides_listed(L, C, o)) || !maxReached || dist > kMinDist) {
+        if (isc) {
+            if (dist > kMinDist) dist = __ddiv_rn(dist, 2.0);
+            maxReached = true;
+            o[0] = __dadd_rn(o[0], dist);
+            o[1] = __dadd_rn(o[1], dist);
+            o[2] = __dsub_rn(o[2], dist);
+            o[3] = __dsub_rn(o[3], dist);
+        } else {
+            if (maxReached) dist = __ddiv_rn(dist, 2.0);
+            o[0] = __dsub_rn(o[0], dist);
+            o[1] = __dsub_rn(o[1], dist);
+            o[2] = __dadd_rn(o[2], dist);
+            o[3] = __dadd_rn(o[3], dist);
+        }
+        if (++it > kReplayCap) {
+            st |= kStReplayCap;
+            break;
+        }
+    }
+    sq[0] = o[0]; sq[1] = o[1]; sq[2] = o[2]; sq[3] = o[3];
+    return st;
+}
+
+// drawBiggestSquareAtPoint + checkCollisons(point) for one point.
+__device__ __forceinline__ uint32_t query_point(const DevLayout &L, double px, double py, double sq[4],
+                                                int &hit) {
+    Cands C;
+    double best;
+    uint32_t st = clearance(L, px, py, C, hit, best);
+    st |= replay_square(L, C, px, py, sq);
+    return st;
+}
+
+// Tree::checkCollisions(box, ignore) for an arbitrary box (complete DFS).
+__device__ __forceinline__ bool box_collides(const DevLayout &L, const double B[4], bool has_ign,
+                                             const double ign[4], uint32_t &st) {
+    if (!(B[1] >= L.by0 && B[0] >= L.bx0 && B[3] <= L.by1 && B[2] <= L.bx1)) return true;
+    int stk[kStackMax];
+    int sp = 1;
+    stk[0] = 0;
+    while (sp > 0) {
+        const int nd = stk[--sp];
+        const int4 rf = __ldg(L.nref + nd);
+        const int ref[4] = {rf.x, rf.y, rf.z, rf.w};
+        for (int c = 0; c < 4; c++) {
+            if (ref[c] == kRefEmpty) continue;
+            const float4 b = __ldg(L.nbox + 4 * nd + c);
+            if (!((double)b.z >= B[0] && B[2] >= (double)b.x && (double)b.w >= B[1] && B[3] >= (double)b.y))
+                continue;
+            if (ref[c] >= 0) {
+                if (sp < kStackMax) stk[sp++] = ref[c];
+                else st |= kStStackOverflow;
+                continue;
+            }
+            const int f = leaf_first(ref[c]), m = leaf_count(ref[c]);
+            for (int k = f; k < f + m; k++) {
+                const float4 r = __ldg(L.rects + k);
+                const double x0 = r.x, y0 = r.y, x1 = r.z, y1 = r.w;
+                if (has_ign && x0 == ign[0] && y0 == ign[1] && x1 == ign[2] && y1 == ign[3]) continue;
+                if (x1 >= B[0] && B[2] >= x0 && y1 >= B[1] && B[3] >= y0) return true;
+            }
+        }
+    }
+    return false;
+}
+
+// RectHost::getPointFromNindex (CPU/rectHost.cpp:107-161; GPU twin
+// Cuda/d_Rect.cu:34-101): branch structure and operand order kept because
+// they decide ties; the perimeter is truncated to int unless `exact`.
+__device__ __forceinline__ void point_from_index(const double s[4], int index, bool exact, double &ox,
+                                                 double &oy) {
+    const double per2 = __dadd_rn(__dmul_rn(2.0, __dsub_rn(s[2], s[0])), __dmul_rn(2.0, __dsub_rn(s[3], s[1])));
+    const double perim = exact ? per2 : (double)__double2int_rz(per2);
+    const double v = __ddiv_rn(perim, (double)FRW_NSAMPLE);
+    const double h = __dsub_rn(s[3], s[1]);
+    const double w = __dsub_rn(s[2], s[0]);
+    const double iv = __dmul_rn((double)index, v), jv = __dmul_rn((double)(index - 1), v);
+    const double hv = __ddiv_rn(v, 2.0);
+    const double wh = __dadd_rn(w, h), w2h = __dadd_rn(__dmul_rn(2.0, w), h);
+    if (iv < w) {
+        ox = (double)__double2int_rz(__dadd_rn(__dadd_rn(jv, hv), s[0]));
+        oy = s[1];
+    } else if (jv < w && iv > w) {
+        ox = s[2];
+        oy = s[1];
+    } else if (iv < wh) {
+        ox = s[2];
+        if (jv > w) oy = __dadd_rn(__dsub_rn(__dadd_rn(s[1], jv), w), hv);
+        else {
+            const double t = __dsub_rn(iv, w);
+            oy = __dadd_rn(__dsub_rn(__dadd_rn(s[1], iv), w), __ddiv_rn(t, 2.0));
+        }
+    } else if (jv < wh && iv > wh) {
+        ox = s[2];
+        oy = s[3];
+    } else if (iv < w2h) {
+        oy = s[3];
+        if (jv > wh) ox = __dsub_rn(s[2], __dadd_rn(__dsub_rn(__dsub_rn(jv, w), h), hv));
+        else {
+            const double t = __dsub_rn(__dsub_rn(iv, w), h);
+            ox = __dsub_rn(s[2], __dadd_rn(t, __ddiv_rn(t, 2.0)));
+        }
+    } else if (jv < w2h && iv > w2h) {
+        ox = s[0];
+        oy = s[3];
+    } else {
+        ox = s[0];
+        const double w2 = __dmul_rn(2.0, w);
+        if (jv > w2h) oy = __dsub_rn(s[3], __dadd_rn(__dsub_rn(__dsub_rn(jv, w2), h), hv));
+        else {
+            const double t = __dsub_rn(__dsub_rn(iv, w2), h);
+            oy = __dsub_rn(s[3], __dadd_rn(t, __ddiv_rn(t, 2.0)));
+        }
+    }
+}
+
+}  // namespace frw

@@ -1,0 +1,405 @@
+// tree_build.cu -- bottom-up Morton quadtree build on the device.
+//
+// Replaces the reference's dynamic-parallelism build (createQuadTreeKernel,
+// Cuda/createquadtree.cu:97-371: one block per node, recursive device
+// launches, a 5.59 M-node array allocated up front) with:
+//   1. Morton keys of the rect centres (16 bits per axis over the bounds);
+//   2. a stable LSD radix sort (4 x 8-bit passes) whose scatter ranks items
+//      with warp match/ballot + popc instead of shared-memory atomics;
+//   3. a level-synchronous split of Morton ranges: each frontier range is cut
+//      at its next base-4 digit by binary search on the sorted keys (no data
+//      movement); child node ids come from a count -> scan -> emit pass, so
+//      the build is deterministic; single-quadrant ranges are re-split one
+//      level down without emitting a node (path compression); ranges whose
+//      keys are all equal are split by index;
+//   4. a bottom-up refit of the child boxes, batch by batch in reverse
+//      allocation order (children are always allocated after their parent).
+// Output is the flat node array of frw_internal.h: 64-byte child-box records
+// plus 16-byte child references, nodes of one level contiguous.
+// The tree shape does not affect query results: queries are exact whatever
+// the structure (the boxes are exact FP32 unions of FP32-exact rects).
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "frw_internal.h"
+
+namespace frw {
+namespace {
+
+constexpr int kRsThreads = 256;
+constexpr int kRsWarps = kRsThreads / 32;
+constexpr int kRsItems = 8;  // per thread
+constexpr int kRsTile = kRsThreads * kRsItems;
+constexpr int kRsChunk = kRsTile / kRsWarps;  // contiguous items per warp
+
+__device__ __forceinline__ uint32_t spread_bits(uint32_t v) {
+    v &= 0xFFFFu;
+    v = (v | (v << 8)) & 0x00FF00FFu;
+    v = (v | (v << 4)) & 0x0F0F0F0Fu;
+    v = (v | (v << 2)) & 0x33333333u;
+    v = (v | (v << 1)) & 0x55555555u;
+    return v;
+}
+
+__global__ void k_morton(const float4 *__restrict__ rects, int n, double bx0, double by0, double sx,
+                         double sy, uint32_t *__restrict__ keys, int32_t *__restrict__ vals) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 r = rects[i];
+    double cx = ((double)r.x + (double)r.z) * 0.5, cy = ((double)r.y + (double)r.w) * 0.5;
+    double fx = (cx - bx0) * sx, fy = (cy - by0) * sy;  // sx = 65536 / W
+    uint32_t qx = fx <= 0.0 ? 0u : (fx >= 65535.0 ? 65535u : (uint32_t)fx);
+    uint32_t qy = fy <= 0.0 ? 0u : (fy >= 65535.0 ? 65535u : (uint32_t)fy);
+    keys[i] = spread_bits(qx) | (spread_bits(qy) << 1);
+    vals[i] = i;
+}
+
+__global__ void __launch_bounds__(kRsThreads) k_rs_hist(const uint32_t *__restrict__ keys, int n,
+                                                        int shift, uint32_t *__restrict__ hist,
+                                                        int nblk) {
+    __shared__ uint32_t h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    int base = blockIdx.x * kRsTile;
+    for (int k = 0; k < kRsItems; k++) {
+        int i = base + k * kRsThreads + threadIdx.x;
+        if (i < n) atomicAdd(&h[(keys[i] >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    hist[threadIdx.x * nblk + blockIdx.x] = h[threadIdx.x];
+}
+
+// Exclusive scan of up to a few million u32/u64 values with one block.
+template <typename T>
+__global__ void __launch_bounds__(1024) k_scan_excl(T *data, int64_t n, T *total) {
+    __shared__ T part[1024];
+    int t = threadIdx.x;
+    int64_t per = (n + 1023) / 1024;
+    int64_t a = t * per, b = a + per < n ? a + per : n;
+    T s = 0;
+    for (int64_t i = a; i < b; i++) s += data[i];
+    part[t] = s;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+        T v = t >= off ? part[t - off] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    T run = t ? part[t - 1] : 0;
+    for (int64_t i = a; i < b; i++) {
+        T v = data[i];
+        data[i] = run;
+        run += v;
+    }
+    if (t == 1023 && total) *total = part[1023];
+}
+
+// Stable scatter: warp w of a tile owns kRsChunk consecutive items and walks
+// them 32 at a time; __match_any_sync groups equal digits, popc of the lower
+// peers gives the rank inside the chunk.
+__global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint32_t *__restrict__ kin,
+                                                           const int32_t *__restrict__ vin,
+                                                           uint32_t *__restrict__ kout,
+                                                           int32_t *__restrict__ vout, int n,
+                                                           int shift, const uint32_t *__restrict__ hist,
+                                                           int nblk) {
+    __shared__ uint32_t cnt[kRsWarps][256];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int d = threadIdx.x; d < kRsWarps * 256; d += kRsThreads) (&cnt[0][0])[d] = 0;
+    __syncthreads();
+    const int base = blockIdx.x * kRsTile + w * kRsChunk;
+    const uint32_t lt = (1u << lane) - 1u;
+    for (int c = 0; c < kRsChunk; c += 32) {
+        int i = base + c + lane;
+        uint32_t d = i < n ? (kin[i] >> shift) & 255u : 256u;
+        uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+        if (d < 256u && (peers & lt) == 0) cnt[w][d] += __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    {
+        int d = threadIdx.x;  // 256 threads == 256 digits
+        uint32_t off = hist[d * nblk + blockIdx.x];
+        for (int ww = 0; ww < kRsWarps; ww++) {
+            uint32_t t = cnt[ww][d];
+            cnt[ww][d] = off;
+            off += t;
+        }
+    }
+    __syncthreads();
+    for (int c = 0; c < kRsChunk; c += 32) {
+        int i = base + c + lane;
+        uint32_t key = i < n ? kin[i] : 0u;
+        uint32_t d = i < n ? (key >> shift) & 255u : 256u;
+        uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+        uint32_t pos = 0;
+        if (d < 256u) pos = cnt[w][d] + __popc(peers & lt);
+        __syncwarp();
+        if (d < 256u) {
+            kout[pos] = key;
+            vout[pos] = vin[i];
+            if ((peers & lt) == 0) cnt[w][d] += __popc(peers);
+        }
+        __syncwarp();
+    }
+}
+
+__global__ void k_gather(const float4 *__restrict__ in, const int32_t *__restrict__ perm, int n,
+                         float4 *__restrict__ out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = in[perm[i]];
+}
+
+struct Frontier {
+    int32_t *node, *level, *start, *end;
+};
+
+__device__ __forceinline__ int lower_digit(const uint32_t *keys, int s, int e, int shift, uint32_t d) {
+    // first index in [s, e) whose digit at `shift` is >= d (digits are sorted there)
+    int lo = s, hi = e;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (((keys[mid] >> shift) & 3u) < d) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ void child_bounds(const uint32_t *keys, int level, int s, int e, int b[5]) {
+    b[0] = s;
+    b[4] = e;
+    if (level < 16) {
+        int shift = 30 - 2 * level;
+        for (int d = 1; d < 4; d++) b[d] = lower_digit(keys, s, e, shift, (uint32_t)d);
+    } else {  // identical keys: split by index
+        for (int d = 1; d < 4; d++) b[d] = s + (int)((int64_t)(e - s) * d / 4);
+    }
+}
+
+// Per frontier entry: (new nodes << 32) | (next-frontier entries).
+__global__ void k_split_count(const uint32_t *__restrict__ keys, Frontier fr, int nfr, int leaf_max,
+                              unsigned long long *__restrict__ cnt) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nfr) return;
+    int b[5];
+    int level = fr.level[i];
+    child_bounds(keys, level, fr.start[i], fr.end[i], b);
+    int nonempty = 0, big = 0;
+    for (int c = 0; c < 4; c++) {
+        int m = b[c + 1] - b[c];
+        nonempty += m > 0;
+        big += m > leaf_max;
+    }
+    unsigned long long v;
+    if (nonempty == 1 && level < 16 && big == 1) v = 1ull;  // compress: re-split one level down
+    else v = ((unsigned long long)big << 32) | (unsigned long long)big;
+    cnt[i] = v;
+}
+
+__global__ void k_split_emit(const uint32_t *__restrict__ keys, Frontier fr, int nfr, int leaf_max,
+                             const unsigned long long *__restrict__ off, int node_base,
+                             int4 *__restrict__ nref, Frontier nx) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nfr) return;
+    int b[5];
+    int level = fr.level[i], node = fr.node[i];
+    child_bounds(keys, level, fr.start[i], fr.end[i], b);
+    int nonempty = 0, big = 0;
+    for (int c = 0; c < 4; c++) {
+        int m = b[c + 1] - b[c];
+        nonempty += m > 0;
+        big += m > leaf_max;
+    }
+    unsigned long long o = off[i];
+    int onode = (int)(o >> 32), onext = (int)(o & 0xFFFFFFFFull);
+    if (nonempty == 1 && level < 16 && big == 1) {
+        nx.node[onext] = node;
+        nx.level[onext] = level + 1;
+        nx.start[onext] = fr.start[i];
+        nx.end[onext] = fr.end[i];
+        return;
+    }
+    int ref[4];
+    int j = 0;
+    for (int c = 0; c < 4; c++) {
+        int m = b[c + 1] - b[c];
+        if (m == 0) ref[c] = kRefEmpty;
+        else if (m <= leaf_max) ref[c] = leaf_ref(b[c], m);
+        else {
+            int id = node_base + onode + j;
+            ref[c] = id;
+            nx.node[onext + j] = id;
+            nx.level[onext + j] = level + 1;
+            nx.start[onext + j] = b[c];
+            nx.end[onext + j] = b[c + 1];
+            j++;
+        }
+    }
+    nref[node] = make_int4(ref[0], ref[1], ref[2], ref[3]);
+}
+
+__device__ __forceinline__ float4 box_union(float4 a, float4 b) {
+    return make_float4(fminf(a.x, b.x), fminf(a.y, b.y), fmaxf(a.z, b.z), fmaxf(a.w, b.w));
+}
+
+__global__ void k_refit(const float4 *__restrict__ rects, const int4 *__restrict__ nref,
+                        float4 *__restrict__ nbox, int a, int b) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int node = a + (t >> 2), c = t & 3;
+    if (node >= b) return;
+    int4 r4 = nref[node];
+    int ref = c == 0 ? r4.x : c == 1 ? r4.y : c == 2 ? r4.z : r4.w;
+    const float inf = __int_as_float(0x7f800000);
+    float4 box = make_float4(inf, inf, -inf, -inf);
+    if (ref >= 0) {
+        for (int k = 0; k < 4; k++) box = box_union(box, nbox[4 * ref + k]);
+    } else if (ref != kRefEmpty) {
+        int f = leaf_first(ref), m = leaf_count(ref);
+        for (int k = 0; k < m; k++) box = box_union(box, rects[f + k]);
+    }
+    nbox[4 * node + c] = box;
+}
+
+}  // namespace
+
+void free_tree(TreeBuffers *t) {
+    cudaFree(t->rects);
+    cudaFree(t->ids);
+    cudaFree(t->nbox);
+    cudaFree(t->nref);
+    *t = TreeBuffers();
+}
+
+frw_status build_tree(const float4 *d_rects_in, int32_t n, const double bounds[4], int leaf_max,
+                      cudaStream_t st, TreeBuffers *out, float *build_ms) {
+    *out = TreeBuffers();
+    if (n <= 0 || leaf_max < 1 || leaf_max > kLeafCountMax) {
+        set_error("build_tree: bad size");
+        return FRW_E_ARG;
+    }
+    if ((int64_t)n > (1ll << 26) - 1) {
+        set_error("build_tree: more than 2^26-1 rects");
+        return FRW_E_ARG;
+    }
+    cudaEvent_t e0, e1;
+    FRW_CK(cudaEventCreate(&e0));
+    FRW_CK(cudaEventCreate(&e1));
+    FRW_CK(cudaEventRecord(e0, st));
+
+    const int nblk = (n + kRsTile - 1) / kRsTile;
+    const int cap_nodes = n > 1 ? n : 1;
+    uint32_t *k0 = nullptr, *k1 = nullptr, *hist = nullptr;
+    int32_t *v0 = nullptr, *v1 = nullptr;
+    unsigned long long *cnt = nullptr, *tot = nullptr;
+    int32_t *frb = nullptr;
+    TreeBuffers T;
+    frw_status rc = FRW_OK;
+    auto ck = [&](cudaError_t e, const char *what) {
+        if (e != cudaSuccess && rc == FRW_OK) rc = cuda_fail(e, what);
+        return rc == FRW_OK;
+    };
+    do {
+        if (!ck(cudaMalloc(&k0, (size_t)n * 4), "malloc keys")) break;
+        if (!ck(cudaMalloc(&k1, (size_t)n * 4), "malloc keys")) break;
+        if (!ck(cudaMalloc(&v0, (size_t)n * 4), "malloc vals")) break;
+        if (!ck(cudaMalloc(&v1, (size_t)n * 4), "malloc vals")) break;
+        if (!ck(cudaMalloc(&hist, (size_t)256 * nblk * 4), "malloc hist")) break;
+        if (!ck(cudaMalloc(&cnt, (size_t)cap_nodes * 8), "malloc cnt")) break;
+        if (!ck(cudaMalloc(&tot, 8), "malloc tot")) break;
+        if (!ck(cudaMalloc(&frb, (size_t)cap_nodes * 8 * 4), "malloc frontier")) break;
+        if (!ck(cudaMalloc(&T.rects, (size_t)n * 16), "malloc rects")) break;
+        if (!ck(cudaMalloc(&T.ids, (size_t)n * 4), "malloc ids")) break;
+        if (!ck(cudaMalloc(&T.nbox, (size_t)cap_nodes * 64), "malloc nbox")) break;
+        if (!ck(cudaMalloc(&T.nref, (size_t)cap_nodes * 16), "malloc nref")) break;
+
+        double W = bounds[2] - bounds[0], H = bounds[3] - bounds[1];
+        double sx = W > 0 ? 65536.0 / W : 0.0, sy = H > 0 ? 65536.0 / H : 0.0;
+        k_morton<<<(n + 255) / 256, 256, 0, st>>>(d_rects_in, n, bounds[0], bounds[1], sx, sy, k0, v0);
+        if (!ck(cudaGetLastError(), "k_morton")) break;
+        for (int shift = 0; shift < 32; shift += 8) {
+            k_rs_hist<<<nblk, kRsThreads, 0, st>>>(k0, n, shift, hist, nblk);
+            k_scan_excl<uint32_t><<<1, 1024, 0, st>>>(hist, (int64_t)256 * nblk, nullptr);
+            k_rs_scatter<<<nblk, kRsThreads, 0, st>>>(k0, v0, k1, v1, n, shift, hist, nblk);
+            if (!ck(cudaGetLastError(), "radix sort")) break;
+            std::swap(k0, k1);
+            std::swap(v0, v1);
+        }
+        if (rc) break;
+        k_gather<<<(n + 255) / 256, 256, 0, st>>>(d_rects_in, v0, n, T.rects);
+        if (!ck(cudaMemcpyAsync(T.ids, v0, (size_t)n * 4, cudaMemcpyDeviceToDevice, st), "ids")) break;
+
+        // level-synchronous split
+        Frontier fa{frb, frb + cap_nodes, frb + 2 * cap_nodes, frb + 3 * cap_nodes};
+        Frontier fb{frb + 4 * cap_nodes, frb + 5 * cap_nodes, frb + 6 * cap_nodes, frb + 7 * cap_nodes};
+        int32_t root[4] = {0, 0, 0, n};
+        if (!ck(cudaMemcpyAsync(fa.node, &root[0], 4, cudaMemcpyHostToDevice, st), "root")) break;
+        if (!ck(cudaMemcpyAsync(fa.level, &root[1], 4, cudaMemcpyHostToDevice, st), "root")) break;
+        if (!ck(cudaMemcpyAsync(fa.start, &root[2], 4, cudaMemcpyHostToDevice, st), "root")) break;
+        if (!ck(cudaMemcpyAsync(fa.end, &root[3], 4, cudaMemcpyHostToDevice, st), "root")) break;
+        // a layout of <= leaf_max rects still gets one internal root node
+        int nodes = 1, nfr = 1, depth = 0;
+        std::vector<int> batch = {0, 1};
+        if (n <= leaf_max) {
+            int4 r = make_int4(leaf_ref(0, n), kRefEmpty, kRefEmpty, kRefEmpty);
+            if (!ck(cudaMemcpyAsync(T.nref, &r, 16, cudaMemcpyHostToDevice, st), "root ref")) break;
+            nfr = 0;
+        }
+        for (int iter = 0; nfr > 0; iter++) {
+            if (iter > 64) {
+                set_error("build_tree: too many levels");
+                rc = FRW_E_KERNEL;
+                break;
+            }
+            k_split_count<<<(nfr + 255) / 256, 256, 0, st>>>(k0, fa, nfr, leaf_max, cnt);
+            k_scan_excl<unsigned long long><<<1, 1024, 0, st>>>(cnt, nfr, tot);
+            unsigned long long h_tot = 0;
+            if (!ck(cudaMemcpyAsync(&h_tot, tot, 8, cudaMemcpyDeviceToHost, st), "scan total")) break;
+            if (!ck(cudaStreamSynchronize(st), "split sync")) break;
+            int new_nodes = (int)(h_tot >> 32), next = (int)(h_tot & 0xFFFFFFFFull);
+            k_split_emit<<<(nfr + 255) / 256, 256, 0, st>>>(k0, fa, nfr, leaf_max, cnt, nodes, T.nref, fb);
+            if (!ck(cudaGetLastError(), "split")) break;
+            if (new_nodes > 0) {
+                nodes += new_nodes;
+                batch.push_back(nodes);
+                depth++;
+            }
+            std::swap(fa, fb);
+            nfr = next;
+        }
+        if (rc) break;
+        for (int k = (int)batch.size() - 1; k > 0; k--) {
+            int a = batch[k - 1], b = batch[k];
+            int thr = 4 * (b - a);
+            k_refit<<<(thr + 255) / 256, 256, 0, st>>>(T.rects, T.nref, T.nbox, a, b);
+        }
+        if (!ck(cudaGetLastError(), "refit")) break;
+        T.nodes = nodes;
+        T.depth = depth;
+        T.bytes = (int64_t)n * 20 + (int64_t)nodes * 80;
+        if (!ck(cudaEventRecord(e1, st), "event")) break;
+        if (!ck(cudaEventSynchronize(e1), "build sync")) break;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (build_ms) *build_ms = ms;
+    } while (0);
+    cudaFree(k0);
+    cudaFree(k1);
+    cudaFree(v0);
+    cudaFree(v1);
+    cudaFree(hist);
+    cudaFree(cnt);
+    cudaFree(tot);
+    cudaFree(frb);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != FRW_OK) {
+        free_tree(&T);
+        return rc;
+    }
+    *out = T;
+    return FRW_OK;
+}
+
+}  // namespace frw

@@ -1,0 +1,352 @@
+// walk.cu -- persistent floating-random-walk kernel.
+//
+// Reference: one CUDA thread per walk, one launch per batch
+// (randomWalkCuda, Cuda/randomwalk.cu:64-121) with curand XORWOW, a device-heap
+// traversal stack per thread, a linear CDF scan in global memory and the hit
+// rect written per walk for a host-side std::map histogram
+// (Cuda/getAvgPathLenCUDA.cu:23-48).  Here:
+//   * the grid is persistent (SM count x resident blocks); each warp lane
+//     carries one walk and, when it ends, is refilled from a global walk
+//     counter (one atomic per warp refill), so warps stay full while walks of
+//     very different lengths finish;
+//   * random numbers are counter-based Philox4x32-10 keyed by (seed) with
+//     counter (hop, walk, stream): a walk's trajectory depends only on its
+//     index, never on scheduling, so every walk can be replayed by the CPU
+//     oracle bit-for-bit;
+//   * the Green CDF (201 doubles) and the first-hop weight tables sit in
+//     shared memory; bins are found by binary search (the reference's linear
+//     scan, CPU/mainFunctions.cpp:40-46, returns the same index because the
+//     CDF is strictly increasing);
+//   * each hop is one clearance traversal + scalar replay (query.cuh);
+//   * walk ends are accumulated per (job, conductor) in a per-warp
+//     shared-memory table with Kahan-compensated FP64 sums (single writer per
+//     update), flushed to global FP64 rows when full and at exit.
+#include "query.cuh"
+
+namespace frw {
+namespace {
+
+constexpr int kWalkThreads = 256;
+constexpr int kWarpsPerBlock = kWalkThreads / 32;
+constexpr int kTabSlots = 32;  // per warp
+constexpr unsigned long long kEmptyKey = ~0ull;
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+struct Slot {
+    unsigned long long key, n, hops;
+    double s, cs, s2, cs2;
+};
+
+__device__ __forceinline__ uint4 philox10(uint4 c, uint2 k) {
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        if (r) {
+            k.x += 0x9E3779B9u;
+            k.y += 0xBB67AE85u;
+        }
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+    }
+    return c;
+}
+
+// First uniform of Philox block (hop, walk, stream) under `seed`: 53 bits.
+__device__ __forceinline__ double draw_u(uint64_t seed, uint32_t stream, uint64_t walk, uint32_t hop) {
+    const uint4 o = philox10(make_uint4(hop, (uint32_t)walk, (uint32_t)(walk >> 32), stream),
+                             make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
+    const unsigned long long m = ((unsigned long long)(o.x >> 5) << 26) | (unsigned long long)(o.y >> 6);
+    return (double)m * 0x1p-53;
+}
+
+__device__ __forceinline__ int bin_of(const double *s_intg, double u) {
+    int lo = 0, hi = FRW_NSAMPLE;  // intg[lo] <= u
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        if (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (s_intg[mid] <= u) lo = mid;
+            else hi = mid;
+        }
+    }
+    return lo;
+}
+
+// Uniform point on the Gaussian perimeter, clockwise from the top-left
+// corner; side code 0 top, 1 right, 2 bottom, 3 left (outward normals
+// (0,-1), (1,0), (0,1), (-1,0) in the layout's y-down axes).
+__device__ __forceinline__ int perimeter_point(const double G[4], double u, double &x, double &y) {
+    const double w = __dsub_rn(G[2], G[0]), h = __dsub_rn(G[3], G[1]);
+    const double s = __dmul_rn(u, __dadd_rn(__dmul_rn(2.0, w), __dmul_rn(2.0, h)));
+    if (s < w) {
+        x = __dadd_rn(G[0], s);
+        y = G[1];
+        return 0;
+    }
+    if (s < __dadd_rn(w, h)) {
+        x = G[2];
+        y = __dadd_rn(G[1], __dsub_rn(s, w));
+        return 1;
+    }
+    if (s < __dadd_rn(__dmul_rn(2.0, w), h)) {
+        x = __dsub_rn(G[2], __dsub_rn(__dsub_rn(s, w), h));
+        y = G[3];
+        return 2;
+    }
+    x = G[0];
+    y = __dsub_rn(G[3], __dsub_rn(__dsub_rn(s, __dmul_rn(2.0, w)), h));
+    return 3;
+}
+
+__device__ __forceinline__ void kahan_add(double &s, double &c, double v) {
+    const double y = __dsub_rn(v, c);
+    const double t = __dadd_rn(s, y);
+    c = __dsub_rn(__dsub_rn(t, s), y);
+    s = t;
+}
+
+__device__ __forceinline__ int slot_hash(unsigned long long key) {
+    return (int)((key * 0x9E3779B97F4A7C15ull) >> 59);  // 5 bits
+}
+
+// Single-lane insert; false when the warp table is full.
+__device__ __forceinline__ bool tab_insert(Slot *tab, unsigned long long key, double w, uint32_t hops) {
+    int h = slot_hash(key);
+    for (int probe = 0; probe < kTabSlots; probe++) {
+        Slot &sl = tab[(h + probe) & (kTabSlots - 1)];
+        if (sl.key == key || sl.key == kEmptyKey) {
+            if (sl.key == kEmptyKey) {
+                sl.key = key;
+                sl.n = 0;
+                sl.hops = 0;
+                sl.s = sl.cs = sl.s2 = sl.cs2 = 0.0;
+            }
+            sl.n += 1;
+            sl.hops += hops;
+            kahan_add(sl.s, sl.cs, w);
+            kahan_add(sl.s2, sl.cs2, __dmul_rn(w, w));
+            return true;
+        }
+    }
+    return false;
+}
+
+template <bool kMulti>
+__device__ __forceinline__ const WalkJob &job_of(const WalkParams &P, int j) {
+    return kMulti ? P.jobs[j] : P.job0;
+}
+
+// Whole warp: push every used slot to the global rows, then clear.
+template <bool kMulti>
+__device__ void tab_flush(const WalkParams &P, Slot *tab, int lane) {
+    for (int q = lane; q < kTabSlots; q += 32) {
+        Slot &sl = tab[q];
+        if (sl.key == kEmptyKey) continue;
+        const int job = (int)(sl.key >> 32);
+        const int code = (int)(uint32_t)(sl.key & 0xFFFFFFFFull) - 2;
+        unsigned long long *js = P.job_stats + 4 * job;
+        if (code >= 0) {
+            const int64_t row = job_of<kMulti>(P, job).acc_base + code;
+            atomicAdd(P.acc_n + row, sl.n);
+            atomicAdd(P.acc_s + row, __dsub_rn(sl.s, sl.cs));
+            atomicAdd(P.acc_s2 + row, __dsub_rn(sl.s2, sl.cs2));
+        } else {
+            atomicAdd(js + (code == -1 ? 0 : 1), sl.n);
+        }
+        atomicAdd(js + 2, sl.hops);
+        atomicAdd(js + 3, sl.n);
+        sl.key = kEmptyKey;
+    }
+    __syncwarp();
+}
+
+template <bool kMulti>
+__global__ void __launch_bounds__(kWalkThreads) k_walk(const WalkParams P) {
+    __shared__ double s_intg[FRW_NSAMPLE + 1];
+    __shared__ double s_wx[FRW_NSAMPLE], s_wy[FRW_NSAMPLE];
+    __shared__ Slot s_tab[kWarpsPerBlock][kTabSlots];
+
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i <= FRW_NSAMPLE; i += blockDim.x) s_intg[i] = P.intg[i];
+    for (int i = threadIdx.x; i < FRW_NSAMPLE; i += blockDim.x) {
+        s_wx[i] = P.wx[i];
+        s_wy[i] = P.wy[i];
+    }
+    Slot *tab = s_tab[wib];
+    for (int q = lane; q < kTabSlots; q += 32) tab[q].key = kEmptyKey;
+    __syncthreads();
+
+    const uint32_t lt = (1u << lane) - 1u;
+    const int refill_min = P.refill_min < 1 ? 1 : (P.refill_min > 32 ? 32 : P.refill_min);
+    const bool uniform_start = P.start_mode == FRW_START_UNIFORM;
+    const bool exact = P.exact_perimeter != 0;
+
+    bool active = false, exhausted = false;
+    int job = 0;
+    uint64_t gw = 0, pw = 0;
+    uint32_t hop = 0, stream = 0;
+    int32_t hops = 0, bin1 = -1;
+    int side = 0;
+    double px = 0, py = 0, a0 = 0, perim = 0;
+    double sq[4] = {0, 0, 0, 0};
+    uint32_t st = 0;
+
+    for (;;) {
+        // ---- refill idle lanes from the global walk counter ----
+        const unsigned idle = __ballot_sync(kFull, !active);
+        if (!exhausted && __popc(idle) >= refill_min) {
+            const int cnt = __popc(idle), leader = __ffs(idle) - 1;
+            unsigned long long base = 0;
+            if (lane == leader) base = atomicAdd(P.counter, (unsigned long long)cnt);
+            base = __shfl_sync(kFull, base, leader);
+            if (base + cnt >= P.total_walks) exhausted = true;
+            if (!active) {
+                gw = base + __popc(idle & lt);
+                if (gw < P.total_walks) {
+                    if (kMulti) {
+                        int lo = 0, hi = P.njobs;  // last job with walk_begin <= gw
+                        while (hi - lo > 1) {
+                            const int mid = (lo + hi) >> 1;
+                            if (P.jobs[mid].walk_begin <= gw) lo = mid;
+                            else hi = mid;
+                        }
+                        job = lo;
+                    }
+                    const WalkJob &J = job_of<kMulti>(P, job);
+                    const double4 g4 = P.gauss[job];
+                    const double G[4] = {g4.x, g4.y, g4.z, g4.w};
+                    perim = __dadd_rn(__dmul_rn(2.0, __dsub_rn(G[2], G[0])), __dmul_rn(2.0, __dsub_rn(G[3], G[1])));
+                    pw = J.first_walk + (gw - J.walk_begin);
+                    stream = J.stream_id;
+                    hop = 0;
+                    hops = 0;
+                    bin1 = -1;
+                    a0 = 0.0;
+                    const double u = draw_u(P.seed, stream, pw, 0);
+                    if (uniform_start) {
+                        side = perimeter_point(G, u, px, py);
+                    } else {
+                        point_from_index(G, bin_of(s_intg, u), exact, px, py);
+                    }
+                    active = true;
+                }
+            }
+        }
+        if (!__any_sync(kFull, active)) {
+            if (exhausted) break;
+            continue;
+        }
+
+        // ---- one hop of every active walk ----
+        int code = 0x7FFFFFFF;  // != ended
+        if (active) {
+            const WalkJob &J = job_of<kMulti>(P, job);
+            const DevLayout &L = J.L;
+            if (!(px > L.bx0 && py > L.by0 && px < L.bx1 && py < L.by1)) {
+                code = -1;  // escaped: left the layer bounds
+            } else {
+                int hit;
+                st |= query_point(L, px, py, sq, hit);
+                hops++;
+                if (hit != kNoHit) code = hit;
+                else if (hops >= P.hop_cap) code = -2;
+                else {
+                    hop++;
+                    const int bin = bin_of(s_intg, draw_u(P.seed, stream, pw, hop));
+                    if (hop == 1) {
+                        bin1 = bin;
+                        a0 = __dsub_rn(sq[2], sq[0]);
+                    }
+                    point_from_index(sq, bin, exact, px, py);
+                }
+            }
+        }
+        const bool ended = active && code != 0x7FFFFFFF;
+
+        // ---- walk ends: weight, optional record, per-warp table ----
+        double wgt = 0.0;
+        if (ended) {
+            if (uniform_start && code >= 0 && bin1 >= 0) {
+                const double nx = side == 1 ? 1.0 : (side == 3 ? -1.0 : 0.0);
+                const double ny = side == 2 ? 1.0 : (side == 0 ? -1.0 : 0.0);
+                const double dot = __dadd_rn(__dmul_rn(s_wx[bin1], nx), __dmul_rn(s_wy[bin1], ny));
+                wgt = __ddiv_rn(__dmul_rn(__dmul_rn(-P.permittivity, perim), dot), a0);
+            }
+            if (P.rec_end) {
+                P.rec_end[gw] = code;
+                P.rec_hops[gw] = hops;
+                P.rec_bin[gw] = bin1;
+                P.rec_w[gw] = wgt;
+            }
+            active = false;
+        }
+        unsigned em = __ballot_sync(kFull, ended);
+        while (em) {
+            const int l = __ffs(em) - 1;
+            bool ok = true;
+            if (lane == l)
+                ok = tab_insert(tab, ((unsigned long long)job << 32) | (uint32_t)(code + 2), wgt, (uint32_t)hops);
+            __syncwarp();
+            if (!__shfl_sync(kFull, ok, l)) {
+                tab_flush<kMulti>(P, tab, lane);
+                continue;  // retry lane l on the empty table
+            }
+            em &= em - 1;
+        }
+    }
+    tab_flush<kMulti>(P, tab, lane);
+    if (st) atomicOr(P.status, st);
+}
+
+__global__ void k_compact(const unsigned long long *__restrict__ acc_n, const double *__restrict__ acc_s,
+                          const double *__restrict__ acc_s2, int64_t rows, int64_t *__restrict__ out_row,
+                          unsigned long long *__restrict__ out_n, double *__restrict__ out_s,
+                          double *__restrict__ out_s2, unsigned long long *count) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool keep = i < rows && acc_n[i] > 0;
+    const unsigned m = __ballot_sync(kFull, keep);
+    if (!m) return;
+    const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(count, (unsigned long long)__popc(m));
+    base = __shfl_sync(kFull, base, leader);
+    if (keep) {
+        const unsigned long long o = base + __popc(m & ((1u << lane) - 1u));
+        out_row[o] = i;
+        out_n[o] = acc_n[i];
+        out_s[o] = acc_s[i];
+        out_s2[o] = acc_s2[i];
+    }
+}
+
+}  // namespace
+
+int walk_max_blocks_per_sm(int threads, bool multi) {
+    int b = 0;
+    if (multi) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<true>, threads, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<false>, threads, 0);
+    return b;
+}
+
+frw_status launch_walk(const WalkParams &P, int threads, int blocks, cudaStream_t stream) {
+    if (threads != kWalkThreads) {
+        set_error("launch_walk: threads per block must be 256");
+        return FRW_E_ARG;
+    }
+    if (P.njobs > 1) k_walk<true><<<blocks, threads, 0, stream>>>(P);
+    else k_walk<false><<<blocks, threads, 0, stream>>>(P);
+    FRW_CK(cudaGetLastError());
+    return FRW_OK;
+}
+
+frw_status launch_compact(const unsigned long long *acc_n, const double *acc_s, const double *acc_s2,
+                          int64_t rows, int64_t *out_row, unsigned long long *out_n, double *out_s,
+                          double *out_s2, unsigned long long *d_count, cudaStream_t stream) {
+    if (rows <= 0) return FRW_OK;
+    k_compact<<<(unsigned)((rows + 255) / 256), 256, 0, stream>>>(acc_n, acc_s, acc_s2, rows, out_row, out_n,
+                                                                  out_s, out_s2, d_count);
+    FRW_CK(cudaGetLastError());
+    return FRW_OK;
+}
+
+}  // namespace frw

@@ -1,0 +1,354 @@
+"""Python mirror of the FRW C ABI (include/frw.h) over lib/libfrw.so.
+
+The compute path is the CUDA library only: importing this module loads
+``lib/libfrw.so`` (built in-tree by ``make -C engineer-thesis_b200``) and every
+compute call raises :class:`FrwError` when no sm_100 device is usable.  There
+is no CPU fallback.
+
+Names follow the reference (piogrzej/engineer-thesis, randomWalk/):
+
+* :class:`Layout` -- ``createQuadTree`` / ``freeQuadTreeManager``
+  (Cuda/mainkernels.h:10,13) plus the layout reader (CPU/Parser.cpp).
+* :meth:`Layout.draw_biggest_square` / :meth:`Layout.check_collisions_point`
+  -- ``drawBiggestSquareAtPoint`` / ``checkCollisons(point)``, batched.
+* :meth:`Layout.check_collisions` -- ``checkCollisions(rect, ignore)``.
+* :meth:`Layout.gauss_surface` -- ``creatGaussianSurfFrom``.
+* :meth:`Layout.walk` -- the estimator of ``getAvgPathLen(CUDA)``.
+* :meth:`Layout.walk_trace` -- ``randomWalkCudaWrapper``'s per-walk outputs.
+* :func:`get_avg_path_len_cuda` -- ``getAvgPathLenCUDA``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG, "lib", "libfrw.so")
+HEADER = os.path.join(os.path.dirname(PKG), "include", "frw.h")
+
+OK, E_ARG, E_IO, E_CUDA, E_OOM, E_HOPCAP, E_TIMEOUT, E_DEVICE, E_KERNEL = 0, -1, -2, -3, -4, -5, -6, -7, -8
+NSAMPLE = 200
+MEM_HOST, MEM_DEVICE = 0, 1
+GAUSS_SCALE, GAUSS_OFFSET = 0, 1
+START_GREEN, START_UNIFORM = 0, 1
+END_ESCAPED, END_ABORTED = -1, -2
+PERMITTIVITY = 8.854187817620e-12
+
+
+class FrwError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"frw status {status}: {msg}")
+        self.status = status
+
+
+class Opts(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_uint32),
+        ("gauss_mode", C.c_int32),
+        ("gauss_param", C.c_double),
+        ("start_mode", C.c_int32),
+        ("exact_perimeter", C.c_int32),
+        ("hop_cap", C.c_int64),
+        ("permittivity", C.c_double),
+        ("stream_id", C.c_uint32),
+        ("threads_per_block", C.c_int32),
+        ("blocks_per_sm", C.c_int32),
+        ("refill_min", C.c_int32),
+    ]
+
+
+class Result(C.Structure):
+    _fields_ = [
+        ("walks", C.c_uint64),
+        ("escaped", C.c_uint64),
+        ("aborted", C.c_uint64),
+        ("hops_total", C.c_uint64),
+        ("gauss", C.c_double * 4),
+        ("fraction_other", C.c_double),
+        ("kernel_ms", C.c_double),
+        ("capacity", C.c_int64),
+        ("n_entries", C.c_int64),
+        ("conductor", C.POINTER(C.c_int64)),
+        ("hits", C.POINTER(C.c_uint64)),
+        ("cap", C.POINTER(C.c_double)),
+        ("cap_se", C.POINTER(C.c_double)),
+    ]
+
+
+class LayoutInfo(C.Structure):
+    _fields_ = [
+        ("n_rects", C.c_int64),
+        ("n_nodes", C.c_int64),
+        ("depth", C.c_int32),
+        ("leaf_max", C.c_int32),
+        ("bounds", C.c_double * 4),
+        ("device_bytes", C.c_int64),
+        ("device", C.c_int32),
+        ("build_ms", C.c_double),
+    ]
+
+
+_D = C.POINTER(C.c_double)
+_F = C.POINTER(C.c_float)
+_I64 = C.POINTER(C.c_int64)
+_I32 = C.POINTER(C.c_int32)
+_U8 = C.POINTER(C.c_uint8)
+_VP = C.c_void_p
+
+_SIGS = {
+    "frw_version": ([], C.c_char_p),
+    "frw_last_error": ([], C.c_char_p),
+    "frw_device_check": ([C.c_int], C.c_int),
+    "frw_green_table": ([_D, _D], C.c_int),
+    "frw_layout_from_file": ([C.c_char_p, C.c_int, C.c_int, C.POINTER(_VP)], C.c_int),
+    "frw_layout_create": ([_F, C.c_int64, _D, C.c_int, _VP, C.POINTER(_VP)], C.c_int),
+    "frw_layout_destroy": ([_VP], C.c_int),
+    "frw_layout_info_get": ([_VP, C.POINTER(LayoutInfo)], C.c_int),
+    "frw_layout_rects": ([_VP, _D], C.c_int),
+    "frw_query_batch": ([_VP, _VP, C.c_int64, _VP, _VP, C.c_int, _VP], C.c_int),
+    "frw_box_collides_batch": ([_VP, _VP, C.c_int64, _D, _VP, C.c_int, _VP], C.c_int),
+    "frw_opts_default": ([C.POINTER(Opts)], None),
+    "frw_walk": ([_VP, C.c_int64, C.c_uint64, C.c_uint64, C.POINTER(Opts), C.POINTER(Result), _VP], C.c_int),
+    "frw_walk_trace": ([_VP, C.c_int64, C.c_uint64, C.c_uint64, C.c_uint64, C.POINTER(Opts), _VP, _VP, _VP,
+                        _VP, C.c_int, _VP], C.c_int),
+    "frw_gauss_surface": ([_VP, C.c_int64, C.POINTER(Opts), _D, _VP], C.c_int),
+    "frw_avg_path_len": ([C.c_char_p, C.c_int64, C.c_int64, C.c_int, C.c_uint64, C.c_int, C.c_char_p, _D],
+                         C.c_int),
+    "frw_generate_layout": ([C.c_uint64, C.c_int64, C.c_double, C.c_int32, C.c_int32, C.c_double, _F], C.c_int),
+    "frw_write_layout": ([C.c_char_p, _F, C.c_int64, C.c_char_p], C.c_int),
+}
+
+_lib = None
+
+
+def lib():
+    """Load lib/libfrw.so; raises ImportError when it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} missing: build it with `make -C {PKG}`")
+        L = C.CDLL(LIB_PATH)
+        for name, (args, res) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def _check(st: int):
+    if st != OK:
+        raise FrwError(st, lib().frw_last_error().decode(errors="replace"))
+
+
+def _ptr(a, t=_VP):
+    return None if a is None else C.cast(a.ctypes.data, t)
+
+
+def version() -> str:
+    return lib().frw_version().decode()
+
+
+def device_check(device: int = 0) -> None:
+    _check(lib().frw_device_check(device))
+
+
+def green_table():
+    """(g[200], intg[201]) -- precompute_unit_square_green's g and intg."""
+    g = np.zeros(NSAMPLE)
+    intg = np.zeros(NSAMPLE + 1)
+    _check(lib().frw_green_table(_ptr(g, _D), _ptr(intg, _D)))
+    return g, intg
+
+
+def opts(gauss_mode=GAUSS_SCALE, gauss_param=1.5, start_mode=START_GREEN, exact_perimeter=False,
+         hop_cap=100000, stream_id=0, blocks_per_sm=0, refill_min=1, permittivity=PERMITTIVITY) -> Opts:
+    o = Opts()
+    lib().frw_opts_default(C.byref(o))
+    o.gauss_mode = gauss_mode
+    o.gauss_param = gauss_param
+    o.start_mode = start_mode
+    o.exact_perimeter = int(exact_perimeter)
+    o.hop_cap = hop_cap
+    o.stream_id = stream_id
+    o.blocks_per_sm = blocks_per_sm
+    o.refill_min = refill_min
+    o.permittivity = permittivity
+    return o
+
+
+def capacitance_opts(offset=1.0, **kw) -> Opts:
+    """Uniform start on the target grown by `offset`: capacitance weights on."""
+    return opts(gauss_mode=GAUSS_OFFSET, gauss_param=offset, start_mode=START_UNIFORM, **kw)
+
+
+def generate_layout(seed: int, n: int, domain: float, wmin: int = 5, wmax: int = 50, gap: float = 2.0):
+    out = np.zeros((n, 4), dtype=np.float32)
+    _check(lib().frw_generate_layout(seed, n, domain, wmin, wmax, gap, _ptr(out, _F)))
+    return out
+
+
+def write_layout(path: str, rects, name: str = "layer") -> None:
+    r = np.ascontiguousarray(rects, dtype=np.float32)
+    _check(lib().frw_write_layout(path.encode(), _ptr(r, _F), len(r), name.encode()))
+
+
+@dataclass
+class WalkResult:
+    walks: int
+    escaped: int
+    aborted: int
+    hops_total: int
+    gauss: np.ndarray
+    fraction_other: float
+    kernel_ms: float
+    conductor: np.ndarray
+    hits: np.ndarray
+    cap: np.ndarray
+    cap_se: np.ndarray
+    extra: dict = field(default_factory=dict)
+
+    def row(self, k: int):
+        i = np.searchsorted(self.conductor, k)
+        if i < len(self.conductor) and self.conductor[i] == k:
+            return self.hits[i], self.cap[i], self.cap_se[i]
+        return 0, 0.0, 0.0
+
+
+class Layout:
+    """A device-resident layout with its Morton quadtree."""
+
+    def __init__(self, handle, n: int):
+        self._h = handle
+        self.n = n
+
+    @classmethod
+    def from_file(cls, path: str, layer: int = 0, device: int = 0) -> "Layout":
+        h = _VP()
+        _check(lib().frw_layout_from_file(path.encode(), layer, device, C.byref(h)))
+        info = LayoutInfo()
+        _check(lib().frw_layout_info_get(h, C.byref(info)))
+        return cls(h, info.n_rects)
+
+    @classmethod
+    def from_rects(cls, rects, bounds=None, device: int = 0, stream: int = 0) -> "Layout":
+        r = np.ascontiguousarray(rects, dtype=np.float32)
+        if r.ndim != 2 or r.shape[1] != 4:
+            raise ValueError("rects must be (n, 4)")
+        b = None if bounds is None else np.ascontiguousarray(bounds, dtype=np.float64)
+        h = _VP()
+        _check(lib().frw_layout_create(_ptr(r, _F), len(r), _ptr(b, _D), device, stream or None, C.byref(h)))
+        return cls(h, len(r))
+
+    def close(self):
+        if self._h:
+            lib().frw_layout_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def info(self) -> LayoutInfo:
+        info = LayoutInfo()
+        _check(lib().frw_layout_info_get(self._h, C.byref(info)))
+        return info
+
+    @property
+    def bounds(self) -> np.ndarray:
+        return np.array(self.info.bounds[:])
+
+    def rects(self) -> np.ndarray:
+        out = np.zeros((self.n, 4))
+        _check(lib().frw_layout_rects(self._h, _ptr(out, _D)))
+        return out
+
+    # ---- queries
+    def query(self, pts):
+        """drawBiggestSquareAtPoint + checkCollisons(point) for (n,2) points."""
+        p = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 2)
+        sq = np.zeros((len(p), 4))
+        hit = np.zeros(len(p), dtype=np.int64)
+        _check(lib().frw_query_batch(self._h, _ptr(p), len(p), _ptr(sq), _ptr(hit), MEM_HOST, None))
+        return sq, hit
+
+    def query_device(self, pts_t, sq_t, hit_t, stream: int = 0):
+        """Device-resident variant on torch CUDA tensors (no host copies)."""
+        _check(lib().frw_query_batch(self._h, C.c_void_p(pts_t.data_ptr()), pts_t.shape[0],
+                                     C.c_void_p(sq_t.data_ptr()), C.c_void_p(hit_t.data_ptr()), MEM_DEVICE,
+                                     stream or None))
+
+    def draw_biggest_square(self, pts):
+        return self.query(pts)[0]
+
+    def check_collisions_point(self, pts):
+        return self.query(pts)[1]
+
+    def check_collisions(self, boxes, ignore=None):
+        b = np.ascontiguousarray(boxes, dtype=np.float64).reshape(-1, 4)
+        ig = None if ignore is None else np.ascontiguousarray(ignore, dtype=np.float64)
+        out = np.zeros(len(b), dtype=np.uint8)
+        _check(lib().frw_box_collides_batch(self._h, _ptr(b), len(b), _ptr(ig, _D), _ptr(out), MEM_HOST, None))
+        return out.astype(bool)
+
+    def gauss_surface(self, target: int, o: Opts | None = None):
+        out = np.zeros(4)
+        _check(lib().frw_gauss_surface(self._h, target, C.byref(o) if o else None, _ptr(out, _D), None))
+        return out
+
+    # ---- walks
+    def walk(self, target: int, walks: int, seed: int, o: Opts | None = None, capacity: int | None = None,
+             stream: int = 0) -> WalkResult:
+        cap = self.n if capacity is None else capacity
+        cond = np.zeros(cap, dtype=np.int64)
+        hits = np.zeros(cap, dtype=np.uint64)
+        c = np.zeros(cap)
+        se = np.zeros(cap)
+        r = Result()
+        r.capacity = cap
+        r.conductor = _ptr(cond, _I64)
+        r.hits = _ptr(hits, C.POINTER(C.c_uint64))
+        r.cap = _ptr(c, _D)
+        r.cap_se = _ptr(se, _D)
+        _check(lib().frw_walk(self._h, target, walks, seed, C.byref(o) if o else None, C.byref(r), stream or None))
+        m = min(r.n_entries, cap)
+        return WalkResult(r.walks, r.escaped, r.aborted, r.hops_total, np.array(r.gauss[:]), r.fraction_other,
+                          r.kernel_ms, cond[:m], hits[:m], c[:m], se[:m])
+
+    def walk_trace(self, target: int, first: int, walks: int, seed: int, o: Opts | None = None):
+        end = np.zeros(walks, dtype=np.int64)
+        hops = np.zeros(walks, dtype=np.int32)
+        b1 = np.zeros(walks, dtype=np.int32)
+        w = np.zeros(walks)
+        _check(lib().frw_walk_trace(self._h, target, first, walks, seed, C.byref(o) if o else None, _ptr(end),
+                                    _ptr(hops), _ptr(b1), _ptr(w), MEM_HOST, None))
+        return end, hops, b1, w
+
+
+def get_avg_path_len_cuda(path: str, iter_num: int, rect_id: int, layer: int = 0, seed: int = 0, device: int = 0,
+                          hist_path: str | None = None) -> float:
+    """getAvgPathLenCUDA: fraction of walks that did not end on rect_id."""
+    out = C.c_double()
+    _check(lib().frw_avg_path_len(path.encode(), iter_num, rect_id, layer, seed, device,
+                                  hist_path.encode() if hist_path else None, C.byref(out)))
+    return out.value
+
+
+def header_symbols(header: str = HEADER):
+    """Function names declared in include/frw.h."""
+    import re
+
+    txt = open(header).read()
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?[a-z_0-9]+\s*\*?\s*(frw_[a-z_0-9]+)\s*\(", txt, re.M)))

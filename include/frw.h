@@ -1,0 +1,207 @@
+/*
+ * frw.h -- C ABI of the B200 floating-random-walk (FRW) capacitance extractor.
+ *
+ * Plain C types only (no CUDA or torch types): streams are passed as void*
+ * (a cudaStream_t, NULL = the legacy default stream).  Every call returns an
+ * frw_status; on failure frw_last_error() returns a thread-local message.
+ * Nothing in the library calls exit(), cudaDeviceReset() or falls back to the
+ * CPU: without an sm_100 device every compute entry point fails with
+ * FRW_E_DEVICE.
+ *
+ * Correspondence with the reference (piogrzej/engineer-thesis, randomWalk/):
+ *   frw_layout_from_file / frw_layout_create   <- createQuadTree
+ *       (Cuda/mainkernels.h:10, Cuda/createquadtree.cu:16-87) and the layout
+ *       reader d_Parser/Parser (Cuda/d_parser.cpp:16-130, CPU/Parser.cpp:15-125)
+ *   frw_layout_destroy                         <- freeQuadTreeManager
+ *       (Cuda/mainkernels.h:13, Cuda/freequadtreemanager.cu:3-11)
+ *   frw_query_batch                            <- d_QuadTree::drawBiggestSquareAtPoint
+ *       + d_QuadTree::checkCollisons(point) (Cuda/d_quadTree.cu:86-134,28-69;
+ *       CPU twins CPU/quadTree.cpp:264-312,240-262), batched
+ *   frw_box_collides_batch                     <- Tree::checkCollisions(rect, ignore)
+ *       (CPU/quadTree.cpp:148-198, Cuda/d_quadTree.cu:136-193), batched
+ *   frw_gauss_surface                          <- Tree::creatGaussianSurfFrom
+ *       (CPU/quadTree.cpp:315-364, Cuda/d_quadTree.cu:216-265)
+ *   frw_walk_trace                             <- randomWalkCudaWrapper
+ *       (Cuda/mainkernels.h:9, Cuda/randomwalk.cu:123-134): per-walk outputs
+ *   frw_walk                                   <- the estimator of
+ *       getAvgPathLenCUDA / getAvgPathLen (Cuda/getAvgPathLenCUDA.cu:50-80,
+ *       CPU/getAvgPathLen.cpp:35-114): per-conductor hits and capacitance row
+ *   frw_avg_path_len                           <- getAvgPathLenCUDA
+ *       (Cuda/mainkernels.h:14): the reference's one-call entry point
+ *   frw_green_table                            <- precompute_unit_square_green
+ *       (green/green.h:50, green/green.cpp:125-152)
+ *   frw_device_check                           <- initCuda (Cuda/initCuda.cu:9-33)
+ */
+#ifndef FRW_H
+#define FRW_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int frw_status;
+#define FRW_OK 0
+#define FRW_E_ARG (-1)      /* invalid argument or layout */
+#define FRW_E_IO (-2)       /* unreadable or malformed layout file */
+#define FRW_E_CUDA (-3)     /* a CUDA runtime call failed */
+#define FRW_E_OOM (-4)      /* device or host allocation failed */
+#define FRW_E_HOPCAP (-5)   /* reserved: walks hit the hop cap (reported as counts, not failure) */
+#define FRW_E_TIMEOUT (-6)  /* a bounded host wait expired */
+#define FRW_E_DEVICE (-7)   /* no usable sm_100 device */
+#define FRW_E_KERNEL (-8)   /* a kernel reported an internal limit (see frw_last_error) */
+
+typedef struct frw_layout frw_layout;
+
+#define FRW_NSAMPLE 200 /* perimeter bins of the Green's-function table (defines.h:28) */
+
+/* ---- diagnostics ---- */
+const char *frw_version(void);
+const char *frw_last_error(void);
+/* Checks that `device` exists and is compute capability 10.x (replaces the
+ * reference's SM >= 3.5 dynamic-parallelism check, Cuda/initCuda.cu:14-31). */
+frw_status frw_device_check(int device);
+
+/* ---- Green's function table ---- */
+/* g[FRW_NSAMPLE] and the normalised cumulative intg[FRW_NSAMPLE+1] of the
+ * unit-square surface Green's function seen from the centre; bit-identical to
+ * the reference's precompute_unit_square_green.  Either pointer may be NULL. */
+frw_status frw_green_table(double *g, double *intg);
+
+/* ---- layouts ---- */
+/* Reads layer `layer` of a reference layout file (lines "rect x0 y0 x1 y1";
+ * layers closed by "<<" lines, the first one skipped; CPU/Parser.cpp:15-50),
+ * computes the reference bounds (bbox grown by int(0.01*width) on both axes,
+ * CPU/Parser.cpp:51-87) and builds the device quadtree on `device`. */
+frw_status frw_layout_from_file(const char *path, int layer, int device, frw_layout **out);
+/* rects_xyxy: host array of n*4 floats (x0,y0,x1,y1), y downwards; every
+ * coordinate must be an integer-or-float value exactly representable in
+ * FP32 with |c| < 2^24.  bounds: NULL for the reference rule, else 4
+ * doubles that must contain every rect.  The build runs on `stream` and the
+ * call returns when the layout is ready. */
+frw_status frw_layout_create(const float *rects_xyxy, int64_t n, const double *bounds, int device,
+                             void *stream, frw_layout **out);
+frw_status frw_layout_destroy(frw_layout *layout);
+
+typedef struct frw_layout_info {
+    int64_t n_rects;
+    int64_t n_nodes;       /* internal quadtree nodes */
+    int32_t depth;         /* levels below the root */
+    int32_t leaf_max;      /* rects per leaf */
+    double bounds[4];      /* x0, y0, x1, y1 */
+    int64_t device_bytes;  /* rects + ids + nodes */
+    int32_t device;
+    double build_ms;       /* device time of the last tree build */
+} frw_layout_info;
+frw_status frw_layout_info_get(const frw_layout *layout, frw_layout_info *info);
+/* Copies the layout's rects (layer order, as doubles) to a host array n*4. */
+frw_status frw_layout_rects(const frw_layout *layout, double *out_xyxy);
+
+/* ---- memory location flag for batch calls ---- */
+#define FRW_MEM_HOST 0   /* pointers are host memory (copied through the stream) */
+#define FRW_MEM_DEVICE 1 /* pointers are device memory on the layout's device */
+
+/* ---- collision queries ---- */
+/* For each point: the reference's maximal empty square at the point
+ * (drawBiggestSquareAtPoint: p+-1, p+-2, then expand/bisect from
+ * 0.05*max(W,H) down to 0.095) and the conductor containing it (closed; the
+ * lowest layer index when several do; -1 when none).  Complete semantics:
+ * a box collides when it leaves the layer bounds or touches ANY rect.
+ * Results are bit-identical to the FP64 CPU reference algorithm. */
+frw_status frw_query_batch(const frw_layout *layout, const double *pts_xy, int64_t n,
+                           double *sq_xyxy_out, int64_t *hit_out, int mem, void *stream);
+/* Tree::checkCollisions(box, ignore) per box: 1 when the box leaves the
+ * layer bounds or touches a rect other than one equal to *ignore
+ * (coordinate-wise; ignore may be NULL, host memory). */
+frw_status frw_box_collides_batch(const frw_layout *layout, const double *boxes_xyxy, int64_t n,
+                                  const double *ignore, uint8_t *out, int mem, void *stream);
+
+/* ---- walks ---- */
+#define FRW_GAUSS_SCALE 0   /* reference creatGaussianSurfFrom(target, param) (default 1.5) */
+#define FRW_GAUSS_OFFSET 1  /* target grown by param on every side */
+#define FRW_START_GREEN 0   /* reference start: Green CDF mapped on the Gaussian rectangle */
+#define FRW_START_UNIFORM 1 /* uniform on the Gaussian perimeter; enables capacitance weights */
+
+typedef struct frw_opts {
+    uint32_t struct_size;    /* sizeof(frw_opts) */
+    int32_t gauss_mode;      /* FRW_GAUSS_* */
+    double gauss_param;      /* 1.5 (scale) or the offset */
+    int32_t start_mode;      /* FRW_START_* */
+    int32_t exact_perimeter; /* 0: perimeter truncated to int as the CPU reference
+                                (rectHost.cpp:102-105); 1: as the GPU reference (d_Rect.cu:29-32) */
+    int64_t hop_cap;         /* walks longer than this end as "aborted" */
+    double permittivity;     /* F/m, default 8.854187817620e-12 (green/phys.h:18) */
+    uint32_t stream_id;      /* Philox counter word 3: independent streams under one seed */
+    /* launch tuning (0 = library choice / autotuned) */
+    int32_t threads_per_block;
+    int32_t blocks_per_sm;
+    int32_t refill_min;      /* refill a warp only when at least this many lanes are idle */
+} frw_opts;
+void frw_opts_default(frw_opts *opts);
+
+typedef struct frw_result {
+    /* scalar outputs */
+    uint64_t walks;
+    uint64_t escaped;          /* left the layer bounds (potential 0) */
+    uint64_t aborted;          /* reached hop_cap */
+    uint64_t hops_total;       /* collision queries issued */
+    double gauss[4];           /* Gaussian surface used */
+    double fraction_other;     /* walks NOT ending on the target, escapes included:
+                                  the value getAvgPathLen(CUDA) returns */
+    double kernel_ms;          /* device time of the walk kernel */
+    /* per-conductor rows, sorted by conductor index (caller-owned, host) */
+    int64_t capacity;          /* length of the arrays below */
+    int64_t n_entries;         /* conductors reached (may exceed capacity: rows truncated) */
+    int64_t *conductor;        /* layer index */
+    uint64_t *hits;            /* walks ending on it */
+    double *cap;               /* capacitance C_t,k in F/m (uniform start; 0 otherwise) */
+    double *cap_se;            /* its standard error */
+} frw_result;
+
+/* Runs `walks` walks from the Gaussian surface of conductor `target`
+ * (layer index) with Philox stream (seed, opts->stream_id).  Walk i's random
+ * numbers depend only on (seed, stream_id, i, hop), so results do not depend
+ * on launch configuration. */
+frw_status frw_walk(const frw_layout *layout, int64_t target, uint64_t walks, uint64_t seed,
+                    const frw_opts *opts, frw_result *result, void *stream);
+
+/* Same walks with per-walk records (device or host arrays of `walks`
+ * entries; any may be NULL): end conductor (layer index, -1 escaped,
+ * -2 aborted), hop count, first-hop bin and capacitance weight.  The
+ * reference's randomWalkCudaWrapper output pair (0/1 "other" flag and hit
+ * rect) is derived from `end`. */
+frw_status frw_walk_trace(const frw_layout *layout, int64_t target, uint64_t first_walk,
+                          uint64_t walks, uint64_t seed, const frw_opts *opts, int64_t *end,
+                          int32_t *hops, int32_t *bin1, double *weight, int mem, void *stream);
+
+/* Gaussian surface of `target` under opts (scale mode runs the reference's
+ * bisection on the device). */
+frw_status frw_gauss_surface(const frw_layout *layout, int64_t target, const frw_opts *opts,
+                             double out_xyxy[4], void *stream);
+
+/* The reference's one-call entry point getAvgPathLenCUDA(path, ITER_NUM,
+ * RECT_ID, measure, layer): parse, build, run iter_num walks from rect_id
+ * (reference start and Gaussian surface) and return the fraction of walks
+ * that did not end on rect_id.  The per-rect histogram is written to
+ * hist_path in the reference's "<ts>wyniki.txt" format when not NULL. */
+frw_status frw_avg_path_len(const char *path, int64_t iter_num, int64_t rect_id, int layer,
+                            uint64_t seed, int device, const char *hist_path, double *fraction);
+
+/* ---- synthetic layouts ---- */
+/* Seeded generator of the benchmark layouts: n rects with integer corners in
+ * [0, domain]^2, width and height uniform integers in [wmin, wmax], rejected
+ * unless their L-infinity gap to every earlier rect is >= gap (splitmix64
+ * stream from `seed`).  Writes n*4 floats; returns FRW_E_ARG when the domain
+ * cannot hold n rects within 64*n attempts. */
+frw_status frw_generate_layout(uint64_t seed, int64_t n, double domain, int32_t wmin,
+                               int32_t wmax, double gap, float *out_xyxy);
+/* Writes rects as a reference layout file (one layer). */
+frw_status frw_write_layout(const char *path, const float *rects_xyxy, int64_t n,
+                            const char *layer_name);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FRW_H */

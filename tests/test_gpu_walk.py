@@ -1,0 +1,125 @@
+"""Walks on the device vs the CPU oracle: every walk's end conductor, hop
+count, first-hop bin and capacitance weight bit-identical on the same Philox
+stream, and the estimator rows equal to the oracle's sums."""
+import numpy as np
+import pytest
+
+import frw
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle_cfg(G, o: frw.Opts, target, seed):
+    return G.walk_cfg(target=target, gauss_mode=o.gauss_mode, gauss_param=o.gauss_param,
+                      start_mode=o.start_mode, exact_perimeter=bool(o.exact_perimeter), hop_cap=o.hop_cap,
+                      seed=seed, stream=o.stream_id)
+
+
+CASES = [
+    ("test2", 10, dict()),  # reference start and surface
+    ("test2", 10, dict(gauss_mode=frw.GAUSS_OFFSET, gauss_param=1.0, start_mode=frw.START_UNIFORM)),
+    ("test", 3, dict(exact_perimeter=True)),
+    ("test100", 7, dict(start_mode=frw.START_UNIFORM)),
+    ("test1000", 500, dict()),
+    ("test1000", 17, dict(gauss_mode=frw.GAUSS_OFFSET, gauss_param=1.0, start_mode=frw.START_UNIFORM,
+                          stream_id=3)),
+]
+
+
+@pytest.mark.parametrize("name,target,kw", CASES)
+def test_walk_records_bit_exact(golden, name, target, kw):
+    gd = golden(name)
+    o = frw.opts(**kw)
+    G = O.Grid(gd["rects"], gd["bounds"])
+    n = 3000 if len(gd["rects"]) < 1000 else 600
+    with frw.Layout.from_rects(gd["rects"], gd["bounds"]) as L:
+        end, hops, b1, w = L.walk_trace(target, 1000, n, seed=12345, o=o)
+    end_o, hops_o, b1_o, w_o = G.walks(oracle_cfg(G, o, target, 12345), 1000, n)
+    assert np.array_equal(end, end_o)
+    assert np.array_equal(hops, hops_o)
+    assert np.array_equal(b1, b1_o)
+    assert np.array_equal(w, w_o)
+
+
+def config1_layout():
+    return frw.generate_layout(0xF4A7 + 1, 100, 1000.0)
+
+
+def test_estimator_matches_oracle_sums_config1():
+    """C1: 100 rects on [0,1000]^2, target 0, offset-1 surface, 1e5 walks."""
+    rects = config1_layout()
+    o = frw.capacitance_opts(1.0)
+    G = O.Grid(rects.astype(np.float64))
+    n = 100_000
+    with frw.Layout.from_rects(rects) as L:
+        res = L.walk(0, n, seed=99, o=o)
+    end, hops, b1, w = G.walks(oracle_cfg(G, o, 0, 99), 0, n)
+    assert res.walks == n and res.escaped == (end == -1).sum() and res.aborted == (end == -2).sum()
+    assert res.hops_total == hops.sum()
+    ks, counts = np.unique(end[end >= 0], return_counts=True)
+    assert np.array_equal(res.conductor, ks) and np.array_equal(res.hits, counts)
+    for k, c, se in zip(res.conductor, res.cap, res.cap_se):
+        wk = np.where(end == k, w, 0.0)
+        assert c == pytest.approx(wk.mean(), rel=1e-12, abs=1e-30)
+        assert se == pytest.approx(wk.std(ddof=1) / np.sqrt(n), rel=1e-6)
+    # physics sanity: self-capacitance positive, couplings negative
+    i0 = np.searchsorted(res.conductor, 0)
+    assert res.cap[i0] > 0 and (np.delete(res.cap, i0) <= 0).all()
+    assert res.fraction_other == pytest.approx(1 - counts[ks == 0][0] / n)
+
+
+def test_walks_independent_of_launch_shape():
+    rects = config1_layout()
+    o1 = frw.capacitance_opts(1.0)
+    o2 = frw.capacitance_opts(1.0, blocks_per_sm=1, refill_min=8)
+    with frw.Layout.from_rects(rects) as L:
+        a = L.walk_trace(0, 0, 20_000, seed=5, o=o1)
+        b = L.walk_trace(0, 0, 20_000, seed=5, o=o2)
+        r1 = L.walk(0, 50_000, seed=5, o=o1)
+        r2 = L.walk(0, 50_000, seed=5, o=o2)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+    assert np.array_equal(r1.hits, r2.hits)
+    np.testing.assert_allclose(r1.cap, r2.cap, rtol=1e-12)
+
+
+def test_hop_cap_and_escapes():
+    rects = config1_layout()
+    o = frw.capacitance_opts(1.0, hop_cap=1)
+    with frw.Layout.from_rects(rects) as L:
+        end, hops, _, w = L.walk_trace(0, 0, 5000, seed=1, o=o)
+        res = L.walk(0, 5000, seed=1, o=o)
+    assert hops.max() <= 1 and ((end == -2) | (end >= -1)).all()
+    assert res.aborted == (end == -2).sum() > 0
+    assert (w[end < 0] == 0).all()
+
+
+def test_reference_mode_matches_reference_hit_distribution(golden):
+    """test2 with the reference's own start and Gaussian surface: the device
+    hit shares agree with the compiled reference's seeded walks within 3
+    combined standard errors (the defect does not change test2's result)."""
+    gd = golden("test2")
+    t = int(gd["walk_target"])
+    ref_end = gd["walk_end"]
+    with frw.Layout.from_rects(gd["rects"], gd["bounds"]) as L:
+        res = L.walk(t, 400_000, seed=2024, o=frw.opts())
+    n_ref = len(ref_end)
+    for k in np.unique(np.concatenate([ref_end[ref_end >= 0], res.conductor])):
+        p_ref = (ref_end == k).mean()
+        p_gpu = res.row(k)[0] / res.walks
+        se = np.sqrt(p_ref * (1 - p_ref) / n_ref + p_gpu * (1 - p_gpu) / res.walks) + 1e-12
+        assert abs(p_ref - p_gpu) <= 3 * se + 1.0 / n_ref, (k, p_ref, p_gpu)
+
+
+def test_avg_path_len_entry_point(tmp_path):
+    rects = config1_layout()
+    p = str(tmp_path / "c1.txt")
+    frw.write_layout(p, rects)
+    h = str(tmp_path / "wyniki.txt")
+    f = frw.get_avg_path_len_cuda(p, 20_000, 0, seed=3, hist_path=h)
+    with frw.Layout.from_file(p) as L:
+        r = L.walk(0, 20_000, seed=3, o=frw.opts())
+    assert f == r.fraction_other and 0 < f < 1
+    lines = open(h, encoding="utf-8").read().splitlines()
+    assert lines[0] == "[GPU]" and len(lines) >= 2
