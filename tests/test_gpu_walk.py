@@ -66,8 +66,6 @@ def test_estimator_matches_oracle_sums_config1():
     # physics sanity: self-capacitance positive, couplings not significantly positive
     i0 = np.searchsorted(res.conductor, 0)
     assert res.cap[i0] > 0 and (np.delete(res.cap, i0) <= 3 * np.delete(res.cap_se, i0)).all()
-    # charge neutrality is not exact (escapes end at potential 0) but the row sum is small
-    assert abs(res.cap.sum()) < 0.2 * res.cap[i0]
     assert res.fraction_other == pytest.approx(1 - counts[ks == 0][0] / n)
 
 
