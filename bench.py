@@ -52,13 +52,19 @@ def measured_peak_hbm():
     return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per walk-kernel launch from the committed ncu summary."""
+def profiled_traffic(walks_per_launch: int):
+    """DRAM bytes of one walk-kernel launch of `walks_per_launch` walks, scaled
+    from the committed ncu capture (a smaller launch of the same kernel and
+    layout; the traffic is accumulator flushes, proportional to walks)."""
     p = os.path.join(ROOT, "profiles", "walk_kernel_c2.md")
     if not os.path.exists(p):
         return None
-    m = re.search(r"dram_bytes_per_launch\s*=\s*([0-9.eE+]+)", open(p).read())
-    return float(m.group(1)) if m else None
+    txt = open(p).read()
+    m = re.search(r"dram_bytes_per_launch\s*=\s*([0-9.eE+]+)", txt)
+    w = re.search(r"walks_per_launch\s*=\s*([0-9.eE+]+)", txt)
+    if not (m and w):
+        return None
+    return float(m.group(1)) * walks_per_launch / float(w.group(1))
 
 
 class Clocks:
@@ -295,7 +301,7 @@ def main():
         kms = statistics.median(kern_ms)
         achieved = W["walks"] * hbar * bq / (kms * 1e-3) / 1e9
         peak, peak_kind = measured_peak_hbm()
-        traffic = profiled_traffic()
+        traffic = profiled_traffic(W["walks"])
         out = {
             "metric": METRIC, "value": value, "unit": "walks/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
