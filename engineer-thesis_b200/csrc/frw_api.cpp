@@ -304,6 +304,29 @@ frw_status run_walks(const frw_layout *lay, int64_t target, uint64_t first_walk,
 
 void set_error(const std::string &msg) { g_err = msg; }
 
+frw_status layout_view(const frw_layout *L, LayoutView *out) {
+    if (!L) {
+        set_error("null layout");
+        return FRW_E_ARG;
+    }
+    out->dl = L->dl;
+    out->device = L->device;
+    out->n = L->n;
+    out->rects = L->rects.data();
+    return FRW_OK;
+}
+
+frw_status device_tables(int device, const double **tables, int *sms) {
+    DeviceCtx *c;
+    frw_status rc = device_ctx(device, &c);
+    if (rc) return rc;
+    *tables = c->tables;
+    *sms = c->sms;
+    return FRW_OK;
+}
+
+frw_status check_opts(const frw_opts *o) { return validate_opts(o); }
+
 frw_status cuda_fail(cudaError_t e, const char *what) {
     g_err = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
     if (e == cudaErrorMemoryAllocation) return FRW_E_OOM;

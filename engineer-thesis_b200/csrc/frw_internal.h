@@ -137,4 +137,16 @@ frw_status launch_compact(const unsigned long long *acc_n, const double *acc_s, 
 // host_green.cpp
 void green_tables(double *g, double *intg, double *wx, double *wy);
 
+// frw_api.cpp: read-only views for other host files (no allocation once the
+// device has been initialised by a layout)
+struct LayoutView {
+    DevLayout dl;
+    int device;
+    int64_t n;
+    const double *rects;  // host copy, layer order
+};
+frw_status layout_view(const frw_layout *layout, LayoutView *out);
+frw_status device_tables(int device, const double **tables, int *sms);
+frw_status check_opts(const frw_opts *opts);
+
 }  // namespace frw

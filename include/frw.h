@@ -176,6 +176,24 @@ frw_status frw_walk_trace(const frw_layout *layout, int64_t target, uint64_t fir
                           uint64_t walks, uint64_t seed, const frw_opts *opts, int64_t *end,
                           int32_t *hops, int32_t *bin1, double *weight, int mem, void *stream);
 
+/* frw_walk_trace for callers that cannot allocate device memory during the
+ * call (an application that owns all GPU memory through its own pool, a
+ * real-time loop that forbids allocator latency, a plugin inside a host
+ * process that manages the CUDA context).  It has no counterpart in the
+ * reference.  end/hops/bin1/weight are DEVICE arrays of `walks` entries on
+ * the layout's device, all required.  The walk kernel's scratch lives in a
+ * fixed file-scope device array sized for layouts of at most 65,536 rects
+ * (1.5 MiB, held by every GPU that loads the library until exit); larger
+ * layouts are rejected with FRW_E_ARG.  The first call on a device resolves
+ * the array's address (cudaGetSymbolAddress) -- make that first call before
+ * any stream capture.  All calls share the array and the call clears it
+ * first, so calls that overlap on the GPU (other streams or threads) race:
+ * serialise them.  Returns after the stream has drained (the kernel status
+ * word is checked).  Results equal frw_walk_trace's. */
+frw_status frw_walk_trace_static(const frw_layout *layout, int64_t target, uint64_t first_walk,
+                                 uint64_t walks, uint64_t seed, const frw_opts *opts, int64_t *end,
+                                 int32_t *hops, int32_t *bin1, double *weight, void *stream);
+
 /* Gaussian surface of `target` under opts (scale mode runs the reference's
  * bisection on the device). */
 frw_status frw_gauss_surface(const frw_layout *layout, int64_t target, const frw_opts *opts,
