@@ -205,6 +205,7 @@ def main():
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     import frw
+    from frw import shard
 
     W = WORKLOAD
     rects = frw.generate_layout(W["layout_seed"], W["rects"], W["domain"])
@@ -224,18 +225,14 @@ def main():
 
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
-    o = frw.capacitance_opts(1.0, stream_id=rank)
+    o = frw.capacitance_opts(1.0, stream_id=shard.plan(W["walks"], rank)["stream"])
     L = frw.Layout.from_rects(rects, device=local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
 
     def step(seed):
         r = L.walk(W["target"], W["walks"], seed, o, stream=stream.cuda_stream)
-        if dist is not None:
-            buf = torch.zeros(3, L.n, dtype=torch.float64, device=dev)
-            idx = torch.as_tensor(r.conductor, device=dev)
-            buf[0, idx] = torch.as_tensor(r.hits.astype(np.float64), device=dev)
-            buf[1, idx] = torch.as_tensor(r.cap * r.walks, device=dev)
-            dist.all_reduce(buf)
+        if dist is not None:  # the one exchange: sum of the packed rows (NCCL)
+            shard.all_reduce_rows(torch.as_tensor(shard.result_rows(r, L.n), device=dev))
         return r
 
     for i in range(args.warmup):

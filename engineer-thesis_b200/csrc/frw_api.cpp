@@ -663,6 +663,8 @@ frw_status frw_walk(const frw_layout *L, int64_t target, uint64_t walks, uint64_
         if (res->hits) res->hits[k] = R.n[i];
         if (res->cap) res->cap[k] = mean;
         if (res->cap_se) res->cap_se[k] = sqrt(var / N);
+        if (res->sum_w) res->sum_w[k] = R.s[i];
+        if (res->sum_w2) res->sum_w2[k] = R.s2[i];
     }
     res->fraction_other = walks ? (double)(walks - on_target) / N : 0.0;
     return FRW_OK;

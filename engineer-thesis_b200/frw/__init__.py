@@ -75,6 +75,8 @@ class Result(C.Structure):
         ("hits", C.POINTER(C.c_uint64)),
         ("cap", C.POINTER(C.c_double)),
         ("cap_se", C.POINTER(C.c_double)),
+        ("sum_w", C.POINTER(C.c_double)),
+        ("sum_w2", C.POINTER(C.c_double)),
     ]
 
 
@@ -209,6 +211,8 @@ class WalkResult:
     hits: np.ndarray
     cap: np.ndarray
     cap_se: np.ndarray
+    sum_w: np.ndarray
+    sum_w2: np.ndarray
     extra: dict = field(default_factory=dict)
 
     def row(self, k: int):
@@ -316,16 +320,20 @@ class Layout:
         hits = np.zeros(cap, dtype=np.uint64)
         c = np.zeros(cap)
         se = np.zeros(cap)
+        s1 = np.zeros(cap)
+        s2 = np.zeros(cap)
         r = Result()
         r.capacity = cap
         r.conductor = _ptr(cond, _I64)
         r.hits = _ptr(hits, C.POINTER(C.c_uint64))
         r.cap = _ptr(c, _D)
         r.cap_se = _ptr(se, _D)
+        r.sum_w = _ptr(s1, _D)
+        r.sum_w2 = _ptr(s2, _D)
         _check(lib().frw_walk(self._h, target, walks, seed, C.byref(o) if o else None, C.byref(r), stream or None))
         m = min(r.n_entries, cap)
         return WalkResult(r.walks, r.escaped, r.aborted, r.hops_total, np.array(r.gauss[:]), r.fraction_other,
-                          r.kernel_ms, cond[:m], hits[:m], c[:m], se[:m])
+                          r.kernel_ms, cond[:m], hits[:m], c[:m], se[:m], s1[:m], s2[:m])
 
     def walk_trace(self, target: int, first: int, walks: int, seed: int, o: Opts | None = None):
         end = np.zeros(walks, dtype=np.int64)

@@ -158,6 +158,8 @@ typedef struct frw_result {
     uint64_t *hits;            /* walks ending on it */
     double *cap;               /* capacitance C_t,k in F/m (uniform start; 0 otherwise) */
     double *cap_se;            /* its standard error */
+    double *sum_w;             /* optional: sum of the weights (rows add exactly across ranks) */
+    double *sum_w2;            /* optional: sum of the squared weights */
 } frw_result;
 
 /* Runs `walks` walks from the Gaussian surface of conductor `target`
