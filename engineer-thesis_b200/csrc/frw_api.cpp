@@ -456,6 +456,14 @@ frw_status frw_layout_create(const float *rects, int64_t n, const double *bounds
         // M = 4 * max(|bounds|, W, H) + 16 after <= 256 roundings of at most
         // M * 2^-53 each, i.e. within M * 2^-45; delta = M * 2^-40 leaves 32x.
         double M = std::max(std::max(fabs(b[0]), fabs(b[1])), std::max(fabs(b[2]), fabs(b[3])));
+        // FP32 pre-filter: a point inside the bounds rounds to float within
+        // ulp(Mb)/2 and a float difference of two such values within ulp(Mb),
+        // so FP32 gaps are within 1.5 ulp(Mb) of the exact ones and the
+        // rounded limit within another ulp; 4 ulp(Mb) is a safe margin.
+        const double Mb = std::max(M, 1.0);
+        int ex = 0;
+        frexp(Mb, &ex);  // Mb in [2^(ex-1), 2^ex)
+        dl.slack = (float)ldexp(4.0, ex - 1 - 23);
         M = 4.0 * std::max(M, std::max(bw, bh)) + 16.0;
         dl.delta = ldexp(M, -40);
     }

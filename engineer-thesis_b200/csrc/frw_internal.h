@@ -40,6 +40,7 @@ struct DevLayout {
     double bx0, by0, bx1, by1;  // layer bounds (reference getLayerSize)
     double dist0;               // 0.05 * max(W, H): drawBiggestSquareAtPoint's first step
     double delta;               // tie window of the clearance replay (see query.cuh)
+    float slack;                // FP32 pre-filter margin: 4 ulp_f32(max |bound|)
     int32_t n, nodes;
 };
 

@@ -36,12 +36,15 @@ struct Cands {
     int n;
 };
 
-__device__ __forceinline__ double lb_box(const float4 b, double px, double py) {
-    double d = fmax(fmax((double)b.x - px, px - (double)b.z), fmax((double)b.y - py, py - (double)b.w));
-    return fmax(d, 0.0);
+// L-infinity distance from a point (in FP32) to a box, 0 inside.
+__device__ __forceinline__ float lb_box_f(const float4 b, float px, float py) {
+    return fmaxf(fmaxf(fmaxf(b.x - px, px - b.z), fmaxf(b.y - py, py - b.w)), 0.f);
 }
 
-// One depth-first, nearest-child-first traversal.  Returns status bits.
+// One depth-first, nearest-child-first traversal.  Node boxes and rect gaps
+// are screened in FP32 (errors below L.slack); only rects that can matter --
+// inside the current tie window or containing p -- get the exact FP64 gap.
+// Returns status bits.
 __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, double py, Cands &C,
                                               int &hit, double &best) {
     uint32_t st = 0;
@@ -49,6 +52,11 @@ __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, dou
     best = fmin(fmin(px - L.bx0, L.bx1 - px), fmin(py - L.by0, L.by1 - py));
     hit = kNoHit;
     C.n = 0;
+    // outside the closed bounds no rect can contain p and p+-1 already
+    // leaves the bounds: nothing to look up
+    if (!(px >= L.bx0 && py >= L.by0 && px <= L.bx1 && py <= L.by1)) return 0;
+    const float pxf = (float)px, pyf = (float)py, slack = L.slack;
+    float limf = (float)(fmax(best, 0.0) + r2) + slack;  // screen: FP32 value > limf => exact > limit
     int stk_node[kStackMax];
     float stk_lb[kStackMax];
     int sp = 1;
@@ -56,8 +64,8 @@ __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, dou
     stk_lb[0] = 0.f;
     while (sp > 0) {
         --sp;
+        if (stk_lb[sp] > limf) continue;
         const int nd = stk_node[sp];
-        if ((double)stk_lb[sp] > fmax(best, 0.0) + r2) continue;
         const float4 *bp = L.nbox + 4 * nd;
         float4 b[4];
         b[0] = __ldg(bp);
@@ -66,17 +74,18 @@ __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, dou
         b[3] = __ldg(bp + 3);
         const int4 rf = __ldg(L.nref + nd);
         const int ref[4] = {rf.x, rf.y, rf.z, rf.w};
-        double lb[4];
+        float lb[4];
 #pragma unroll
-        for (int c = 0; c < 4; c++) lb[c] = ref[c] == kRefEmpty ? 1e300 : lb_box(b[c], px, py);
+        for (int c = 0; c < 4; c++) lb[c] = ref[c] == kRefEmpty ? 3.0e38f : lb_box_f(b[c], pxf, pyf);
         // leaves of this node first: they tighten `best` before children are pushed
 #pragma unroll
         for (int c = 0; c < 4; c++) {
-            if (ref[c] > kRefEmpty || ref[c] == kRefEmpty) continue;
-            if (lb[c] > fmax(best, 0.0) + r2) continue;
+            if (ref[c] >= kRefEmpty || lb[c] > limf) continue;
             const int f = leaf_first(ref[c]), m = leaf_count(ref[c]);
             for (int k = f; k < f + m; k++) {
                 const float4 r = __ldg(L.rects + k);
+                const float gf = fmaxf(fmaxf(r.x - pxf, pxf - r.z), fmaxf(r.y - pyf, pyf - r.w));
+                if (gf > limf) continue;
                 const double x0 = r.x, y0 = r.y, x1 = r.z, y1 = r.w;
                 const double g = fmax(fmax(x0 - px, px - x1), fmax(y0 - py, py - y1));
                 if (g <= 0.0 && px >= x0 && py >= y0 && px <= x1 && py <= y1) {
@@ -85,6 +94,7 @@ __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, dou
                 }
                 if (g < best) {
                     best = g;
+                    limf = (float)(fmax(best, 0.0) + r2) + slack;
                     int j = 0;
                     for (int q = 0; q < C.n; q++)
                         if ((double)C.g[q] <= best + r2) {
@@ -106,7 +116,6 @@ __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, dou
             }
         }
         // internal children, farthest pushed first so the nearest is popped next
-        const double lim = fmax(best, 0.0) + r2;
         int ord[4] = {0, 1, 2, 3};
 #pragma unroll
         for (int a = 0; a < 3; a++)
@@ -120,10 +129,10 @@ __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, dou
 #pragma unroll
         for (int c = 0; c < 4; c++) {
             const int q = ord[c];
-            if (ref[q] < 0 || lb[q] > lim) continue;
+            if (ref[q] < 0 || lb[q] > limf) continue;
             if (sp < kStackMax) {
                 stk_node[sp] = ref[q];
-                stk_lb[sp] = __double2float_rd(lb[q]);
+                stk_lb[sp] = lb[q];
                 sp++;
             } else {
                 st |= kStStackOverflow;

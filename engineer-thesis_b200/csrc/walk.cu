@@ -10,9 +10,9 @@
 //     counter (one atomic per warp refill), so warps stay full while walks of
 //     very different lengths finish;
 //   * random numbers are counter-based Philox4x32-10 keyed by (seed) with
-//     counter (hop, walk, stream): a walk's trajectory depends only on its
-//     index, never on scheduling, so every walk can be replayed by the CPU
-//     oracle bit-for-bit;
+//     counter (hop/4, walk, stream), one 32-bit word per hop: a walk's
+//     trajectory depends only on its index, never on scheduling, so every
+//     walk can be replayed by the CPU oracle bit-for-bit;
 //   * the Green CDF (201 doubles) and the first-hop weight tables sit in
 //     shared memory; bins are found by binary search (the reference's linear
 //     scan, CPU/mainFunctions.cpp:40-46, returns the same index because the
@@ -51,12 +51,17 @@ __device__ __forceinline__ uint4 philox10(uint4 c, uint2 k) {
     return c;
 }
 
-// First uniform of Philox block (hop, walk, stream) under `seed`: 53 bits.
-__device__ __forceinline__ double draw_u(uint64_t seed, uint32_t stream, uint64_t walk, uint32_t hop) {
-    const uint4 o = philox10(make_uint4(hop, (uint32_t)walk, (uint32_t)(walk >> 32), stream),
-                             make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
-    const unsigned long long m = ((unsigned long long)(o.x >> 5) << 26) | (unsigned long long)(o.y >> 6);
-    return (double)m * 0x1p-53;
+// Philox block (hop / 4, walk, stream) under key `seed`: the four uniforms of
+// hops 4k..4k+3 of one walk.
+__device__ __forceinline__ uint4 draw_block(uint64_t seed, uint32_t stream, uint64_t walk, uint32_t hop) {
+    return philox10(make_uint4(hop >> 2, (uint32_t)walk, (uint32_t)(walk >> 32), stream),
+                    make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
+}
+
+__device__ __forceinline__ double word_u(const uint4 &b, uint32_t hop) {
+    const uint32_t k = hop & 3;
+    const uint32_t x = k == 0 ? b.x : (k == 1 ? b.y : (k == 2 ? b.z : b.w));
+    return (double)x * 0x1p-32;
 }
 
 __device__ __forceinline__ int bin_of(const double *s_intg, double u) {
@@ -185,6 +190,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(const WalkParams P) {
     int job = 0;
     uint64_t gw = 0, pw = 0;
     uint32_t hop = 0, stream = 0;
+    uint4 rnd = make_uint4(0, 0, 0, 0);  // uniforms of hops (hop & ~3) .. +3
     int32_t hops = 0, bin1 = -1;
     int side = 0;
     double px = 0, py = 0, a0 = 0, perim = 0;
@@ -222,7 +228,8 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(const WalkParams P) {
                     hops = 0;
                     bin1 = -1;
                     a0 = 0.0;
-                    const double u = draw_u(P.seed, stream, pw, 0);
+                    rnd = draw_block(P.seed, stream, pw, 0);
+                    const double u = word_u(rnd, 0);
                     if (uniform_start) {
                         side = perimeter_point(G, u, px, py);
                     } else {
@@ -252,7 +259,8 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(const WalkParams P) {
                 else if (hops >= P.hop_cap) code = -2;
                 else {
                     hop++;
-                    const int bin = bin_of(s_intg, draw_u(P.seed, stream, pw, hop));
+                    if ((hop & 3) == 0) rnd = draw_block(P.seed, stream, pw, hop);
+                    const int bin = bin_of(s_intg, word_u(rnd, hop));
                     if (hop == 1) {
                         bin1 = bin;
                         a0 = __dsub_rn(sq[2], sq[0]);

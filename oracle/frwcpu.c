@@ -750,14 +750,14 @@ static void perimeter_point(const double G[4], double u, double p[2], double n[2
     else { p[0] = G[0]; p[1] = G[3] - (s - 2 * w - h); n[0] = -1; n[1] = 0; }
 }
 
-static void draw(uint64_t seed, uint32_t stream, uint64_t walk, uint32_t hop, double *u0,
-                 double *u1) {
-    uint32_t ctr[4] = {hop, (uint32_t)walk, (uint32_t)(walk >> 32), stream};
+/* Uniform number of hop `hop` of walk `walk`: Philox4x32-10 block
+ * (hop / 4, walk, stream) under key `seed`, word hop % 4, scaled by 2^-32. */
+static double draw(uint64_t seed, uint32_t stream, uint64_t walk, uint32_t hop) {
+    uint32_t ctr[4] = {hop >> 2, (uint32_t)walk, (uint32_t)(walk >> 32), stream};
     uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
     uint32_t o[4];
     oc_philox4x32_10(ctr, key, o);
-    *u0 = oc_u01(o[0], o[1]);
-    *u1 = oc_u01(o[2], o[3]);
+    return (double)o[hop & 3] * (1.0 / 4294967296.0);
 }
 
 /* The walk of CPU/mainFunctions.cpp:48-90 on complete queries, with the
@@ -776,9 +776,9 @@ int oc_walk_run(const oc_grid *g, const double *rects, const oc_walk_cfg *cfg, u
     double L = 2 * (G[2] - G[0]) + 2 * (G[3] - G[1]);
     for (uint64_t k = 0; k < count; k++) {
         uint64_t w = first + k;
-        double u0, u1, p[2], nrm[2] = {0, 0}, sq[4];
+        double u0, p[2], nrm[2] = {0, 0}, sq[4];
         uint32_t hop = 0;
-        draw(cfg->seed, cfg->stream, w, hop, &u0, &u1);
+        u0 = draw(cfg->seed, cfg->stream, w, hop);
         if (cfg->start_mode == OC_START_UNIFORM) {
             perimeter_point(G, u0, p, nrm);
         } else {
@@ -796,7 +796,7 @@ int oc_walk_run(const oc_grid *g, const double *rects, const oc_walk_cfg *cfg, u
             if (hit >= 0) { end = hit; break; }
             if (hops >= cfg->hop_cap) { end = OC_END_ABORTED; break; }
             hop++;
-            draw(cfg->seed, cfg->stream, w, hop, &u0, &u1);
+            u0 = draw(cfg->seed, cfg->stream, w, hop);
             int bin = oc_bin_index(intg, OC_NSAMPLE, u0);
             if (hop == 1) { bin1 = bin; a0 = sq[2] - sq[0]; }
             oc_point_from_index(sq, bin, OC_NSAMPLE, cfg->exact_perimeter, p);
