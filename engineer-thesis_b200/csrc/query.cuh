@@ -59,13 +59,9 @@ __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, dou
     float limf = (float)(fmax(best, 0.0) + r2) + slack;  // screen: FP32 value > limf => exact > limit
     int stk_node[kStackMax];
     float stk_lb[kStackMax];
-    int sp = 1;
-    stk_node[0] = 0;
-    stk_lb[0] = 0.f;
-    while (sp > 0) {
-        --sp;
-        if (stk_lb[sp] > limf) continue;
-        const int nd = stk_node[sp];
+    int sp = 0;
+    int nd = 0;  // node being visited; the nearest qualifying child is visited next directly
+    for (;;) {
         const float4 *bp = L.nbox + 4 * nd;
         float4 b[4];
         b[0] = __ldg(bp);
@@ -77,7 +73,7 @@ __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, dou
         float lb[4];
 #pragma unroll
         for (int c = 0; c < 4; c++) lb[c] = ref[c] == kRefEmpty ? 3.0e38f : lb_box_f(b[c], pxf, pyf);
-        // leaves of this node first: they tighten `best` before children are pushed
+        // leaves of this node first: they tighten `best` before descending
 #pragma unroll
         for (int c = 0; c < 4; c++) {
             if (ref[c] >= kRefEmpty || lb[c] > limf) continue;
@@ -115,29 +111,38 @@ __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, dou
                 }
             }
         }
-        // internal children, farthest pushed first so the nearest is popped next
-        int ord[4] = {0, 1, 2, 3};
-#pragma unroll
-        for (int a = 0; a < 3; a++)
-#pragma unroll
-            for (int c = 0; c < 3 - a; c++)
-                if (lb[ord[c]] < lb[ord[c + 1]]) {
-                    int t = ord[c];
-                    ord[c] = ord[c + 1];
-                    ord[c + 1] = t;
-                }
+        // internal children within reach: visit the nearest next, stack the rest
+        int next = -1;
+        float nlb = 0.f;
 #pragma unroll
         for (int c = 0; c < 4; c++) {
-            const int q = ord[c];
-            if (ref[q] < 0 || lb[q] > limf) continue;
-            if (sp < kStackMax) {
-                stk_node[sp] = ref[q];
-                stk_lb[sp] = lb[q];
-                sp++;
-            } else {
-                st |= kStStackOverflow;
+            if (ref[c] < 0 || lb[c] > limf) continue;
+            int push = ref[c];
+            float plb = lb[c];
+            if (next < 0 || lb[c] < nlb) {
+                push = next;
+                plb = nlb;
+                next = ref[c];
+                nlb = lb[c];
+            }
+            if (push >= 0) {
+                if (sp < kStackMax) {
+                    stk_node[sp] = push;
+                    stk_lb[sp] = plb;
+                    sp++;
+                } else {
+                    st |= kStStackOverflow;
+                }
             }
         }
+        if (next >= 0) {
+            nd = next;
+            continue;
+        }
+        // nothing below: resume the most recent stacked subtree still in reach
+        while (sp > 0 && stk_lb[sp - 1] > limf) --sp;
+        if (sp == 0) break;
+        nd = stk_node[--sp];
     }
     return st;
 }

@@ -31,6 +31,7 @@ constexpr int kWarpsPerBlock = kWalkThreads / 32;
 constexpr int kTabSlots = 32;  // per warp
 constexpr unsigned long long kEmptyKey = ~0ull;
 constexpr unsigned kFull = 0xFFFFFFFFu;
+constexpr uint64_t kChunk = 128;  // walks a warp claims from the global counter at a time
 
 struct Slot {
     unsigned long long key, n, hops;
@@ -114,22 +115,30 @@ __device__ __forceinline__ int slot_hash(unsigned long long key) {
     return (int)((key * 0x9E3779B97F4A7C15ull) >> 59);  // 5 bits
 }
 
-// Single-lane insert; false when the warp table is full.
-__device__ __forceinline__ bool tab_insert(Slot *tab, unsigned long long key, double w, uint32_t hops) {
-    int h = slot_hash(key);
+// Insert one (job, conductor) aggregate; called by several lanes of a warp at
+// once with DISTINCT keys (so distinct slots): empty slots are claimed with a
+// shared-memory CAS, the rest of the update has a single writer.  False when
+// the warp table is full.
+__device__ __forceinline__ bool tab_insert(Slot *tab, unsigned long long key, unsigned long long n, double s,
+                                           double s2, unsigned long long hops) {
+    const int h = slot_hash(key);
     for (int probe = 0; probe < kTabSlots; probe++) {
         Slot &sl = tab[(h + probe) & (kTabSlots - 1)];
-        if (sl.key == key || sl.key == kEmptyKey) {
-            if (sl.key == kEmptyKey) {
-                sl.key = key;
+        unsigned long long k = *(volatile unsigned long long *)&sl.key;
+        if (k == kEmptyKey) {
+            k = atomicCAS(&sl.key, kEmptyKey, key);
+            if (k == kEmptyKey) {
                 sl.n = 0;
                 sl.hops = 0;
                 sl.s = sl.cs = sl.s2 = sl.cs2 = 0.0;
+                k = key;
             }
-            sl.n += 1;
+        }
+        if (k == key) {
+            sl.n += n;
             sl.hops += hops;
-            kahan_add(sl.s, sl.cs, w);
-            kahan_add(sl.s2, sl.cs2, __dmul_rn(w, w));
+            kahan_add(sl.s, sl.cs, s);
+            kahan_add(sl.s2, sl.cs2, s2);
             return true;
         }
     }
@@ -187,6 +196,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(const WalkParams P) {
     const bool exact = P.exact_perimeter != 0;
 
     bool active = false, exhausted = false;
+    uint64_t chunk_next = 0, chunk_end = 0;  // warp-uniform: unclaimed part of this warp's walk chunk
     int job = 0;
     uint64_t gw = 0, pw = 0;
     uint32_t hop = 0, stream = 0;
@@ -198,16 +208,27 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(const WalkParams P) {
     uint32_t st = 0;
 
     for (;;) {
-        // ---- refill idle lanes from the global walk counter ----
+        // ---- refill idle lanes from the warp's chunk of the walk counter ----
         const unsigned idle = __ballot_sync(kFull, !active);
         if (!exhausted && __popc(idle) >= refill_min) {
-            const int cnt = __popc(idle), leader = __ffs(idle) - 1;
-            unsigned long long base = 0;
-            if (lane == leader) base = atomicAdd(P.counter, (unsigned long long)cnt);
-            base = __shfl_sync(kFull, base, leader);
-            if (base + cnt >= P.total_walks) exhausted = true;
+            const uint64_t need = (uint64_t)__popc(idle), avail = chunk_end - chunk_next;
+            const uint64_t r = (uint64_t)__popc(idle & lt);
+            uint64_t mine;
+            if (avail >= need) {
+                mine = chunk_next + r;
+                chunk_next += need;
+            } else {  // top up: one atomic per kChunk walks per warp
+                const int leader = __ffs(idle) - 1;
+                unsigned long long nb = 0;
+                if (lane == leader) nb = atomicAdd(P.counter, (unsigned long long)kChunk);
+                nb = __shfl_sync(kFull, nb, leader);
+                mine = r < avail ? chunk_next + r : nb + (r - avail);
+                chunk_next = nb + (need - avail);
+                chunk_end = nb + kChunk;
+            }
+            if (chunk_end >= P.total_walks && chunk_next >= P.total_walks) exhausted = true;
             if (!active) {
-                gw = base + __popc(idle & lt);
+                gw = mine;
                 if (gw < P.total_walks) {
                     if (kMulti) {
                         int lo = 0, hi = P.njobs;  // last job with walk_begin <= gw
@@ -288,20 +309,39 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(const WalkParams P) {
             }
             active = false;
         }
-        unsigned em = __ballot_sync(kFull, ended);
-        while (em) {
-            const int l = __ffs(em) - 1;
-            bool ok = true;
-            if (lane == l)
-                ok = tab_insert(tab, ((unsigned long long)job << 32) | (uint32_t)(code + 2), wgt, (uint32_t)hops);
-            __syncwarp();
-            if (!__shfl_sync(kFull, ok, l)) {
-                tab_flush<kMulti>(P, tab, lane);
-                continue;  // retry lane l on the empty table
+        const unsigned em = __ballot_sync(kFull, ended);
+        if (em) {
+            // group equal (job, conductor) keys; each group's lowest lane adds
+            // the group's sums to the table, all groups in parallel
+            const unsigned long long key = ((unsigned long long)job << 32) | (uint32_t)(code + 2);
+            bool lead = false;
+            if (ended) lead = (__match_any_sync(em, key) & lt) == 0;
+            const unsigned leaders = __ballot_sync(kFull, lead);
+            double s1 = wgt, s2 = __dmul_rn(wgt, wgt);
+            unsigned long long hs = (unsigned long long)hops, cnt = 1;
+            for (unsigned rest = em & ~leaders; rest; rest &= rest - 1) {
+                const int l = __ffs(rest) - 1;
+                const double wl = __shfl_sync(kFull, wgt, l);
+                const unsigned long long kl = __shfl_sync(kFull, key, l);
+                const int hl = __shfl_sync(kFull, hops, l);
+                if (lead && kl == key) {
+                    s1 = __dadd_rn(s1, wl);
+                    s2 = __dadd_rn(s2, __dmul_rn(wl, wl));
+                    hs += (unsigned long long)hl;
+                    cnt++;
+                }
             }
-            em &= em - 1;
+            bool pending = lead;
+            for (;;) {
+                const bool failed = pending && !tab_insert(tab, key, cnt, s1, s2, hs);
+                pending = failed;
+                __syncwarp();
+                if (!__any_sync(kFull, failed)) break;
+                tab_flush<kMulti>(P, tab, lane);  // table full: empty it, retry the rest
+            }
         }
     }
+    __syncwarp();
     tab_flush<kMulti>(P, tab, lane);
     if (st) atomicOr(P.status, st);
 }
