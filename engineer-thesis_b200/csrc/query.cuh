@@ -148,10 +148,32 @@ __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, dou
 }
 
 // Tree::checkCollisions(box) restricted to the near-tie list (exact for the
-// boxes of the replay, see the file comment).
-__device__ __forceinline__ bool collides_listed(const DevLayout &L, const Cands &C, const double o[4]) {
+// boxes of the replay, see the file comment).  The first two listed rects
+// are held as doubles for the whole replay; further ones (rare) are read back.
+struct Listed {
+    double x0[2], y0[2], x1[2], y1[2];
+    int n;
+};
+
+__device__ __forceinline__ void load_listed(const DevLayout &L, const Cands &C, Listed &T) {
+    T.n = C.n;
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+        const float4 r = q < C.n ? __ldg(L.rects + C.idx[q]) : make_float4(1.f, 1.f, 0.f, 0.f);
+        T.x0[q] = r.x;
+        T.y0[q] = r.y;
+        T.x1[q] = r.z;
+        T.y1[q] = r.w;
+    }
+}
+
+__device__ __forceinline__ bool collides_listed(const DevLayout &L, const Cands &C, const Listed &T,
+                                                const double o[4]) {
     if (!(o[1] >= L.by0 && o[0] >= L.bx0 && o[3] <= L.by1 && o[2] <= L.bx1)) return true;
-    for (int q = 0; q < C.n; q++) {
+#pragma unroll
+    for (int q = 0; q < 2; q++)
+        if (q < T.n && T.x1[q] >= o[0] && o[2] >= T.x0[q] && T.y1[q] >= o[1] && o[3] >= T.y0[q]) return true;
+    for (int q = 2; q < T.n; q++) {
         const float4 r = __ldg(L.rects + C.idx[q]);
         if ((double)r.z >= o[0] && o[2] >= (double)r.x && (double)r.w >= o[1] && o[3] >= (double)r.y)
             return true;
@@ -163,14 +185,16 @@ __device__ __forceinline__ bool collides_listed(const DevLayout &L, const Cands 
 // explicit round-to-nearest intrinsics (no contraction).
 __device__ __forceinline__ uint32_t replay_square(const DevLayout &L, const Cands &C, double px,
                                                   double py, double sq[4]) {
+    Listed T;
+    load_listed(L, C, T);
     double o[4] = {__dsub_rn(px, 1.0), __dsub_rn(py, 1.0), __dadd_rn(px, 1.0), __dadd_rn(py, 1.0)};
-    if (collides_listed(L, C, o)) {
+    if (collides_listed(L, C, T, o)) {
         sq[0] = o[0]; sq[1] = o[1]; sq[2] = o[2]; sq[3] = o[3];
         return 0;
     }
     const double in2[4] = {__dsub_rn(px, 2.0), __dsub_rn(py, 2.0), __dadd_rn(px, 2.0),
                            __dadd_rn(py, 2.0)};
-    if (collides_listed(L, C, in2)) {
+    if (collides_listed(L, C, T, in2)) {
         sq[0] = in2[0]; sq[1] = in2[1]; sq[2] = in2[2]; sq[3] = in2[3];
         return 0;
     }
@@ -178,7 +202,7 @@ __device__ __forceinline__ uint32_t replay_square(const DevLayout &L, const Cand
     bool maxReached = false, isc;
     uint32_t st = 0;
     int it = 0;
-    while ((isc = collides_listed(L, C, o)) || !maxReached || dist > kMinDist) {
+    while ((isc = collides_listed(L, C, T, o)) || !maxReached || dist > kMinDist) {
         if (isc) {
             if (dist > kMinDist) dist = __ddiv_rn(dist, 2.0);
             maxReached = true;
