@@ -1,0 +1,57 @@
+// cv.cuh -- declarations of the learned control variate (cv.cu).
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include "frw_internal.h"
+
+namespace frw {
+namespace cv {
+
+// MLP 16 -> 64 -> 64 -> 1, SiLU.  FP32 master parameters, packed:
+constexpr int kIn = 16, kHid = 64;
+constexpr int oW1 = 0;                   // [64][16]  (out, in)
+constexpr int oB1 = oW1 + kHid * kIn;    // [64]
+constexpr int oW2 = oB1 + kHid;          // [64][64]  (out, in)
+constexpr int oB2 = oW2 + kHid * kHid;   // [64]
+constexpr int oW3 = oB2 + kHid;          // [64]
+constexpr int oB3 = oW3 + kHid;          // [1]
+constexpr int kParams = oB3 + 1;         // 5313
+constexpr int kRowsPerBlock = 64;        // training chunk: 4 warps x 16 rows
+
+// Device copy of the network: FP32 master + BF16 operand copies.
+struct Net {
+    float *p = nullptr;          // [kParams] master
+    __nv_bfloat16 *w1 = nullptr; // [64][16]
+    __nv_bfloat16 *w2 = nullptr; // [64][64]
+    __nv_bfloat16 *w2t = nullptr;// [64][64] transposed (in, out)
+};
+
+frw_status net_alloc(Net *n, cudaStream_t st);
+void net_free(Net *n);
+frw_status net_upload(Net *n, const float *host_params, cudaStream_t st);
+frw_status net_refresh_bf16(const Net &n, cudaStream_t st);
+
+// features of points p (first-hop points) w.r.t. a target rect: the
+// (dx, dy) from p to the nearest point of each edge of the target and of
+// the nearest other conductor, divided by a0 and clamped to [-16, 16].
+frw_status launch_features(const DevLayout &L, double4 target_rect, int target_id, const double4 *rec,
+                           int64_t n, __nv_bfloat16 *xb, float *xf, cudaStream_t st);
+frw_status launch_forward(const Net &n, const __nv_bfloat16 *x, int64_t rows, float *out, cudaStream_t st);
+// grad += d/dparams sum_r wt_r (f(x_r) - y_r)^2 * inv_wsum ; loss += same sum
+frw_status launch_train_grad(const Net &n, const __nv_bfloat16 *x, const float *y, const float *wt, int64_t rows,
+                             float inv_wsum, float *grad, double *loss, cudaStream_t st);
+frw_status launch_adam(const Net &n, float *grad, float *m, float *v, int *step, float lr, cudaStream_t st);
+// per walk: z = c (1{end==target} - phi); w = c 1{end==target}; sums of z, z^2, w, w^2
+frw_status launch_cv_reduce(const int64_t *end, const double4 *rec, const float *phi, int64_t n, int target,
+                            double *sums /*4*/, cudaStream_t st);
+// exact mean: points and weights of the first-hop distribution on the grid start
+frw_status launch_quad_points(const DevLayout &L, const double4 *gauss, uint32_t Q, const double *pi_exact,
+                              const double *wx, const double *wy, double eps, bool exact_perimeter,
+                              double4 *rec /*Q*200: p1x, p1y, a0, weight*/, cudaStream_t st);
+frw_status launch_weighted_sum(const double4 *rec, const float *phi, int64_t n, double *sum, cudaStream_t st);
+frw_status launch_targets(const int64_t *end, const double4 *rec, int64_t n, int target, float *y, float *wt,
+                          double *wsum, cudaStream_t st);
+
+}  // namespace cv
+}  // namespace frw

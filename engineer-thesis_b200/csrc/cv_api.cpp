@@ -1,0 +1,507 @@
+// cv_api.cpp -- C ABI of the learned control variate (host side).
+//
+// frw_cv_train: walks from an independent seed give training pairs
+// (features of the first-hop point, 1{walk ends on the target}, weight c^2);
+// the MLP is fitted on the device (fused forward+backward + Adam, the whole
+// loop captured once in a CUDA graph); then the exact mean E[c*phi] is summed
+// over the grid start x first-hop bins.  frw_cv_walk: walks + features +
+// inference + reduction, giving the plain and the control-variate estimate of
+// C_tt side by side from the same walks.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "cv.cuh"
+#include "frw_internal.h"
+
+struct frw_cv {
+    const frw_layout *layout = nullptr;
+    int64_t target = 0;
+    frw_opts opts{};
+    frw::LayoutView view{};
+    frw::cv::Net net;
+    double mean_term = 0.0, train_loss = 0.0, train_ms = 0.0, quad_ms = 0.0;
+    uint64_t train_walks = 0;
+    uint32_t quad_points = 0;
+};
+
+namespace frw {
+namespace {
+
+struct Buf {
+    std::vector<void *> p;
+    cudaStream_t st;
+    explicit Buf(cudaStream_t s) : st(s) {}
+    template <typename T>
+    cudaError_t get(T **x, size_t bytes) {
+        cudaError_t e = cudaMallocAsync((void **)x, bytes ? bytes : 16, st);
+        if (e == cudaSuccess) p.push_back(*x);
+        return e;
+    }
+    ~Buf() {
+        for (void *q : p) cudaFreeAsync(q, st);
+    }
+};
+
+struct SetDevice {
+    int prev = -1;
+    explicit SetDevice(int d) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != d) cudaSetDevice(d);
+    }
+    ~SetDevice() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+bool pow2(uint32_t q) { return q && !(q & (q - 1)); }
+
+// Exact probability of bin i under the 32-bit uniform u = x 2^-32 and the
+// CDF search of the walk: #{x : intg[i] <= x 2^-32 < intg[i+1]} / 2^32.
+void exact_bin_probs(double *pi) {
+    double g[FRW_NSAMPLE], intg[FRW_NSAMPLE + 1];
+    green_tables(g, intg, nullptr, nullptr);
+    for (int i = 0; i < FRW_NSAMPLE; i++)
+        pi[i] = (ceil(ldexp(intg[i + 1], 32)) - ceil(ldexp(intg[i], 32))) / 4294967296.0;
+}
+
+void init_params(uint64_t seed, float *p) {
+    uint64_t s = seed ^ 0x5DEECE66Dull;
+    auto unif = [&]() {
+        uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        return (double)(z >> 11) * 0x1p-53 * 2.0 - 1.0;
+    };
+    memset(p, 0, sizeof(float) * cv::kParams);
+    const double a1 = sqrt(6.0 / (cv::kIn + cv::kHid)), a2 = sqrt(6.0 / (2 * cv::kHid)),
+                 a3 = sqrt(6.0 / (cv::kHid + 1));
+    for (int i = 0; i < cv::kHid * cv::kIn; i++) p[cv::oW1 + i] = (float)(a1 * unif());
+    for (int i = 0; i < cv::kHid * cv::kHid; i++) p[cv::oW2 + i] = (float)(a2 * unif());
+    for (int i = 0; i < cv::kHid; i++) p[cv::oW3 + i] = (float)(a3 * unif());
+    p[cv::oB3] = 0.5f;
+}
+
+frw_status check_cv_walk_opts(const frw_opts &o) {
+    frw_status rc = check_opts(&o);
+    if (rc) return rc;
+    if (o.start_mode != FRW_START_UNIFORM || !pow2(o.start_grid) || o.hop_cap < 2) {
+        set_error("control variate: needs FRW_START_UNIFORM, start_grid a power of two and hop_cap >= 2");
+        return FRW_E_ARG;
+    }
+    return FRW_OK;
+}
+
+}  // namespace
+}  // namespace frw
+
+using namespace frw;
+
+extern "C" {
+
+void frw_cv_opts_default(frw_cv_opts *o) {
+    memset(o, 0, sizeof(*o));
+    o->struct_size = sizeof(frw_cv_opts);
+    o->train_walks = 1000000;
+    o->train_seed = 0x7E57C0DEull;
+    o->epochs = 4;
+    o->batch = 8192;
+    o->lr = 3e-3f;
+}
+
+frw_status frw_cv_train(const frw_layout *layout, int64_t target, const frw_opts *walk_opts,
+                        const frw_cv_opts *cv_opts, frw_cv **out, void *stream) {
+    if (!layout || !walk_opts || !out) {
+        set_error("frw_cv_train: null argument");
+        return FRW_E_ARG;
+    }
+    *out = nullptr;
+    frw_cv_opts co;
+    frw_cv_opts_default(&co);
+    if (cv_opts) co = *cv_opts;
+    if (co.struct_size != sizeof(frw_cv_opts) || co.train_walks < 64 || co.epochs < 1 || co.batch < 64 ||
+        co.batch % 64 || !(co.lr > 0)) {
+        set_error("frw_cv_train: bad frw_cv_opts");
+        return FRW_E_ARG;
+    }
+    frw_status rc = check_cv_walk_opts(*walk_opts);
+    if (rc) return rc;
+    LayoutView v;
+    rc = layout_view(layout, &v);
+    if (rc) return rc;
+    if (target < 0 || target >= v.n) {
+        set_error("frw_cv_train: target out of range");
+        return FRW_E_ARG;
+    }
+    SetDevice sd(v.device);
+    const double *tables;
+    int sms;
+    rc = device_tables(v.device, &tables, &sms);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    frw_cv *M = new frw_cv();
+    M->layout = layout;
+    M->target = target;
+    M->opts = *walk_opts;
+    M->view = v;
+    M->train_walks = co.train_walks;
+    auto fail = [&](frw_status r) {
+        cv::net_free(&M->net);
+        delete M;
+        return r;
+    };
+    cudaEvent_t e0, e1, e2;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventCreate(&e2);
+    const int64_t N = (int64_t)co.train_walks;
+    {
+        Buf B(st);
+        int64_t *d_end;
+        double4 *d_rec;
+        __nv_bfloat16 *d_x;
+        float *d_y, *d_wt, *d_grad, *d_m, *d_v;
+        double *d_wsum, *d_loss;
+        int *d_step;
+        const int steps_per_epoch = (int)((N + co.batch - 1) / co.batch);
+        const int steps = steps_per_epoch * co.epochs;
+        cudaError_t e = cudaSuccess;
+        if (e == cudaSuccess) e = B.get(&d_end, N * 8);
+        if (e == cudaSuccess) e = B.get(&d_rec, N * 32);
+        if (e == cudaSuccess) e = B.get(&d_x, N * 32);
+        if (e == cudaSuccess) e = B.get(&d_y, N * 4);
+        if (e == cudaSuccess) e = B.get(&d_wt, N * 4);
+        if (e == cudaSuccess) e = B.get(&d_grad, cv::kParams * 4);
+        if (e == cudaSuccess) e = B.get(&d_m, cv::kParams * 4);
+        if (e == cudaSuccess) e = B.get(&d_v, cv::kParams * 4);
+        if (e == cudaSuccess) e = B.get(&d_wsum, 8);
+        if (e == cudaSuccess) e = B.get(&d_loss, (size_t)steps * 8);
+        if (e == cudaSuccess) e = B.get(&d_step, 4);
+        if (e != cudaSuccess) return fail(cuda_fail(e, "frw_cv_train: allocation"));
+        cudaEventRecord(e0, st);
+        rc = walk_records(layout, target, 0, (uint64_t)N, co.train_seed, *walk_opts, st, d_end, d_rec);
+        if (rc) return fail(rc);
+        const double *r = v.rects + 4 * target;
+        const double4 trect = make_double4(r[0], r[1], r[2], r[3]);
+        rc = cv::launch_features(v.dl, trect, (int)target, d_rec, N, d_x, nullptr, st);
+        if (!rc) {
+            cudaMemsetAsync(d_wsum, 0, 8, st);
+            rc = cv::launch_targets(d_end, d_rec, N, (int)target, d_y, d_wt, d_wsum, st);
+        }
+        if (rc) return fail(rc);
+        double wsum = 0.0;
+        e = cudaMemcpyAsync(&wsum, d_wsum, 8, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return fail(cuda_fail(e, "frw_cv_train: training set"));
+        if (!(wsum > 0)) {
+            set_error("frw_cv_train: no training walk has a first hop");
+            return fail(FRW_E_ARG);
+        }
+        std::vector<float> h(cv::kParams);
+        init_params(co.train_seed, h.data());
+        rc = cv::net_alloc(&M->net, st);
+        if (!rc) rc = cv::net_upload(&M->net, h.data(), st);
+        if (rc) return fail(rc);
+        cudaMemsetAsync(d_grad, 0, cv::kParams * 4, st);
+        cudaMemsetAsync(d_m, 0, cv::kParams * 4, st);
+        cudaMemsetAsync(d_v, 0, cv::kParams * 4, st);
+        cudaMemsetAsync(d_loss, 0, (size_t)steps * 8, st);
+        cudaMemsetAsync(d_step, 0, 4, st);
+        // the training loop, captured once and replayed as one graph
+        cudaStream_t cs;
+        e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return fail(cuda_fail(e, "stream"));
+        cudaEvent_t ready;
+        cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
+        cudaEventRecord(ready, st);
+        cudaStreamWaitEvent(cs, ready, 0);
+        e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        const double scale = (double)N / wsum;  // per-batch normalisation of the weighted MSE
+        for (int s = 0; s < steps && e == cudaSuccess && !rc; s++) {
+            const int64_t start = (int64_t)(s % steps_per_epoch) * co.batch;
+            const int64_t rows = std::min<int64_t>(co.batch, N - start);
+            const float inv = (float)(scale / (double)rows);
+            rc = cv::launch_train_grad(M->net, d_x + 16 * start, d_y + start, d_wt + start, rows, inv, d_grad,
+                                       d_loss + s, cs);
+            if (!rc) rc = cv::launch_adam(M->net, d_grad, d_m, d_v, d_step, co.lr, cs);
+        }
+        cudaGraph_t graph = nullptr;
+        cudaError_t e2c = cudaStreamEndCapture(cs, &graph);
+        if (e == cudaSuccess) e = e2c;
+        cudaGraphExec_t exec = nullptr;
+        if (e == cudaSuccess && !rc) e = cudaGraphInstantiate(&exec, graph, 0);
+        if (e == cudaSuccess && !rc) e = cudaGraphLaunch(exec, cs);
+        if (e == cudaSuccess && !rc) e = cudaStreamSynchronize(cs);
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        cudaStreamDestroy(cs);
+        cudaEventDestroy(ready);
+        if (rc) return fail(rc);
+        if (e != cudaSuccess) return fail(cuda_fail(e, "frw_cv_train: training graph"));
+        cudaEventRecord(e1, st);
+        std::vector<double> losses(steps);
+        e = cudaMemcpyAsync(losses.data(), d_loss, (size_t)steps * 8, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return fail(cuda_fail(e, "frw_cv_train: loss read-back"));
+        double l = 0;
+        for (int s = steps - steps_per_epoch; s < steps; s++) l += losses[s];
+        M->train_loss = l / steps_per_epoch;
+    }
+    // exact mean of the control variate over the grid start x first-hop bins
+    {
+        Buf B(st);
+        const uint32_t Q = walk_opts->start_grid;
+        const int64_t nq = (int64_t)Q * FRW_NSAMPLE;
+        double4 *d_gauss, *d_tgt, *d_q;
+        __nv_bfloat16 *d_xq;
+        float *d_phi;
+        double *d_pi, *d_mu;
+        uint32_t *d_status;
+        cudaError_t e = cudaSuccess;
+        if (e == cudaSuccess) e = B.get(&d_gauss, 32);
+        if (e == cudaSuccess) e = B.get(&d_tgt, 32);
+        if (e == cudaSuccess) e = B.get(&d_q, nq * 32);
+        if (e == cudaSuccess) e = B.get(&d_xq, nq * 32);
+        if (e == cudaSuccess) e = B.get(&d_phi, nq * 4);
+        if (e == cudaSuccess) e = B.get(&d_pi, FRW_NSAMPLE * 8);
+        if (e == cudaSuccess) e = B.get(&d_mu, 8);
+        if (e == cudaSuccess) e = B.get(&d_status, 4);
+        if (e != cudaSuccess) return fail(cuda_fail(e, "frw_cv_train: quadrature allocation"));
+        double pi[FRW_NSAMPLE];
+        exact_bin_probs(pi);
+        const double *r = v.rects + 4 * target;
+        cudaMemcpyAsync(d_pi, pi, sizeof(pi), cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_tgt, r, 32, cudaMemcpyHostToDevice, st);
+        cudaMemsetAsync(d_mu, 0, 8, st);
+        cudaMemsetAsync(d_status, 0, 4, st);
+        rc = launch_gauss(v.dl, (const double *)d_tgt, 1, walk_opts->gauss_mode, walk_opts->gauss_param,
+                          (double *)d_gauss, d_status, st);
+        if (!rc)
+            rc = cv::launch_quad_points(v.dl, d_gauss, Q, d_pi, tables + FRW_NSAMPLE + 1, tables + 2 * FRW_NSAMPLE + 1,
+                                        walk_opts->permittivity, walk_opts->exact_perimeter != 0, d_q, st);
+        const double4 trect = make_double4(r[0], r[1], r[2], r[3]);
+        if (!rc) rc = cv::launch_features(v.dl, trect, (int)target, d_q, nq, d_xq, nullptr, st);
+        if (!rc) rc = cv::launch_forward(M->net, d_xq, nq, d_phi, st);
+        if (!rc) rc = cv::launch_weighted_sum(d_q, d_phi, nq, d_mu, st);
+        if (rc) return fail(rc);
+        uint32_t hs = 0;
+        e = cudaMemcpyAsync(&M->mean_term, d_mu, 8, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&hs, d_status, 4, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaEventRecord(e2, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return fail(cuda_fail(e, "frw_cv_train: quadrature"));
+        if (hs) {
+            set_error("frw_cv_train: a kernel reported an internal limit during the quadrature");
+            return fail(FRW_E_KERNEL);
+        }
+        M->quad_points = (uint32_t)nq;
+    }
+    float a = 0, b = 0;
+    cudaEventElapsedTime(&a, e0, e1);
+    cudaEventElapsedTime(&b, e1, e2);
+    M->train_ms = a;
+    M->quad_ms = b;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(e2);
+    *out = M;
+    return FRW_OK;
+}
+
+frw_status frw_cv_info_get(const frw_cv *M, frw_cv_info *info) {
+    if (!M || !info) {
+        set_error("null argument");
+        return FRW_E_ARG;
+    }
+    info->mean_term = M->mean_term;
+    info->train_loss = M->train_loss;
+    info->train_ms = M->train_ms;
+    info->quad_ms = M->quad_ms;
+    info->train_walks = M->train_walks;
+    info->quad_points = M->quad_points;
+    return FRW_OK;
+}
+
+frw_status frw_cv_walk(const frw_cv *M, uint64_t walks, uint64_t seed, frw_cv_result *res, void *stream) {
+    if (!M || !res || walks < 2) {
+        set_error("frw_cv_walk: bad arguments");
+        return FRW_E_ARG;
+    }
+    SetDevice sd(M->view.device);
+    cudaStream_t st = (cudaStream_t)stream;
+    const uint64_t chunk = std::min<uint64_t>(walks, 1ull << 23);
+    Buf B(st);
+    int64_t *d_end;
+    double4 *d_rec;
+    __nv_bfloat16 *d_x;
+    float *d_phi;
+    double *d_sums;
+    cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = B.get(&d_end, chunk * 8);
+    if (e == cudaSuccess) e = B.get(&d_rec, chunk * 32);
+    if (e == cudaSuccess) e = B.get(&d_x, chunk * 32);
+    if (e == cudaSuccess) e = B.get(&d_phi, chunk * 4);
+    if (e == cudaSuccess) e = B.get(&d_sums, 32);
+    if (e != cudaSuccess) return cuda_fail(e, "frw_cv_walk: allocation");
+    cudaMemsetAsync(d_sums, 0, 32, st);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, st);
+    const double *r = M->view.rects + 4 * M->target;
+    const double4 trect = make_double4(r[0], r[1], r[2], r[3]);
+    frw_status rc = FRW_OK;
+    for (uint64_t first = 0; first < walks && !rc; first += chunk) {
+        const uint64_t n = std::min<uint64_t>(chunk, walks - first);
+        rc = walk_records(M->layout, M->target, first, n, seed, M->opts, st, d_end, d_rec);
+        if (!rc) rc = cv::launch_features(M->view.dl, trect, (int)M->target, d_rec, (int64_t)n, d_x, nullptr, st);
+        if (!rc) rc = cv::launch_forward(M->net, d_x, (int64_t)n, d_phi, st);
+        if (!rc) rc = cv::launch_cv_reduce(d_end, d_rec, d_phi, (int64_t)n, (int)M->target, d_sums, st);
+    }
+    cudaEventRecord(e1, st);
+    double h[4] = {0, 0, 0, 0};
+    if (!rc) {
+        e = cudaMemcpyAsync(h, d_sums, 32, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) rc = cuda_fail(e, "frw_cv_walk: read-back");
+    }
+    float ms = 0;
+    if (!rc) cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    const double N = (double)walks;
+    const double mz = h[0] / N, vz = std::max(h[1] / N - mz * mz, 0.0) * N / (N - 1);
+    const double mw = h[2] / N, vw = std::max(h[3] / N - mw * mw, 0.0) * N / (N - 1);
+    res->walks = walks;
+    res->plain = mw;
+    res->plain_se = sqrt(vw / N);
+    res->cv = mz + M->mean_term;
+    res->cv_se = sqrt(vz / N);
+    res->variance_ratio = vz > 0 ? vw / vz : 0.0;
+    res->kernel_ms = ms;
+    return FRW_OK;
+}
+
+frw_status frw_cv_destroy(frw_cv *M) {
+    if (!M) return FRW_OK;
+    SetDevice sd(M->view.device);
+    cv::net_free(&M->net);
+    delete M;
+    return FRW_OK;
+}
+
+frw_status frw_cv_params(const frw_cv *M, float *out) {
+    if (!M || !out) {
+        set_error("null argument");
+        return FRW_E_ARG;
+    }
+    SetDevice sd(M->view.device);
+    FRW_CK(cudaMemcpy(out, M->net.p, cv::kParams * sizeof(float), cudaMemcpyDeviceToHost));
+    return FRW_OK;
+}
+
+// ---- direct access to the MLP and feature kernels (host arrays) ----
+frw_status frw_mlp_forward(const float *params, const float *x, int64_t n, float *out, int device) {
+    if (!params || !x || !out || n <= 0) {
+        set_error("frw_mlp_forward: bad arguments");
+        return FRW_E_ARG;
+    }
+    const double *tables;
+    int sms;
+    frw_status rc = device_tables(device, &tables, &sms);
+    if (rc) return rc;
+    SetDevice sd(device);
+    cudaStream_t st = nullptr;
+    Buf B(st);
+    float *d_xf, *d_out;
+    __nv_bfloat16 *d_x;
+    FRW_CK(B.get(&d_xf, n * 64));
+    FRW_CK(B.get(&d_x, n * 32));
+    FRW_CK(B.get(&d_out, n * 4));
+    cv::Net net;
+    rc = cv::net_alloc(&net, st);
+    if (!rc) rc = cv::net_upload(&net, params, st);
+    if (!rc) {
+        FRW_CK(cudaMemcpyAsync(d_xf, x, n * 64, cudaMemcpyHostToDevice, st));
+        std::vector<__nv_bfloat16> hb((size_t)n * 16);
+        for (int64_t i = 0; i < n * 16; i++) hb[i] = __float2bfloat16_rn(x[i]);
+        FRW_CK(cudaMemcpyAsync(d_x, hb.data(), n * 32, cudaMemcpyHostToDevice, st));
+        rc = cv::launch_forward(net, d_x, n, d_out, st);
+        if (!rc) FRW_CK(cudaMemcpyAsync(out, d_out, n * 4, cudaMemcpyDeviceToHost, st));
+        if (!rc) FRW_CK(cudaStreamSynchronize(st));
+    }
+    cv::net_free(&net);
+    return rc;
+}
+
+frw_status frw_mlp_grad(const float *params, const float *x, const float *y, const float *wt, int64_t n,
+                        double inv_wsum, float *grad, double *loss, int device) {
+    if (!params || !x || !y || !wt || !grad || n <= 0) {
+        set_error("frw_mlp_grad: bad arguments");
+        return FRW_E_ARG;
+    }
+    const double *tables;
+    int sms;
+    frw_status rc = device_tables(device, &tables, &sms);
+    if (rc) return rc;
+    SetDevice sd(device);
+    cudaStream_t st = nullptr;
+    Buf B(st);
+    __nv_bfloat16 *d_x;
+    float *d_y, *d_wt, *d_g;
+    double *d_l;
+    FRW_CK(B.get(&d_x, n * 32));
+    FRW_CK(B.get(&d_y, n * 4));
+    FRW_CK(B.get(&d_wt, n * 4));
+    FRW_CK(B.get(&d_g, cv::kParams * 4));
+    FRW_CK(B.get(&d_l, 8));
+    cv::Net net;
+    rc = cv::net_alloc(&net, st);
+    if (!rc) rc = cv::net_upload(&net, params, st);
+    if (!rc) {
+        std::vector<__nv_bfloat16> hb((size_t)n * 16);
+        for (int64_t i = 0; i < n * 16; i++) hb[i] = __float2bfloat16_rn(x[i]);
+        FRW_CK(cudaMemcpyAsync(d_x, hb.data(), n * 32, cudaMemcpyHostToDevice, st));
+        FRW_CK(cudaMemcpyAsync(d_y, y, n * 4, cudaMemcpyHostToDevice, st));
+        FRW_CK(cudaMemcpyAsync(d_wt, wt, n * 4, cudaMemcpyHostToDevice, st));
+        FRW_CK(cudaMemsetAsync(d_g, 0, cv::kParams * 4, st));
+        FRW_CK(cudaMemsetAsync(d_l, 0, 8, st));
+        rc = cv::launch_train_grad(net, d_x, d_y, d_wt, n, (float)inv_wsum, d_g, d_l, st);
+        if (!rc) FRW_CK(cudaMemcpyAsync(grad, d_g, cv::kParams * 4, cudaMemcpyDeviceToHost, st));
+        if (!rc && loss) FRW_CK(cudaMemcpyAsync(loss, d_l, 8, cudaMemcpyDeviceToHost, st));
+        if (!rc) FRW_CK(cudaStreamSynchronize(st));
+    }
+    cv::net_free(&net);
+    return rc;
+}
+
+frw_status frw_cv_features(const frw_layout *layout, int64_t target, const double *rec4, int64_t n, float *out) {
+    LayoutView v;
+    frw_status rc = layout_view(layout, &v);
+    if (rc) return rc;
+    if (!rec4 || !out || n <= 0 || target < 0 || target >= v.n) {
+        set_error("frw_cv_features: bad arguments");
+        return FRW_E_ARG;
+    }
+    SetDevice sd(v.device);
+    cudaStream_t st = nullptr;
+    Buf B(st);
+    double4 *d_rec;
+    float *d_f;
+    FRW_CK(B.get(&d_rec, n * 32));
+    FRW_CK(B.get(&d_f, n * 64));
+    FRW_CK(cudaMemcpyAsync(d_rec, rec4, n * 32, cudaMemcpyHostToDevice, st));
+    const double *r = v.rects + 4 * target;
+    rc = cv::launch_features(v.dl, make_double4(r[0], r[1], r[2], r[3]), (int)target, d_rec, n, nullptr, d_f, st);
+    if (rc) return rc;
+    FRW_CK(cudaMemcpyAsync(out, d_f, n * 64, cudaMemcpyDeviceToHost, st));
+    FRW_CK(cudaStreamSynchronize(st));
+    return FRW_OK;
+}
+
+}  // extern "C"

@@ -72,6 +72,7 @@ struct WalkParams {
     int32_t start_mode;
     int32_t exact_perimeter;
     int32_t refill_min;
+    uint32_t start_grid;   // 0: continuous uniform start; Q: midpoints of Q equal arcs
     int64_t hop_cap;
     double permittivity;
     uint64_t seed;
@@ -89,6 +90,7 @@ struct WalkParams {
     int32_t *rec_hops;
     int32_t *rec_bin;
     double *rec_w;
+    double4 *rec_cv;  // optional: (first-hop point x, y, first square side a0, weight factor c)
     // tables
     const double *intg;  // [201]
     const double *wx;    // [200]
@@ -149,5 +151,8 @@ struct LayoutView {
 frw_status layout_view(const frw_layout *layout, LayoutView *out);
 frw_status device_tables(int device, const double **tables, int *sms);
 frw_status check_opts(const frw_opts *opts);
+// walks with per-walk end and (first-hop point, a0, weight factor) records (device arrays)
+frw_status walk_records(const frw_layout *layout, int64_t target, uint64_t first_walk, uint64_t walks,
+                        uint64_t seed, const frw_opts &o, cudaStream_t st, int64_t *rec_end, double4 *rec_cv);
 
 }  // namespace frw

@@ -319,4 +319,30 @@ __device__ __forceinline__ void point_from_index(const double s[4], int index, b
     }
 }
 
+// Uniform point on the Gaussian perimeter, clockwise from the top-left
+// corner; side code 0 top, 1 right, 2 bottom, 3 left (outward normals
+// (0,-1), (1,0), (0,1), (-1,0) in the layout's y-down axes).
+__device__ __forceinline__ int perimeter_point(const double G[4], double u, double &x, double &y) {
+    const double w = __dsub_rn(G[2], G[0]), h = __dsub_rn(G[3], G[1]);
+    const double s = __dmul_rn(u, __dadd_rn(__dmul_rn(2.0, w), __dmul_rn(2.0, h)));
+    if (s < w) {
+        x = __dadd_rn(G[0], s);
+        y = G[1];
+        return 0;
+    }
+    if (s < __dadd_rn(w, h)) {
+        x = G[2];
+        y = __dadd_rn(G[1], __dsub_rn(s, w));
+        return 1;
+    }
+    if (s < __dadd_rn(__dmul_rn(2.0, w), h)) {
+        x = __dsub_rn(G[2], __dsub_rn(__dsub_rn(s, w), h));
+        y = G[3];
+        return 2;
+    }
+    x = G[0];
+    y = __dsub_rn(G[3], __dsub_rn(__dsub_rn(s, __dmul_rn(2.0, w)), h));
+    return 3;
+}
+
 }  // namespace frw

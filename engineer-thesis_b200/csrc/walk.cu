@@ -78,32 +78,6 @@ __device__ __forceinline__ int bin_of(const double *s_intg, double u) {
     return lo;
 }
 
-// Uniform point on the Gaussian perimeter, clockwise from the top-left
-// corner; side code 0 top, 1 right, 2 bottom, 3 left (outward normals
-// (0,-1), (1,0), (0,1), (-1,0) in the layout's y-down axes).
-__device__ __forceinline__ int perimeter_point(const double G[4], double u, double &x, double &y) {
-    const double w = __dsub_rn(G[2], G[0]), h = __dsub_rn(G[3], G[1]);
-    const double s = __dmul_rn(u, __dadd_rn(__dmul_rn(2.0, w), __dmul_rn(2.0, h)));
-    if (s < w) {
-        x = __dadd_rn(G[0], s);
-        y = G[1];
-        return 0;
-    }
-    if (s < __dadd_rn(w, h)) {
-        x = G[2];
-        y = __dadd_rn(G[1], __dsub_rn(s, w));
-        return 1;
-    }
-    if (s < __dadd_rn(__dmul_rn(2.0, w), h)) {
-        x = __dsub_rn(G[2], __dsub_rn(__dsub_rn(s, w), h));
-        y = G[3];
-        return 2;
-    }
-    x = G[0];
-    y = __dsub_rn(G[3], __dsub_rn(__dsub_rn(s, __dmul_rn(2.0, w)), h));
-    return 3;
-}
-
 __device__ __forceinline__ void kahan_add(double &s, double &c, double v) {
     const double y = __dsub_rn(v, c);
     const double t = __dadd_rn(s, y);
@@ -203,7 +177,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(const WalkParams P) {
     uint4 rnd = make_uint4(0, 0, 0, 0);  // uniforms of hops (hop & ~3) .. +3
     int32_t hops = 0, bin1 = -1;
     int side = 0;
-    double px = 0, py = 0, a0 = 0, perim = 0;
+    double px = 0, py = 0, a0 = 0, perim = 0, p1x = 0, p1y = 0;
     double sq[4] = {0, 0, 0, 0};
     uint32_t st = 0;
 
@@ -249,8 +223,13 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(const WalkParams P) {
                     hops = 0;
                     bin1 = -1;
                     a0 = 0.0;
+                    p1x = p1y = 0.0;
                     rnd = draw_block(P.seed, stream, pw, 0);
-                    const double u = word_u(rnd, 0);
+                    double u = word_u(rnd, 0);
+                    if (P.start_grid) {  // midpoint of arc floor(u*Q) of Q equal arcs
+                        const uint32_t q = (uint32_t)__dmul_rn(u, (double)P.start_grid);
+                        u = __ddiv_rn(__dadd_rn((double)q, 0.5), (double)P.start_grid);
+                    }
                     if (uniform_start) {
                         side = perimeter_point(G, u, px, py);
                     } else {
@@ -282,31 +261,36 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(const WalkParams P) {
                     hop++;
                     if ((hop & 3) == 0) rnd = draw_block(P.seed, stream, pw, hop);
                     const int bin = bin_of(s_intg, word_u(rnd, hop));
+                    point_from_index(sq, bin, exact, px, py);
                     if (hop == 1) {
                         bin1 = bin;
                         a0 = __dsub_rn(sq[2], sq[0]);
+                        p1x = px;
+                        p1y = py;
                     }
-                    point_from_index(sq, bin, exact, px, py);
                 }
             }
         }
         const bool ended = active && code != 0x7FFFFFFF;
 
-        // ---- walk ends: weight, optional record, per-warp table ----
+        // ---- walk ends: weight, optional records, per-warp table ----
         double wgt = 0.0;
         if (ended) {
-            if (uniform_start && code >= 0 && bin1 >= 0) {
+            double c = 0.0;  // weight factor: counts for the end conductor only
+            if (uniform_start && bin1 >= 0) {
                 const double nx = side == 1 ? 1.0 : (side == 3 ? -1.0 : 0.0);
                 const double ny = side == 2 ? 1.0 : (side == 0 ? -1.0 : 0.0);
                 const double dot = __dadd_rn(__dmul_rn(s_wx[bin1], nx), __dmul_rn(s_wy[bin1], ny));
-                wgt = __ddiv_rn(__dmul_rn(__dmul_rn(-P.permittivity, perim), dot), a0);
+                c = __ddiv_rn(__dmul_rn(__dmul_rn(-P.permittivity, perim), dot), a0);
             }
+            if (code >= 0) wgt = c;
             if (P.rec_end) {
                 P.rec_end[gw] = code;
                 P.rec_hops[gw] = hops;
                 P.rec_bin[gw] = bin1;
-                P.rec_w[gw] = wgt;
+                P.rec_w[gw] = c;
             }
+            if (P.rec_cv) P.rec_cv[gw] = make_double4(p1x, p1y, a0, c);
             active = false;
         }
         const unsigned em = __ballot_sync(kFull, ended);

@@ -57,6 +57,7 @@ class Opts(C.Structure):
         ("threads_per_block", C.c_int32),
         ("blocks_per_sm", C.c_int32),
         ("refill_min", C.c_int32),
+        ("start_grid", C.c_uint32),
     ]
 
 
@@ -77,6 +78,40 @@ class Result(C.Structure):
         ("cap_se", C.POINTER(C.c_double)),
         ("sum_w", C.POINTER(C.c_double)),
         ("sum_w2", C.POINTER(C.c_double)),
+    ]
+
+
+class CvOpts(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_uint32),
+        ("train_walks", C.c_uint64),
+        ("train_seed", C.c_uint64),
+        ("epochs", C.c_int32),
+        ("batch", C.c_int32),
+        ("lr", C.c_float),
+    ]
+
+
+class CvInfo(C.Structure):
+    _fields_ = [
+        ("mean_term", C.c_double),
+        ("train_loss", C.c_double),
+        ("train_ms", C.c_double),
+        ("quad_ms", C.c_double),
+        ("train_walks", C.c_uint64),
+        ("quad_points", C.c_uint32),
+    ]
+
+
+class CvResult(C.Structure):
+    _fields_ = [
+        ("walks", C.c_uint64),
+        ("plain", C.c_double),
+        ("plain_se", C.c_double),
+        ("cv", C.c_double),
+        ("cv_se", C.c_double),
+        ("variance_ratio", C.c_double),
+        ("kernel_ms", C.c_double),
     ]
 
 
@@ -121,7 +156,17 @@ _SIGS = {
                          C.c_int),
     "frw_generate_layout": ([C.c_uint64, C.c_int64, C.c_double, C.c_int32, C.c_int32, C.c_double, _F], C.c_int),
     "frw_write_layout": ([C.c_char_p, _F, C.c_int64, C.c_char_p], C.c_int),
+    "frw_cv_opts_default": ([C.POINTER(CvOpts)], None),
+    "frw_cv_train": ([_VP, C.c_int64, C.POINTER(Opts), C.POINTER(CvOpts), C.POINTER(_VP), _VP], C.c_int),
+    "frw_cv_info_get": ([_VP, C.POINTER(CvInfo)], C.c_int),
+    "frw_cv_walk": ([_VP, C.c_uint64, C.c_uint64, C.POINTER(CvResult), _VP], C.c_int),
+    "frw_cv_destroy": ([_VP], C.c_int),
+    "frw_cv_params": ([_VP, _F], C.c_int),
+    "frw_mlp_forward": ([_F, _F, C.c_int64, _F, C.c_int], C.c_int),
+    "frw_mlp_grad": ([_F, _F, _F, _F, C.c_int64, C.c_double, _F, _D, C.c_int], C.c_int),
+    "frw_cv_features": ([_VP, C.c_int64, _D, C.c_int64, _F], C.c_int),
 }
+CV_PARAMS = 5313
 
 _lib = None
 
@@ -167,7 +212,8 @@ def green_table():
 
 
 def opts(gauss_mode=GAUSS_SCALE, gauss_param=1.5, start_mode=START_GREEN, exact_perimeter=False,
-         hop_cap=100000, stream_id=0, blocks_per_sm=0, refill_min=1, permittivity=PERMITTIVITY) -> Opts:
+         hop_cap=100000, stream_id=0, blocks_per_sm=0, refill_min=1, permittivity=PERMITTIVITY,
+         start_grid=0) -> Opts:
     o = Opts()
     lib().frw_opts_default(C.byref(o))
     o.gauss_mode = gauss_mode
@@ -179,6 +225,7 @@ def opts(gauss_mode=GAUSS_SCALE, gauss_param=1.5, start_mode=START_GREEN, exact_
     o.blocks_per_sm = blocks_per_sm
     o.refill_min = refill_min
     o.permittivity = permittivity
+    o.start_grid = start_grid
     return o
 
 
@@ -335,6 +382,12 @@ class Layout:
         return WalkResult(r.walks, r.escaped, r.aborted, r.hops_total, np.array(r.gauss[:]), r.fraction_other,
                           r.kernel_ms, cond[:m], hits[:m], c[:m], se[:m], s1[:m], s2[:m])
 
+    def cv_features(self, target: int, rec4) -> np.ndarray:
+        q = np.ascontiguousarray(rec4, dtype=np.float64).reshape(-1, 4)
+        out = np.zeros((len(q), 16), dtype=np.float32)
+        _check(lib().frw_cv_features(self._h, target, _ptr(q, _D), len(q), _ptr(out, _F)))
+        return out
+
     def walk_trace(self, target: int, first: int, walks: int, seed: int, o: Opts | None = None):
         end = np.zeros(walks, dtype=np.int64)
         hops = np.zeros(walks, dtype=np.int32)
@@ -343,6 +396,72 @@ class Layout:
         _check(lib().frw_walk_trace(self._h, target, first, walks, seed, C.byref(o) if o else None, _ptr(end),
                                     _ptr(hops), _ptr(b1), _ptr(w), MEM_HOST, None))
         return end, hops, b1, w
+
+
+def cv_opts(train_walks=1_000_000, train_seed=0x7E57C0DE, epochs=4, batch=8192, lr=3e-3) -> CvOpts:
+    o = CvOpts()
+    lib().frw_cv_opts_default(C.byref(o))
+    o.train_walks, o.train_seed, o.epochs, o.batch, o.lr = train_walks, train_seed, epochs, batch, lr
+    return o
+
+
+class ControlVariate:
+    """frw_cv: a trained control variate for C_tt of one layout and target."""
+
+    def __init__(self, layout: "Layout", target: int, walk_opts: Opts, opts: CvOpts | None = None):
+        self._layout = layout  # keeps the layout alive
+        self._o = walk_opts
+        h = _VP()
+        _check(lib().frw_cv_train(layout._h, target, C.byref(walk_opts), C.byref(opts) if opts else None,
+                                  C.byref(h), None))
+        self._h = h
+
+    @property
+    def info(self) -> CvInfo:
+        i = CvInfo()
+        _check(lib().frw_cv_info_get(self._h, C.byref(i)))
+        return i
+
+    def walk(self, walks: int, seed: int) -> CvResult:
+        r = CvResult()
+        _check(lib().frw_cv_walk(self._h, walks, seed, C.byref(r), None))
+        return r
+
+    def params(self) -> np.ndarray:
+        out = np.zeros(CV_PARAMS, dtype=np.float32)
+        _check(lib().frw_cv_params(self._h, _ptr(out, _F)))
+        return out
+
+    def close(self):
+        if self._h:
+            lib().frw_cv_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def mlp_forward(params, x, device: int = 0) -> np.ndarray:
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    xx = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, 16)
+    out = np.zeros(len(xx), dtype=np.float32)
+    _check(lib().frw_mlp_forward(_ptr(p, _F), _ptr(xx, _F), len(xx), _ptr(out, _F), device))
+    return out
+
+
+def mlp_grad(params, x, y, wt, inv_wsum: float, device: int = 0):
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    xx = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, 16)
+    yy = np.ascontiguousarray(y, dtype=np.float32)
+    ww = np.ascontiguousarray(wt, dtype=np.float32)
+    g = np.zeros(CV_PARAMS, dtype=np.float32)
+    loss = C.c_double()
+    _check(lib().frw_mlp_grad(_ptr(p, _F), _ptr(xx, _F), _ptr(yy, _F), _ptr(ww, _F), len(xx), inv_wsum, _ptr(g, _F),
+                              C.byref(loss), device))
+    return loss.value, g
 
 
 def get_avg_path_len_cuda(path: str, iter_num: int, rect_id: int, layer: int = 0, seed: int = 0, device: int = 0,

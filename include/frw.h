@@ -138,6 +138,9 @@ typedef struct frw_opts {
     int32_t threads_per_block;
     int32_t blocks_per_sm;
     int32_t refill_min;      /* refill a warp only when at least this many lanes are idle */
+    uint32_t start_grid;     /* uniform start only: 0 = continuous; Q > 0 = the Q midpoints of Q equal
+                                arcs of the Gaussian perimeter (the start distribution a control
+                                variate's exact mean is summed over) */
 } frw_opts;
 void frw_opts_default(frw_opts *opts);
 
@@ -171,7 +174,10 @@ frw_status frw_walk(const frw_layout *layout, int64_t target, uint64_t walks, ui
 
 /* Same walks with per-walk records (device or host arrays of `walks`
  * entries; any may be NULL): end conductor (layer index, -1 escaped,
- * -2 aborted), hop count, first-hop bin and capacitance weight.  The
+ * -2 aborted), hop count, first-hop bin and the walk's capacitance weight
+ * factor c = -eps*L*(W_bin . n)/a0 (0 without a first hop or in green-start
+ * mode); the walk adds c to the conductor in `end` and nothing when it
+ * escaped or was aborted.  The
  * reference's randomWalkCudaWrapper output pair (0/1 "other" flag and hit
  * rect) is derived from `end`. */
 frw_status frw_walk_trace(const frw_layout *layout, int64_t target, uint64_t first_walk,
@@ -208,6 +214,62 @@ frw_status frw_gauss_surface(const frw_layout *layout, int64_t target, const frw
  * hist_path in the reference's "<ts>wyniki.txt" format when not NULL. */
 frw_status frw_avg_path_len(const char *path, int64_t iter_num, int64_t rect_id, int layer,
                             uint64_t seed, int device, const char *hist_path, double *fraction);
+
+/* ---- learned control variate (no reference counterpart) ----
+ * For C_tt the walk estimate is w = c * 1{end = t} (c: first-hop weight
+ * factor).  The control variate is f = c * phi(x1), phi an MLP (16 -> 64 ->
+ * 64 -> 1, SiLU; BF16 tensor-core kernels with FP32 accumulation) of 16
+ * edge features of the first-hop point x1: (dx, dy) to the nearest point of
+ * each edge of the target and of the nearest other conductor, divided by the
+ * first square's side, clamped to +-16.  It is trained on the device on
+ * walks of an independent seed (weighted least squares, weight c^2, Adam),
+ * and E[f] is summed exactly over the start grid (opts.start_grid = Q, a
+ * power of two) x the 200 first-hop bins, so  mean(w - f) + E[f]  is an
+ * unbiased estimate of C_tt; frw_cv_walk reports it next to the plain
+ * estimate from the same walks. */
+typedef struct frw_cv frw_cv;
+typedef struct frw_cv_opts {
+    uint32_t struct_size;  /* sizeof(frw_cv_opts) */
+    uint64_t train_walks;  /* walks generating training pairs (default 1e6) */
+    uint64_t train_seed;   /* independent of the estimation seed */
+    int32_t epochs;        /* passes over the training pairs (default 4) */
+    int32_t batch;         /* rows per Adam step, a multiple of 64 (default 8192) */
+    float lr;              /* Adam step size (default 3e-3) */
+} frw_cv_opts;
+void frw_cv_opts_default(frw_cv_opts *opts);
+typedef struct frw_cv_info {
+    double mean_term;      /* E[f], exact over start grid x first-hop bins */
+    double train_loss;     /* weighted MSE over the last epoch */
+    double train_ms;       /* training walks + features + fit (device time) */
+    double quad_ms;        /* exact-mean sum (device time) */
+    uint64_t train_walks;
+    uint32_t quad_points;  /* Q * 200 */
+} frw_cv_info;
+typedef struct frw_cv_result {
+    uint64_t walks;
+    double plain, plain_se;  /* C_tt from the plain estimator */
+    double cv, cv_se;        /* C_tt with the control variate */
+    double variance_ratio;   /* plain variance / control-variate variance */
+    double kernel_ms;        /* device time of walks + features + inference + sums */
+} frw_cv_result;
+/* walk_opts must use FRW_START_UNIFORM with start_grid a power of two. */
+frw_status frw_cv_train(const frw_layout *layout, int64_t target, const frw_opts *walk_opts,
+                        const frw_cv_opts *cv_opts, frw_cv **out, void *stream);
+frw_status frw_cv_info_get(const frw_cv *cv, frw_cv_info *info);
+frw_status frw_cv_walk(const frw_cv *cv, uint64_t walks, uint64_t seed, frw_cv_result *result,
+                       void *stream);
+frw_status frw_cv_destroy(frw_cv *cv);
+#define FRW_CV_PARAMS 5313 /* W1[64][16] b1[64] W2[64][64] b2[64] w3[64] b3 */
+frw_status frw_cv_params(const frw_cv *cv, float *out);
+/* The MLP and feature kernels on host arrays (FP32 in, BF16 operands on the
+ * device): forward outputs, and the gradient of
+ * sum_r wt_r (f(x_r) - y_r)^2 * inv_wsum with the summed loss. */
+frw_status frw_mlp_forward(const float *params, const float *x, int64_t n, float *out, int device);
+frw_status frw_mlp_grad(const float *params, const float *x, const float *y, const float *wt, int64_t n,
+                        double inv_wsum, float *grad, double *loss, int device);
+/* features of points rec4 = n x (x, y, a0, unused) relative to `target` */
+frw_status frw_cv_features(const frw_layout *layout, int64_t target, const double *rec4, int64_t n,
+                           float *out);
 
 /* ---- synthetic layouts ---- */
 /* Seeded generator of the benchmark layouts: n rects with integer corners in

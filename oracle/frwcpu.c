@@ -767,7 +767,7 @@ static double draw(uint64_t seed, uint32_t stream, uint64_t walk, uint32_t hop) 
  * first-hop bin, n = outward normal of the Gaussian side at p0). */
 int oc_walk_run(const oc_grid *g, const double *rects, const oc_walk_cfg *cfg, uint64_t first,
                 uint64_t count, int64_t *end_out, int32_t *hops_out, int32_t *bin_out,
-                double *weight_out) {
+                double *weight_out, double *cv_out) {
     double gtab[OC_NSAMPLE], intg[OC_NSAMPLE + 1], wx[OC_NSAMPLE], wy[OC_NSAMPLE];
     oc_green_table(OC_NSAMPLE, gtab, intg);
     oc_weight_table(OC_NSAMPLE, intg, wx, wy);
@@ -780,6 +780,10 @@ int oc_walk_run(const oc_grid *g, const double *rects, const oc_walk_cfg *cfg, u
         uint32_t hop = 0;
         u0 = draw(cfg->seed, cfg->stream, w, hop);
         if (cfg->start_mode == OC_START_UNIFORM) {
+            if (cfg->start_grid) {
+                uint32_t q = (uint32_t)(u0 * (double)cfg->start_grid);
+                u0 = ((double)q + 0.5) / (double)cfg->start_grid;
+            }
             perimeter_point(G, u0, p, nrm);
         } else {
             oc_point_from_index(G, oc_bin_index(intg, OC_NSAMPLE, u0), OC_NSAMPLE,
@@ -787,7 +791,7 @@ int oc_walk_run(const oc_grid *g, const double *rects, const oc_walk_cfg *cfg, u
         }
         int64_t end;
         int32_t hops = 0, bin1 = -1;
-        double a0 = 0.0;
+        double a0 = 0.0, p1[2] = {0.0, 0.0};
         for (;;) {
             if (!pt_in(g->b, p[0], p[1])) { end = OC_END_ESCAPED; break; }
             oc_grid_biggest_square(g, p[0], p[1], sq);
@@ -798,16 +802,22 @@ int oc_walk_run(const oc_grid *g, const double *rects, const oc_walk_cfg *cfg, u
             hop++;
             u0 = draw(cfg->seed, cfg->stream, w, hop);
             int bin = oc_bin_index(intg, OC_NSAMPLE, u0);
-            if (hop == 1) { bin1 = bin; a0 = sq[2] - sq[0]; }
             oc_point_from_index(sq, bin, OC_NSAMPLE, cfg->exact_perimeter, p);
+            if (hop == 1) { bin1 = bin; a0 = sq[2] - sq[0]; p1[0] = p[0]; p1[1] = p[1]; }
         }
-        double wgt = 0.0;
-        if (cfg->start_mode == OC_START_UNIFORM && bin1 >= 0 && end >= 0)
-            wgt = -cfg->permittivity * L * (wx[bin1] * nrm[0] + wy[bin1] * nrm[1]) / a0;
+        double c = 0.0;
+        if (cfg->start_mode == OC_START_UNIFORM && bin1 >= 0)
+            c = -cfg->permittivity * L * (wx[bin1] * nrm[0] + wy[bin1] * nrm[1]) / a0;
         end_out[k] = end;
         hops_out[k] = hops;
         bin_out[k] = bin1;
-        weight_out[k] = wgt;
+        weight_out[k] = c;
+        if (cv_out) {
+            cv_out[4 * k] = p1[0];
+            cv_out[4 * k + 1] = p1[1];
+            cv_out[4 * k + 2] = a0;
+            cv_out[4 * k + 3] = c;
+        }
     }
     return OC_OK;
 }
@@ -838,4 +848,48 @@ int64_t oc_walk_stream(const oc_grid *g, const oc_rtree *t, int defect, const do
     *used = k;
     *hops = h;
     return end;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Control-variate features (brute force over all rects)                    */
+/* ------------------------------------------------------------------------ */
+static float cv_feat(double d, double a0) {
+    double v = d / a0;
+    v = fmin(fmax(v, -16.0), 16.0);
+    return (float)v;
+}
+
+static void cv_edges(double px, double py, const double *r, double a0, float *f) {
+    double cx = fmin(fmax(px, r[0]), r[2]), cy = fmin(fmax(py, r[1]), r[3]);
+    f[0] = cv_feat(cx - px, a0);
+    f[1] = cv_feat(r[1] - py, a0);
+    f[2] = cv_feat(r[2] - px, a0);
+    f[3] = cv_feat(cy - py, a0);
+    f[4] = cv_feat(cx - px, a0);
+    f[5] = cv_feat(r[3] - py, a0);
+    f[6] = cv_feat(r[0] - px, a0);
+    f[7] = cv_feat(cy - py, a0);
+}
+
+void oc_cv_features(const double *rects, int64_t n, int64_t target, const double *rec4, int64_t m,
+                    float *out) {
+    for (int64_t i = 0; i < m; i++) {
+        double px = rec4[4 * i], py = rec4[4 * i + 1], a0 = rec4[4 * i + 2];
+        float *f = out + 16 * i;
+        if (!(a0 > 0.0)) {
+            for (int q = 0; q < 16; q++) f[q] = 0.f;
+            continue;
+        }
+        cv_edges(px, py, rects + 4 * target, a0, f);
+        int64_t bk = -1;
+        double best = 1e300;
+        for (int64_t k = 0; k < n; k++) {
+            if (k == target) continue;
+            const double *r = rects + 4 * k;
+            double g = fmax(fmax(r[0] - px, px - r[2]), fmax(r[1] - py, py - r[3]));
+            if (g < best) { best = g; bk = k; }
+        }
+        if (bk >= 0) cv_edges(px, py, rects + 4 * bk, a0, f + 8);
+        else for (int q = 8; q < 16; q++) f[q] = 16.f;
+    }
 }

@@ -136,6 +136,7 @@ typedef struct oc_walk_cfg {
     double permittivity;
     uint64_t seed;
     uint32_t stream;       /* Philox counter word 3 */
+    uint32_t start_grid;   /* uniform start: 0 continuous, Q = midpoints of Q equal arcs */
 } oc_walk_cfg;
 
 /* Gaussian surface of cfg->target (complete semantics). */
@@ -143,10 +144,12 @@ void oc_walk_gauss_surface(const oc_grid *g, const double *rects, const oc_walk_
                            double out[4]);
 /* Run walks [first, first+count) of the Philox stream; per-walk records:
  * end conductor (layer index / OC_END_*), hop count, first-hop bin and the
- * capacitance weight (0 in green-start mode). */
+ * weight factor c (0 without a first hop or in green-start mode; the walk
+ * adds c to its end conductor only).  cv_out (nullable): 4 doubles per walk,
+ * first-hop point x, y, first square side a0, c. */
 int oc_walk_run(const oc_grid *g, const double *rects, const oc_walk_cfg *cfg,
                 uint64_t first, uint64_t count, int64_t *end_out, int32_t *hops_out,
-                int32_t *bin_out, double *weight_out);
+                int32_t *bin_out, double *weight_out, double *cv_out);
 /* One reference-style walk driven by an explicit stream of uniforms r in
  * [0,1) (green-start mode, CPU perimeter), on either the grid (complete) or
  * the restated reference tree (defect=1/0).  Returns the end rect index or
@@ -154,6 +157,15 @@ int oc_walk_run(const oc_grid *g, const double *rects, const oc_walk_cfg *cfg,
 int64_t oc_walk_stream(const oc_grid *g, const oc_rtree *t, int defect,
                        const double gauss[4], const double *intg, const double *r,
                        int64_t nr, int64_t *used, int32_t *hops);
+
+/* ---- control-variate features ---- */
+/* For each point rec4[i] = (x, y, a0, unused): (dx, dy) from the point to the
+ * nearest point of each edge (top, right, bottom, left) of rect `target`,
+ * then of the nearest other rect (smallest L-inf gap, then smallest index),
+ * each divided by a0 and clamped to [-16, 16]; 16 floats per point, all 0
+ * when a0 <= 0, the second eight 16 when there is no other rect. */
+void oc_cv_features(const double *rects, int64_t n, int64_t target, const double *rec4, int64_t m,
+                    float *out);
 
 #ifdef __cplusplus
 }

@@ -54,6 +54,7 @@ class WalkCfg(C.Structure):
         ("permittivity", C.c_double),
         ("seed", C.c_uint64),
         ("stream", C.c_uint32),
+        ("start_grid", C.c_uint32),
     ]
 
 
@@ -98,10 +99,11 @@ def lib():
         L.oc_rtree_stats.argtypes = [C.c_void_p, _I64, _I64, C.POINTER(C.c_int)]
         L.oc_walk_gauss_surface.argtypes = [C.c_void_p, _D, C.POINTER(WalkCfg), _D]
         L.oc_walk_run.argtypes = [C.c_void_p, _D, C.POINTER(WalkCfg), C.c_uint64, C.c_uint64,
-                                  _I64, _I32, _I32, _D]
+                                  _I64, _I32, _I32, _D, _D]
         L.oc_walk_stream.argtypes = [C.c_void_p, C.c_void_p, C.c_int, _D, _D, _D, C.c_int64,
                                      _I64, _I32]
         L.oc_walk_stream.restype = C.c_int64
+        L.oc_cv_features.argtypes = [_D, C.c_int64, C.c_int64, _D, C.c_int64, C.POINTER(C.c_float)]
         _lib = L
     return _lib
 
@@ -200,23 +202,25 @@ class Grid:
         return o
 
     def walk_cfg(self, target=0, gauss_mode=GAUSS_OFFSET, gauss_param=1.0, start_mode=START_UNIFORM,
-                 exact_perimeter=False, hop_cap=100000, seed=1, stream=0):
+                 exact_perimeter=False, hop_cap=100000, seed=1, stream=0, start_grid=0):
         return WalkCfg(target, gauss_mode, gauss_param, start_mode, int(exact_perimeter), hop_cap,
-                       PERMITTIVITY, seed, stream)
+                       PERMITTIVITY, seed, stream, start_grid)
 
     def gauss_surface(self, cfg: WalkCfg):
         o = np.zeros(4)
         lib().oc_walk_gauss_surface(self.h, _p(self.rects), C.byref(cfg), _p(o))
         return o
 
-    def walks(self, cfg: WalkCfg, first: int, count: int):
+    def walks(self, cfg: WalkCfg, first: int, count: int, cv: bool = False):
+        """Per-walk (end, hops, first bin, weight factor c[, (p1x, p1y, a0, c)])."""
         end = np.zeros(count, dtype=np.int64)
         hops = np.zeros(count, dtype=np.int32)
         b1 = np.zeros(count, dtype=np.int32)
         w = np.zeros(count)
+        cvo = np.zeros((count, 4)) if cv else None
         lib().oc_walk_run(self.h, _p(self.rects), C.byref(cfg), first, count, _p(end, _I64),
-                          _p(hops, _I32), _p(b1, _I32), _p(w))
-        return end, hops, b1, w
+                          _p(hops, _I32), _p(b1, _I32), _p(w), _p(cvo))
+        return (end, hops, b1, w, cvo) if cv else (end, hops, b1, w)
 
 
 class RefTree:
@@ -258,6 +262,15 @@ class RefTree:
         a, b, c = C.c_int64(), C.c_int64(), C.c_int()
         lib().oc_rtree_stats(self.h, C.byref(a), C.byref(b), C.byref(c))
         return a.value, b.value, c.value
+
+
+def cv_features(rects, target: int, rec4):
+    """Control-variate features (16 floats per point) of points rec4 = (x, y, a0, _)."""
+    r = np.ascontiguousarray(rects, dtype=np.float64)
+    q = np.ascontiguousarray(rec4, dtype=np.float64).reshape(-1, 4)
+    out = np.zeros((len(q), 16), dtype=np.float32)
+    lib().oc_cv_features(_p(r), len(r), int(target), _p(q), len(q), out.ctypes.data_as(C.POINTER(C.c_float)))
+    return out
 
 
 def walk_stream(grid: Grid | None, tree: RefTree | None, defect: bool, gauss, intg, r):

@@ -1,0 +1,101 @@
+"""The learned control variate on the device: features equal the oracle's
+bit-for-bit, the BF16 tensor-core forward and gradients agree with an FP64
+reference, the estimate is unbiased against an independent plain run, and
+the trained network reduces the variance."""
+import numpy as np
+import pytest
+
+import frw
+import mlp_ref as M
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def config1():
+    return frw.generate_layout(0xF4A7 + 1, 100, 1000.0)
+
+
+def test_features_match_oracle(golden):
+    gd = golden("test2")
+    rects, t = gd["rects"], int(gd["walk_target"])
+    rng = np.random.default_rng(2)
+    r = rects[t]
+    n = 4000
+    rec = np.zeros((n, 4))
+    rec[:, 0] = rng.uniform(r[0] - 40, r[2] + 40, n)
+    rec[:, 1] = rng.uniform(r[1] - 40, r[3] + 40, n)
+    rec[: n // 4, :2] = np.round(rec[: n // 4, :2])
+    rec[:, 2] = rng.choice([0.0, 1.0, 2.0, 4.0, 7.5], n)
+    with frw.Layout.from_rects(rects, gd["bounds"]) as L:
+        got = L.cv_features(t, rec)
+    want = O.cv_features(rects, t, rec)
+    assert np.array_equal(got, want)
+
+
+def _random_params(seed):
+    rng = np.random.default_rng(seed)
+    p = rng.normal(0, 0.3, M.NPARAM).astype(np.float32)
+    return p
+
+
+def test_mlp_forward_matches_fp64():
+    p = _random_params(1)
+    x = np.random.default_rng(3).uniform(-3, 3, (5000, 16)).astype(np.float32)
+    got = frw.mlp_forward(p, x)
+    want, _ = M.forward(p, x)
+    err = np.abs(got - want)
+    assert err.max() < 2e-2 * (1 + np.abs(want).max())
+    assert np.corrcoef(got, want)[0, 1] > 0.9999
+
+
+def test_mlp_gradients_match_fp64():
+    p = _random_params(4)
+    rng = np.random.default_rng(5)
+    n = 4096 + 37  # a ragged last chunk
+    x = rng.uniform(-3, 3, (n, 16)).astype(np.float32)
+    y = (rng.random(n) < 0.4).astype(np.float32)
+    wt = rng.exponential(1.0, n).astype(np.float32)
+    wt[:50] = 0
+    inv = 1.0 / float(wt.sum())
+    loss, g = frw.mlp_grad(p, x, y, wt, inv)
+    loss_r, g_r = M.loss_grad(p, x.astype(np.float64), y, wt, inv)
+    assert loss == pytest.approx(loss_r, rel=1e-2)
+    cos = float(g @ g_r / np.linalg.norm(g) / np.linalg.norm(g_r))
+    assert cos > 0.999
+    assert np.linalg.norm(g - g_r) / np.linalg.norm(g_r) < 3e-2
+    # every parameter block gets its gradient
+    for a, b in [(M.O_W1, M.O_B1), (M.O_B1, M.O_W2), (M.O_W2, M.O_B2), (M.O_B2, M.O_W3), (M.O_W3, M.O_B3)]:
+        ga, gb = g[a:b], g_r[a:b]
+        assert np.linalg.norm(ga - gb) <= 5e-2 * np.linalg.norm(gb) + 1e-7
+    assert g[M.O_B3] == pytest.approx(g_r[M.O_B3], rel=1e-2)
+
+
+def test_cv_unbiased_and_reduces_variance():
+    rects = config1()
+    o = frw.capacitance_opts(1.0, start_grid=4096)
+    with frw.Layout.from_rects(rects) as L:
+        cv = frw.ControlVariate(L, 0, o, frw.cv_opts(train_walks=200_000, epochs=6, batch=4096))
+        info = cv.info
+        r = cv.walk(2_000_000, seed=99)
+        ref = L.walk(0, 20_000_000, seed=12345, o=o)  # independent plain run
+        cv.close()
+    c_ref, se_ref = ref.row(0)[1:]
+    assert r.plain == pytest.approx(c_ref, abs=4 * np.hypot(r.plain_se, se_ref))
+    assert abs(r.cv - c_ref) <= 3.5 * np.hypot(r.cv_se, se_ref), (r.cv, c_ref, r.cv_se, se_ref)
+    assert r.variance_ratio > 1.5, r.variance_ratio
+    assert info.quad_points == 4096 * 200 and info.train_loss > 0
+
+
+def test_cv_mean_term_is_the_mean_of_f():
+    """Unbiasedness of the re-added term: over many walks, mean(f) = E[f]."""
+    rects = config1()
+    o = frw.capacitance_opts(1.0, start_grid=1024)
+    with frw.Layout.from_rects(rects) as L:
+        cv = frw.ControlVariate(L, 0, o, frw.cv_opts(train_walks=100_000, epochs=3, batch=4096))
+        mu = cv.info.mean_term
+        r = cv.walk(8_000_000, seed=7)
+        cv.close()
+    # mean(f) = plain - (cv - mu); its standard error is bounded by se_plain + se_cv
+    mean_f = r.plain - (r.cv - mu)
+    assert abs(mean_f - mu) <= 4 * (r.plain_se + r.cv_se)

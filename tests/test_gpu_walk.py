@@ -13,7 +13,7 @@ pytestmark = pytest.mark.gpu
 def oracle_cfg(G, o: frw.Opts, target, seed):
     return G.walk_cfg(target=target, gauss_mode=o.gauss_mode, gauss_param=o.gauss_param,
                       start_mode=o.start_mode, exact_perimeter=bool(o.exact_perimeter), hop_cap=o.hop_cap,
-                      seed=seed, stream=o.stream_id)
+                      seed=seed, stream=o.stream_id, start_grid=o.start_grid)
 
 
 CASES = [
@@ -24,6 +24,8 @@ CASES = [
     ("test1000", 500, dict()),
     ("test1000", 17, dict(gauss_mode=frw.GAUSS_OFFSET, gauss_param=1.0, start_mode=frw.START_UNIFORM,
                           stream_id=3)),
+    ("test100", 5, dict(gauss_mode=frw.GAUSS_OFFSET, gauss_param=1.0, start_mode=frw.START_UNIFORM,
+                        start_grid=4096)),
 ]
 
 
@@ -59,6 +61,7 @@ def test_estimator_matches_oracle_sums_config1():
     assert res.hops_total == hops.sum()
     ks, counts = np.unique(end[end >= 0], return_counts=True)
     assert np.array_equal(res.conductor, ks) and np.array_equal(res.hits, counts)
+    w = np.where(end >= 0, w, 0.0)  # the weight factor counts for the end conductor only
     for k, c, se in zip(res.conductor, res.cap, res.cap_se):
         wk = np.where(end == k, w, 0.0)
         assert c == pytest.approx(wk.mean(), rel=1e-12, abs=1e-30)
@@ -88,11 +91,12 @@ def test_hop_cap_and_escapes():
     rects = config1_layout()
     o = frw.capacitance_opts(1.0, hop_cap=1)
     with frw.Layout.from_rects(rects) as L:
-        end, hops, _, w = L.walk_trace(0, 0, 5000, seed=1, o=o)
+        end, hops, b1, w = L.walk_trace(0, 0, 5000, seed=1, o=o)
         res = L.walk(0, 5000, seed=1, o=o)
     assert hops.max() <= 1 and ((end == -2) | (end >= -1)).all()
     assert res.aborted == (end == -2).sum() > 0
-    assert (w[end < 0] == 0).all()
+    # a cap of one query ends every walk before its first hop: no weight anywhere
+    assert (b1 == -1).all() and (w == 0).all()
 
 
 def test_reference_mode_matches_reference_hit_distribution(golden):
