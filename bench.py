@@ -36,7 +36,7 @@ sys.path.insert(0, os.path.join(ROOT, "engineer-thesis_b200"))
 
 WORKLOAD = dict(workload="frw-c2-10k-rects-1e7-walks", rects=10_000, domain=1e4, walks=10_000_000,
                 target=0, gauss="offset-1", start="uniform", layout_seed=0xF4A7 + 2)
-METRIC = "walks/s (plain FRW, 10k-rect layout, 1e7 walks/step, capacitance row)"
+METRIC = "walks/s (plain FRW, 10k-rect layout, 1e7 walks/step, capacitance row); time to 0.1% rel. SE plain vs CV"
 
 
 def algorithmic_bytes_per_query(n_rects: int) -> int:
@@ -174,6 +174,72 @@ def run_reference(args):
     return 0
 
 
+# ------------------------------------------------------------ headline runs
+HEADLINE = dict(workload="frw-c5-1e6-rects", rects=1_000_000, domain=1e5, layout_seed=0xF4A7 + 3, target=0,
+                start_grid=16384, cv_train_walks=1_000_000, cv_epochs=4, rel_se=1e-3)
+
+
+def time_to_rel_se(frw, device, stream):
+    """Wall time to reach 0.1% rel. SE of C_00 on the 10^6-rect layout, plain vs
+    control variate (training included), each run as: pilot batch -> walks needed
+    -> main batch.  Device time from CUDA events, wall time from the host clock."""
+    import torch
+
+    H = HEADLINE
+    rects = frw.generate_layout(H["layout_seed"], H["rects"], H["domain"])
+    L = frw.Layout.from_rects(rects, device=device)
+    o = frw.capacitance_opts(1.0, start_grid=H["start_grid"])
+    L.walk(0, 1_000_000, seed=1, o=o)  # warm-up
+    torch.cuda.synchronize()
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return out, e0.elapsed_time(e1) * 1e-3, time.perf_counter() - t0
+
+    def plain():
+        pilot = L.walk(H["target"], 2_000_000, seed=11, o=o)
+        c, se = pilot.row(H["target"])[1:]
+        need = int(pilot.walks * (se / abs(c) / H["rel_se"]) ** 2 * 1.05) + 1
+        main_ = L.walk(H["target"], need, seed=12, o=o)
+        n = pilot.walks + main_.walks
+        i0, i1 = (np.searchsorted(r.conductor, H["target"]) for r in (pilot, main_))
+        s1 = pilot.sum_w[i0] + main_.sum_w[i1]
+        s2 = pilot.sum_w2[i0] + main_.sum_w2[i1]
+        mean = s1 / n
+        se = np.sqrt(max(s2 / n - mean * mean, 0.0) * n / (n - 1) / n)
+        return {"walks": n, "c00": mean, "rel_se": se / abs(mean)}
+
+    def with_cv():
+        cv = frw.ControlVariate(L, H["target"], o, frw.cv_opts(train_walks=H["cv_train_walks"],
+                                                              epochs=H["cv_epochs"]))
+        pilot = cv.walk(1_000_000, seed=21)
+        need = int(pilot.walks * (pilot.cv_se / abs(pilot.cv) / H["rel_se"]) ** 2 * 1.05) + 1
+        main_ = cv.walk(max(need, 2), seed=22)
+        n = pilot.walks + main_.walks
+        c = (pilot.cv * pilot.walks + main_.cv * main_.walks) / n
+        se = np.sqrt((pilot.cv_se * pilot.walks) ** 2 + (main_.cv_se * main_.walks) ** 2) / n
+        info = cv.info
+        out = {"walks": n, "c00": c, "rel_se": se / abs(c), "variance_reduction": main_.variance_ratio,
+               "train_walks": info.train_walks, "train_device_s": info.train_ms * 1e-3,
+               "exact_mean_device_s": info.quad_ms * 1e-3, "exact_mean_points": info.quad_points}
+        cv.close()
+        return out
+
+    p, p_dev, p_wall = timed(plain)
+    c, c_dev, c_wall = timed(with_cv)
+    L.close()
+    return {"workload": H["workload"], "target_rel_se": H["rel_se"], "start_grid": H["start_grid"],
+            "plain": dict(p, device_s=p_dev, wall_s=p_wall),
+            "cv": dict(c, device_s=c_dev, wall_s=c_wall),
+            "speedup_wall": p_wall / c_wall, "speedup_device": p_dev / c_dev,
+            "agree_sigma": abs(p["c00"] - c["c00"]) / np.hypot(p["c00"] * p["rel_se"], c["c00"] * c["rel_se"])}
+
+
 # ------------------------------------------------------------------ our arm
 def main():
     ap = argparse.ArgumentParser()
@@ -185,6 +251,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--walks", type=int, default=None, help="override walks per step (profiling runs)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-headline", action="store_true", help="skip the time-to-0.1%% plain vs CV runs")
     args = ap.parse_args()
     if args.walks:
         WORKLOAD["walks"] = args.walks
@@ -289,6 +356,10 @@ def main():
         torch.cuda.synchronize()
         e2e_ms = e0.elapsed_time(e1) / e2e_steps
 
+    headline = None
+    if rank == 0 and world == 1 and not args.no_headline:
+        headline = time_to_rel_se(frw, local, stream)
+
     if rank == 0:
         last = results[-1]
         i0 = int(np.searchsorted(last.conductor, W["target"]))
@@ -316,6 +387,8 @@ def main():
                                  "(the tree is L2-resident, so HBM is an upper-bound denominator)"},
             "clocks": clk.summary(),
         }
+        if headline:
+            out["time_to_0.1pct_rel_se"] = headline
         if cpu:
             out["cpu_baseline"] = cpu
         print(json.dumps(out))
