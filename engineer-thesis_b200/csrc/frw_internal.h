@@ -76,6 +76,8 @@ struct WalkParams {
     int64_t hop_cap;
     double permittivity;
     uint64_t seed;
+    const uint64_t *seed_dev;  // when set, the seed is read here (captured graphs replay with new seeds)
+    uint32_t chunk;            // walks a warp claims per global atomic (0: 128)
     uint64_t total_walks;
     unsigned long long *counter;  // global walk counter (refill)
     // per-conductor accumulators (dense rows, acc_base + layer index)
@@ -128,6 +130,9 @@ frw_status launch_box_collides(const DevLayout &L, const double *d_boxes, int64_
                                cudaStream_t stream);
 frw_status launch_gauss(const DevLayout &L, const double *d_targets /*[n][4]*/, int n, int mode,
                         double param, double *d_out, uint32_t *d_status, cudaStream_t stream);
+// one Gaussian surface per job, each on its job's layout
+frw_status launch_gauss_jobs(const WalkJob *d_jobs, const double *d_targets, int njobs, int mode, double param,
+                             double *d_out, uint32_t *d_status, cudaStream_t stream);
 
 // walk.cu
 frw_status launch_walk(const WalkParams &P, int threads, int blocks, cudaStream_t stream);

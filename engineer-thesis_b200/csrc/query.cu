@@ -69,14 +69,9 @@ __device__ double adjusted_factor(const DevLayout &L, const double r[4], double 
     return adj;
 }
 
-__global__ void k_gauss(DevLayout L, const double4 *__restrict__ targets, int n, int mode, double param,
-                        double4 *__restrict__ out, uint32_t *status) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const double4 t = targets[i];
+// creatGaussianSurfFrom (scale mode) or the target grown by `param`.
+__device__ void gauss_one(const DevLayout &L, const double4 t, int mode, double param, double o[4], uint32_t &st) {
     const double r[4] = {t.x, t.y, t.z, t.w};
-    double o[4];
-    uint32_t st = 0;
     if (mode == FRW_GAUSS_SCALE) {
         if (param < 1.0) {  // creatGaussianSurfFrom returns the rect itself
             o[0] = r[0]; o[1] = r[1]; o[2] = r[2]; o[3] = r[3];
@@ -91,11 +86,41 @@ __global__ void k_gauss(DevLayout L, const double4 *__restrict__ targets, int n,
         o[2] = __dadd_rn(r[2], param);
         o[3] = __dadd_rn(r[3], param);
     }
+}
+
+__global__ void k_gauss(DevLayout L, const double4 *__restrict__ targets, int n, int mode, double param,
+                        double4 *__restrict__ out, uint32_t *status) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double o[4];
+    uint32_t st = 0;
+    gauss_one(L, targets[i], mode, param, o, st);
+    out[i] = make_double4(o[0], o[1], o[2], o[3]);
+    if (st) atomicOr(status, st);
+}
+
+// One job per thread, each on its own layout (batched runs).
+__global__ void k_gauss_jobs(const WalkJob *__restrict__ jobs, const double4 *__restrict__ targets, int n, int mode,
+                             double param, double4 *__restrict__ out, uint32_t *status) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double o[4];
+    uint32_t st = 0;
+    gauss_one(jobs[i].L, targets[i], mode, param, o, st);
     out[i] = make_double4(o[0], o[1], o[2], o[3]);
     if (st) atomicOr(status, st);
 }
 
 }  // namespace
+
+frw_status launch_gauss_jobs(const WalkJob *d_jobs, const double *d_targets, int njobs, int mode, double param,
+                             double *d_out, uint32_t *d_status, cudaStream_t stream) {
+    if (njobs <= 0) return FRW_OK;
+    k_gauss_jobs<<<(njobs + 63) / 64, 64, 0, stream>>>(d_jobs, (const double4 *)d_targets, njobs, mode, param,
+                                                      (double4 *)d_out, d_status);
+    FRW_CK(cudaGetLastError());
+    return FRW_OK;
+}
 
 frw_status launch_query(const DevLayout &L, const double *d_pts, int64_t n, double *d_sq, int64_t *d_hit,
                         uint32_t *d_status, cudaStream_t stream) {

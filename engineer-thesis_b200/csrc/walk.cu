@@ -31,7 +31,7 @@ constexpr int kWarpsPerBlock = kWalkThreads / 32;
 constexpr int kTabSlots = 32;  // per warp
 constexpr unsigned long long kEmptyKey = ~0ull;
 constexpr unsigned kFull = 0xFFFFFFFFu;
-constexpr uint64_t kChunk = 128;  // walks a warp claims from the global counter at a time
+constexpr uint64_t kChunkDefault = 128;  // walks a warp claims from the global counter at a time
 
 struct Slot {
     unsigned long long key, n, hops;
@@ -168,6 +168,8 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(const WalkParams P) {
     const int refill_min = P.refill_min < 1 ? 1 : (P.refill_min > 32 ? 32 : P.refill_min);
     const bool uniform_start = P.start_mode == FRW_START_UNIFORM;
     const bool exact = P.exact_perimeter != 0;
+    const uint64_t seed = P.seed_dev ? *P.seed_dev : P.seed;
+    const uint64_t kChunk = P.chunk ? (uint64_t)P.chunk : kChunkDefault;
 
     bool active = false, exhausted = false;
     uint64_t chunk_next = 0, chunk_end = 0;  // warp-uniform: unclaimed part of this warp's walk chunk
@@ -224,7 +226,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(const WalkParams P) {
                     bin1 = -1;
                     a0 = 0.0;
                     p1x = p1y = 0.0;
-                    rnd = draw_block(P.seed, stream, pw, 0);
+                    rnd = draw_block(seed, stream, pw, 0);
                     double u = word_u(rnd, 0);
                     if (P.start_grid) {  // midpoint of arc floor(u*Q) of Q equal arcs
                         const uint32_t q = (uint32_t)__dmul_rn(u, (double)P.start_grid);
@@ -259,7 +261,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(const WalkParams P) {
                 else if (hops >= P.hop_cap) code = -2;
                 else {
                     hop++;
-                    if ((hop & 3) == 0) rnd = draw_block(P.seed, stream, pw, hop);
+                    if ((hop & 3) == 0) rnd = draw_block(seed, stream, pw, hop);
                     const int bin = bin_of(s_intg, word_u(rnd, hop));
                     point_from_index(sq, bin, exact, px, py);
                     if (hop == 1) {

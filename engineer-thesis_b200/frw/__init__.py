@@ -115,6 +115,20 @@ class CvResult(C.Structure):
     ]
 
 
+class Tuning(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_uint32),
+        ("blocks_per_sm", C.c_int32),
+        ("refill_min", C.c_int32),
+        ("chunk", C.c_int32),
+        ("ms", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {"blocks_per_sm": self.blocks_per_sm, "refill_min": self.refill_min, "chunk": self.chunk,
+                "trial_ms": self.ms}
+
+
 class LayoutInfo(C.Structure):
     _fields_ = [
         ("n_rects", C.c_int64),
@@ -156,6 +170,13 @@ _SIGS = {
                          C.c_int),
     "frw_generate_layout": ([C.c_uint64, C.c_int64, C.c_double, C.c_int32, C.c_int32, C.c_double, _F], C.c_int),
     "frw_write_layout": ([C.c_char_p, _F, C.c_int64, C.c_char_p], C.c_int),
+    "frw_batch_create": ([C.POINTER(_VP), _I64, C.POINTER(C.c_uint64), C.c_int32, C.POINTER(Opts), C.POINTER(_VP)],
+                         C.c_int),
+    "frw_batch_tune": ([_VP, C.c_uint64, C.POINTER(Tuning)], C.c_int),
+    "frw_batch_set_tuning": ([_VP, C.POINTER(Tuning)], C.c_int),
+    "frw_batch_get_tuning": ([_VP, C.POINTER(Tuning)], C.c_int),
+    "frw_batch_run": ([_VP, C.c_uint64, C.POINTER(Result), _VP], C.c_int),
+    "frw_batch_destroy": ([_VP], C.c_int),
     "frw_cv_opts_default": ([C.POINTER(CvOpts)], None),
     "frw_cv_train": ([_VP, C.c_int64, C.POINTER(Opts), C.POINTER(CvOpts), C.POINTER(_VP), _VP], C.c_int),
     "frw_cv_info_get": ([_VP, C.POINTER(CvInfo)], C.c_int),
@@ -396,6 +417,78 @@ class Layout:
         _check(lib().frw_walk_trace(self._h, target, first, walks, seed, C.byref(o) if o else None, _ptr(end),
                                     _ptr(hops), _ptr(b1), _ptr(w), MEM_HOST, None))
         return end, hops, b1, w
+
+
+class Batch:
+    """frw_batch: many (layout, target, walks) jobs in one persistent graph-captured launch."""
+
+    def __init__(self, layouts, targets, walks, o: Opts | None = None):
+        self._layouts = list(layouts)  # keep alive
+        n = len(self._layouts)
+        arr = (_VP * n)(*[L._h for L in self._layouts])
+        t = np.ascontiguousarray(targets, dtype=np.int64)
+        w = np.ascontiguousarray(walks, dtype=np.uint64)
+        self.walks = w
+        h = _VP()
+        _check(lib().frw_batch_create(arr, _ptr(t, _I64), _ptr(w, C.POINTER(C.c_uint64)), n,
+                                      C.byref(o) if o else None, C.byref(h)))
+        self._h = h
+
+    def tune(self, trial_walks: int) -> Tuning:
+        t = Tuning()
+        _check(lib().frw_batch_tune(self._h, trial_walks, C.byref(t)))
+        return t
+
+    def set_tuning(self, blocks_per_sm: int, refill_min: int, chunk: int):
+        t = Tuning(C.sizeof(Tuning), blocks_per_sm, refill_min, chunk, 0.0)
+        _check(lib().frw_batch_set_tuning(self._h, C.byref(t)))
+
+    @property
+    def tuning(self) -> Tuning:
+        t = Tuning()
+        _check(lib().frw_batch_get_tuning(self._h, C.byref(t)))
+        return t
+
+    def run(self, seed: int, capacity: int = 64):
+        n = len(self._layouts)
+        res = (Result * n)()
+        keep = []
+        for j in range(n):
+            cond = np.zeros(capacity, dtype=np.int64)
+            hits = np.zeros(capacity, dtype=np.uint64)
+            c = np.zeros(capacity)
+            se = np.zeros(capacity)
+            s1 = np.zeros(capacity)
+            s2 = np.zeros(capacity)
+            keep.append((cond, hits, c, se, s1, s2))
+            r = res[j]
+            r.capacity = capacity
+            r.conductor = _ptr(cond, _I64)
+            r.hits = _ptr(hits, C.POINTER(C.c_uint64))
+            r.cap = _ptr(c, _D)
+            r.cap_se = _ptr(se, _D)
+            r.sum_w = _ptr(s1, _D)
+            r.sum_w2 = _ptr(s2, _D)
+        _check(lib().frw_batch_run(self._h, seed, res, None))
+        out = []
+        for j in range(n):
+            r = res[j]
+            m = min(r.n_entries, capacity)
+            cond, hits, c, se, s1, s2 = keep[j]
+            out.append(WalkResult(r.walks, r.escaped, r.aborted, r.hops_total, np.array(r.gauss[:]), r.fraction_other,
+                                  r.kernel_ms, cond[:m], hits[:m], c[:m], se[:m], s1[:m], s2[:m]))
+        return out
+
+    def close(self):
+        if self._h:
+            lib().frw_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def cv_opts(train_walks=1_000_000, train_seed=0x7E57C0DE, epochs=4, batch=8192, lr=3e-3) -> CvOpts:

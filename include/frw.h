@@ -215,6 +215,33 @@ frw_status frw_gauss_surface(const frw_layout *layout, int64_t target, const frw
 frw_status frw_avg_path_len(const char *path, int64_t iter_num, int64_t rect_id, int layer,
                             uint64_t seed, int device, const char *hist_path, double *fraction);
 
+/* ---- batched walks: many layouts / targets in one persistent launch ----
+ * Job j walks walks[j] times from targets[j] of layouts[j] (all layouts on
+ * one device) with Philox stream opts->stream_id + j; its results equal a
+ * frw_walk of that job alone with stream_id = opts->stream_id + j.  The
+ * device work of a run is one captured CUDA graph (clears, Gaussian
+ * surfaces, ONE multi-job walk launch, row compaction); frw_batch_run
+ * replays it with a new seed.  No reference counterpart (the reference runs
+ * one target of one layout per process). */
+typedef struct frw_batch frw_batch;
+typedef struct frw_tuning {
+    uint32_t struct_size;   /* sizeof(frw_tuning) */
+    int32_t blocks_per_sm;  /* resident walk blocks per SM (0: occupancy limit) */
+    int32_t refill_min;     /* refill a warp when at least this many lanes are idle */
+    int32_t chunk;          /* walks a warp claims per global atomic (32 .. 2^20) */
+    double ms;              /* walk-kernel time of the tuning trial that chose it */
+} frw_tuning;
+frw_status frw_batch_create(const frw_layout *const *layouts, const int64_t *targets, const uint64_t *walks,
+                            int32_t njobs, const frw_opts *opts, frw_batch **out);
+/* Measured search over blocks_per_sm x refill_min x chunk on a proportional
+ * sample of trial_walks walks of the batch; keeps and returns the fastest. */
+frw_status frw_batch_tune(frw_batch *batch, uint64_t trial_walks, frw_tuning *chosen);
+frw_status frw_batch_set_tuning(frw_batch *batch, const frw_tuning *tuning);
+frw_status frw_batch_get_tuning(const frw_batch *batch, frw_tuning *tuning);
+/* results: njobs caller-owned frw_result (capacity and arrays per job). */
+frw_status frw_batch_run(frw_batch *batch, uint64_t seed, frw_result *results, void *stream);
+frw_status frw_batch_destroy(frw_batch *batch);
+
 /* ---- learned control variate (no reference counterpart) ----
  * For C_tt the walk estimate is w = c * 1{end = t} (c: first-hop weight
  * factor).  The control variate is f = c * phi(x1), phi an MLP (16 -> 64 ->
