@@ -189,7 +189,11 @@ def time_to_rel_se(frw, device, stream):
     rects = frw.generate_layout(H["layout_seed"], H["rects"], H["domain"])
     L = frw.Layout.from_rects(rects, device=device)
     o = frw.capacitance_opts(1.0, start_grid=H["start_grid"])
-    L.walk(0, 1_000_000, seed=1, o=o)  # warm-up
+    # untimed warm-up of both paths (module loading, memory-pool growth)
+    L.walk(0, 1_000_000, seed=1, o=o)
+    w = frw.ControlVariate(L, H["target"], o, frw.cv_opts(train_walks=65_536, epochs=1))
+    w.walk(1_000_000, seed=2)
+    w.close()
     torch.cuda.synchronize()
 
     def timed(fn):
@@ -240,6 +244,52 @@ def time_to_rel_se(frw, device, stream):
             "agree_sigma": abs(p["c00"] - c["c00"]) / np.hypot(p["c00"] * p["rel_se"], c["c00"] * c["rel_se"])}
 
 
+# ------------------------------------------------------------ batched config
+BATCHED = dict(workload="frw-c4-256-layouts-1e8-walks", layouts=256, min_rects=100, max_rects=100_000,
+               total_walks=100_000_000, layout_seed=0x0C4, tune_walks=5_000_000)
+
+
+def batched_run(frw, device, stream, steps):
+    """256 layouts (log-uniform 100..1e5 rects), one target each, walks
+    proportional to rects (1e8 in total): one graph-captured persistent launch
+    per run, launch parameters from the autotuner."""
+    import torch
+
+    B = BATCHED
+    rng = np.random.default_rng(B["layout_seed"])
+    counts = np.exp(rng.uniform(np.log(B["min_rects"]), np.log(B["max_rects"]), B["layouts"])).astype(int)
+    t0 = time.perf_counter()
+    layouts = []
+    for i, n in enumerate(counts):
+        dom = float(np.sqrt(n) * 100.0)  # the configs' density: 1e4 rects on [0,1e4]^2
+        layouts.append(frw.Layout.from_rects(frw.generate_layout(B["layout_seed"] + i, int(n), dom), device=device))
+    t_layouts = time.perf_counter() - t0
+    walks = np.maximum(1, np.round(counts / counts.sum() * B["total_walks"])).astype(np.uint64)
+    o = frw.capacitance_opts(1.0)
+    batch = frw.Batch(layouts, np.zeros(len(layouts), dtype=np.int64), walks, o)
+    t0 = time.perf_counter()
+    tuning = batch.tune(B["tune_walks"])
+    t_tune = time.perf_counter() - t0
+    batch.run(seed=1)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(steps):
+        res = batch.run(seed=10 + k)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    total = int(walks.sum())
+    out = {"workload": B["workload"], "rects_total": int(counts.sum()), "walks_per_run": total,
+           "ms_per_run": ms, "walks_per_s": total / (ms * 1e-3), "tuning": tuning.as_dict(),
+           "tune_s": t_tune, "layout_build_s": t_layouts,
+           "mean_hops": float(sum(r.hops_total for r in res) / total)}
+    batch.close()
+    for L in layouts:
+        L.close()
+    return out
+
+
 # ------------------------------------------------------------------ our arm
 def main():
     ap = argparse.ArgumentParser()
@@ -252,6 +302,7 @@ def main():
     ap.add_argument("--walks", type=int, default=None, help="override walks per step (profiling runs)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-headline", action="store_true", help="skip the time-to-0.1%% plain vs CV runs")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 256-layout batched runs")
     args = ap.parse_args()
     if args.walks:
         WORKLOAD["walks"] = args.walks
@@ -356,9 +407,11 @@ def main():
         torch.cuda.synchronize()
         e2e_ms = e0.elapsed_time(e1) / e2e_steps
 
-    headline = None
+    headline = batched = None
     if rank == 0 and world == 1 and not args.no_headline:
         headline = time_to_rel_se(frw, local, stream)
+    if rank == 0 and world == 1 and not args.no_batched:
+        batched = batched_run(frw, local, stream, 3)
 
     if rank == 0:
         last = results[-1]
@@ -389,6 +442,8 @@ def main():
         }
         if headline:
             out["time_to_0.1pct_rel_se"] = headline
+        if batched:
+            out["batched"] = batched
         if cpu:
             out["cpu_baseline"] = cpu
         print(json.dumps(out))
