@@ -660,7 +660,8 @@ frw_status frw_walk(const frw_layout *L, int64_t target, uint64_t walks, uint64_
     }
     DeviceGuard g(L->device);
     WalkRun R;
-    rc = run_walks(L, target, 0, walks, seed, o, (cudaStream_t)stream, nullptr, nullptr, nullptr, nullptr, &R);
+    rc = run_walks(L, target, o.first_walk, walks, seed, o, (cudaStream_t)stream, nullptr, nullptr, nullptr, nullptr,
+                   &R);
     if (rc) return rc;
     res->walks = walks;
     res->escaped = R.escaped;

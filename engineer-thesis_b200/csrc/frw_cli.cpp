@@ -6,7 +6,8 @@
 // capacitance weights), --offset <d> (Gaussian surface = target grown by d),
 // --scale <f> (reference scaled surface, default 1.5), --exact-perimeter,
 // --cap (print the capacitance row), --hist <file> (histogram file name;
-// default "<unixtime>wyniki.txt" as the reference writes).
+// default "<unixtime>wyniki.txt" as the reference writes), --json (one JSON
+// result record on stdout after the reference's two lines).
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -26,7 +27,7 @@ static const char *kHelp =
     "\t-G\t--GPU\t\t\t(accepted; walks always run on the GPU)\n"
     "\t-L\t--layer\t\t\tlayer number\n"
     "\t\t--seed <u64> --device <k> --uniform --offset <d> --scale <f>\n"
-    "\t\t--exact-perimeter --cap --hist <file>\n"
+    "\t\t--exact-perimeter --cap --hist <file> --json\n"
     "\t\t--help\t\t\tthis text\n"
     "\tDefaults: -I 1000 -O 10 -S ../tests/test -L 0\n";
 
@@ -34,7 +35,7 @@ int main(int argc, char **argv) {
     std::string path = "../tests/test", hist;
     long long iters = 1000, object = 10;
     int layer = 0, device = 0;
-    bool measure = false, uniform = false, cap = false, exact = false;
+    bool measure = false, uniform = false, cap = false, exact = false, json = false;
     unsigned long long seed = (unsigned long long)time(nullptr);
     double offset = -1.0, scale = 1.5;
     for (int i = 1; i < argc; i++) {
@@ -60,6 +61,7 @@ int main(int argc, char **argv) {
         else if (a == "--exact-perimeter") exact = true;
         else if (a == "--cap") cap = true;
         else if (a == "--hist") hist = val("--hist");
+        else if (a == "--json") json = true;
         else if (a == "--help" || a == "-h") {
             printf("%s", kHelp);
             return 0;
@@ -137,6 +139,20 @@ int main(int argc, char **argv) {
         printf("capacitance row of conductor %lld (F/m), %llu walks:\n", object, (unsigned long long)iters);
         for (int64_t k = 0; k < r.n_entries && k < r.capacity; k++)
             printf("  C[%lld,%lld] = %.6e +- %.2e\n", object, (long long)cond[k], c[k], se[k]);
+    }
+    if (json) {
+        printf("{\"layout\": \"%s\", \"layer\": %d, \"rects\": %lld, \"target\": %lld, \"walks\": %llu, "
+               "\"seed\": %llu, \"fraction_other\": %.17g, \"escaped\": %llu, \"aborted\": %llu, "
+               "\"hops_per_walk\": %.6f, \"walk_kernel_ms\": %.4f, \"walks_per_s\": %.6g, "
+               "\"tree_build_ms\": %.4f, \"gauss\": [%.17g, %.17g, %.17g, %.17g], \"rows\": [",
+               path.c_str(), layer, (long long)info.n_rects, object, (unsigned long long)iters, seed, r.fraction_other,
+               (unsigned long long)r.escaped, (unsigned long long)r.aborted, (double)r.hops_total / (double)iters,
+               r.kernel_ms, iters / (r.kernel_ms * 1e-3), info.build_ms, r.gauss[0], r.gauss[1], r.gauss[2],
+               r.gauss[3]);
+        for (int64_t k = 0; k < r.n_entries && k < r.capacity; k++)
+            printf("%s{\"conductor\": %lld, \"hits\": %llu, \"cap\": %.17g, \"cap_se\": %.6g}", k ? ", " : "",
+                   (long long)cond[k], (unsigned long long)hits[k], c[k], se[k]);
+        printf("]}\n");
     }
     frw_layout_destroy(L);
     return 0;

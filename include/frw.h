@@ -141,6 +141,10 @@ typedef struct frw_opts {
     uint32_t start_grid;     /* uniform start only: 0 = continuous; Q > 0 = the Q midpoints of Q equal
                                 arcs of the Gaussian perimeter (the start distribution a control
                                 variate's exact mean is summed over) */
+    uint64_t first_walk;     /* frw_walk: Philox index of its first walk.  Runs over disjoint walk
+                                ranges are independent and their rows (hits, sum_w, sum_w2) add up
+                                exactly to one run over the union: a run can be checkpointed as
+                                (seed, stream_id, next first_walk, rows) and resumed. */
 } frw_opts;
 void frw_opts_default(frw_opts *opts);
 

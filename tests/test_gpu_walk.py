@@ -127,3 +127,61 @@ def test_avg_path_len_entry_point(tmp_path):
     assert f == r.fraction_other and 0 < f < 1
     lines = open(h, encoding="utf-8").read().splitlines()
     assert lines[0] == "[GPU]" and len(lines) >= 2
+
+
+def test_resume_from_checkpoint():
+    """Two runs over disjoint walk ranges add up exactly to one run over both."""
+    rects = config1_layout()
+    with frw.Layout.from_rects(rects) as L:
+        full = L.walk(0, 60_000, seed=8, o=frw.capacitance_opts(1.0))
+        a = L.walk(0, 25_000, seed=8, o=frw.capacitance_opts(1.0))
+        b = L.walk(0, 35_000, seed=8, o=frw.capacitance_opts(1.0, first_walk=25_000))
+    ks = np.union1d(a.conductor, b.conductor)
+    assert np.array_equal(ks, full.conductor)
+    for k in ks:
+        ha, _, _ = a.row(k)
+        hb, _, _ = b.row(k)
+        assert ha + hb == full.row(k)[0]
+    ia, ib, i = (np.searchsorted(r.conductor, 0) for r in (a, b, full))
+    assert a.sum_w[ia] + b.sum_w[ib] == pytest.approx(full.sum_w[i], rel=1e-12)
+    assert a.hops_total + b.hops_total == full.hops_total
+
+
+def test_cli_reference_flags(tmp_path):
+    """The command-line front end with the reference's flags prints the
+    reference's two lines, writes the histogram and a JSON record."""
+    import json
+    import os
+    import subprocess
+
+    rects = config1_layout()
+    p = str(tmp_path / "c1.txt")
+    frw.write_layout(p, rects)
+    exe = os.path.join(frw.PKG, "lib", "frw")
+    h = str(tmp_path / "hist.txt")
+    out = subprocess.run([exe, "-S", p, "-I", "20000", "-O", "0", "-G", "-L", "0", "--seed", "3", "--hist", h,
+                          "--json"], capture_output=True, text=True, check=True).stdout.splitlines()
+    assert out[1].startswith("[GPU] Ile sciezek trafi") and out[2].startswith("Czas wykonania:")
+    rec = json.loads(out[3])
+    with frw.Layout.from_file(p) as L:
+        r = L.walk(0, 20_000, seed=3, o=frw.opts())
+    assert rec["fraction_other"] == r.fraction_other and rec["walks"] == 20_000
+    assert open(h, encoding="utf-8").readline().strip() == "[GPU]"
+
+
+def test_multilayer_file_and_layer_flag(tmp_path):
+    a = frw.generate_layout(1, 30, 400.0)
+    b = frw.generate_layout(2, 40, 500.0)
+    p = str(tmp_path / "two.txt")
+    with open(p, "w") as f:
+        f.write("magic\n<< metal1 >>\n")
+        for r in a:
+            f.write("rect %d %d %d %d\n" % tuple(r))
+        f.write("<< metal2 >>\n")
+        for r in b:
+            f.write("rect %d %d %d %d\n" % tuple(r))
+        f.write("<< end >>\n")
+    with frw.Layout.from_file(p, layer=1) as L:
+        assert np.array_equal(L.rects(), b.astype(np.float64))
+    with pytest.raises(frw.FrwError):
+        frw.Layout.from_file(p, layer=2)
