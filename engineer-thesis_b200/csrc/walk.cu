@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(const WalkParams P) {
     uint4 rnd = make_uint4(0, 0, 0, 0);  // uniforms of hops (hop & ~3) .. +3
     int32_t hops = 0, bin1 = -1;
     int side = 0;
-    double px = 0, py = 0, a0 = 0, perim = 0, p1x = 0, p1y = 0;
+    double px = 0, py = 0, a0 = 0, perim = 0;
     double sq[4] = {0, 0, 0, 0};
     uint32_t st = 0;
 
@@ -225,7 +225,6 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(const WalkParams P) {
                     hops = 0;
                     bin1 = -1;
                     a0 = 0.0;
-                    p1x = p1y = 0.0;
                     rnd = draw_block(seed, stream, pw, 0);
                     double u = word_u(rnd, 0);
                     if (P.start_grid) {  // midpoint of arc floor(u*Q) of Q equal arcs
@@ -267,8 +266,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(const WalkParams P) {
                     if (hop == 1) {
                         bin1 = bin;
                         a0 = __dsub_rn(sq[2], sq[0]);
-                        p1x = px;
-                        p1y = py;
+                        if (P.rec_cv) *reinterpret_cast<double2 *>(&P.rec_cv[gw]) = make_double2(px, py);
                     }
                 }
             }
@@ -292,7 +290,10 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(const WalkParams P) {
                 P.rec_bin[gw] = bin1;
                 P.rec_w[gw] = c;
             }
-            if (P.rec_cv) P.rec_cv[gw] = make_double4(p1x, p1y, a0, c);
+            if (P.rec_cv) {  // first-hop point written at hop 1 (zero when there was none)
+                if (bin1 < 0) *reinterpret_cast<double2 *>(&P.rec_cv[gw]) = make_double2(0.0, 0.0);
+                reinterpret_cast<double2 *>(&P.rec_cv[gw])[1] = make_double2(a0, c);
+            }
             active = false;
         }
         const unsigned em = __ballot_sync(kFull, ended);
