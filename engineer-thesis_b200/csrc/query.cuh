@@ -181,20 +181,34 @@ __device__ __forceinline__ bool collides_listed(const DevLayout &L, const Cands 
     return false;
 }
 
+// Decision of one box of the replay.  Its four extents (distances from p to
+// its sides) lie within eps << delta of each other, so comparing one extent
+// with the clearance d* settles every box farther than delta from d*: all
+// extents above d* means the nearest obstacle (bounds side or listed rect) is
+// touched; all below means nothing can be.  Only boxes within delta of d*
+// take the exact predicate.
+__device__ __forceinline__ bool collides_box(const DevLayout &L, const Cands &C, const Listed &T,
+                                             const double o[4], double px, double dstar) {
+    const double e = __dsub_rn(o[2], px);
+    if (e > dstar + L.delta) return true;
+    if (e < dstar - L.delta) return false;
+    return collides_listed(L, C, T, o);
+}
+
 // drawBiggestSquareAtPoint replayed on scalars: same operations, same order,
 // explicit round-to-nearest intrinsics (no contraction).
 __device__ __forceinline__ uint32_t replay_square(const DevLayout &L, const Cands &C, double px,
-                                                  double py, double sq[4]) {
+                                                  double py, double dstar, double sq[4]) {
     Listed T;
     load_listed(L, C, T);
     double o[4] = {__dsub_rn(px, 1.0), __dsub_rn(py, 1.0), __dadd_rn(px, 1.0), __dadd_rn(py, 1.0)};
-    if (collides_listed(L, C, T, o)) {
+    if (collides_box(L, C, T, o, px, dstar)) {
         sq[0] = o[0]; sq[1] = o[1]; sq[2] = o[2]; sq[3] = o[3];
         return 0;
     }
     const double in2[4] = {__dsub_rn(px, 2.0), __dsub_rn(py, 2.0), __dadd_rn(px, 2.0),
                            __dadd_rn(py, 2.0)};
-    if (collides_listed(L, C, T, in2)) {
+    if (collides_box(L, C, T, in2, px, dstar)) {
         sq[0] = in2[0]; sq[1] = in2[1]; sq[2] = in2[2]; sq[3] = in2[3];
         return 0;
     }
@@ -202,7 +216,7 @@ __device__ __forceinline__ uint32_t replay_square(const DevLayout &L, const Cand
     bool maxReached = false, isc;
     uint32_t st = 0;
     int it = 0;
-    while ((isc = collides_listed(L, C, T, o)) || !maxReached || dist > kMinDist) {
+    while ((isc = collides_box(L, C, T, o, px, dstar)) || !maxReached || dist > kMinDist) {
         if (isc) {
             if (dist > kMinDist) dist = __ddiv_rn(dist, 2.0);
             maxReached = true;
@@ -232,7 +246,7 @@ __device__ __forceinline__ uint32_t query_point(const DevLayout &L, double px, d
     Cands C;
     double best;
     uint32_t st = clearance(L, px, py, C, hit, best);
-    st |= replay_square(L, C, px, py, sq);
+    st |= replay_square(L, C, px, py, best, sq);
     return st;
 }
 
