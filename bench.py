@@ -191,7 +191,7 @@ def time_to_rel_se(frw, device, stream):
     o = frw.capacitance_opts(1.0, start_grid=H["start_grid"])
     # untimed warm-up of both paths (module loading, memory-pool growth)
     L.walk(0, 1_000_000, seed=1, o=o)
-    w = frw.ControlVariate(L, H["target"], o, frw.cv_opts(train_walks=65_536, epochs=1))
+    w = frw.ControlVariate(L, H["target"], o, frw.cv_opts(train_walks=H["cv_train_walks"], epochs=1))
     w.walk(1_000_000, seed=2)
     w.close()
     torch.cuda.synchronize()

@@ -576,15 +576,6 @@ __global__ void k_cv_reduce(const int64_t *__restrict__ end, const double4 *__re
     }
 }
 
-__global__ void k_weighted_sum(const double4 *__restrict__ rec, const float *__restrict__ phi, int64_t n,
-                               double *sum) {
-    double s = 0.0;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        s += rec[i].w * (double)phi[i];
-    s = warp_sum(s);
-    if ((threadIdx.x & 31) == 0) atomicAdd(sum, s);
-}
-
 // Training pairs from walk records: y = 1{end == target}, weight c^2.
 __global__ void k_targets(const int64_t *__restrict__ end, const double4 *__restrict__ rec, int64_t n, int target,
                           float *__restrict__ y, float *__restrict__ wt, double *wsum) {
@@ -623,32 +614,73 @@ __global__ void k_quad_starts(DevLayout L, const double4 *__restrict__ gauss, ui
     side_out[q] = code;
 }
 
-// Every (start q, bin i): first-hop point, a0 and weight c * pi_i / Q.
-__global__ void k_quad_points(const double4 *__restrict__ gauss, const double4 *__restrict__ sqs,
-                              const int *__restrict__ sides, uint32_t Q, const double *__restrict__ pi_exact,
-                              const double *__restrict__ wx, const double *__restrict__ wy, double eps, bool exact,
-                              double4 *__restrict__ out) {
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (int64_t)Q * FRW_NSAMPLE) return;
-    const uint32_t q = (uint32_t)(t / FRW_NSAMPLE);
-    const int i = (int)(t % FRW_NSAMPLE);
-    const int side = sides[q];
-    if (side < 0) {
-        out[t] = make_double4(0, 0, 0, 0);
-        return;
-    }
+// Exact mean of f over every (grid start q, first-hop bin i): per item the
+// first-hop point x1, its probability weight c * pi_i / Q, the features and
+// phi(x1) on the tensor cores, summed in FP64.  Fused, so nothing of size
+// Q x 200 is stored: each warp takes 32 items, stages their BF16 features
+// in shared memory and runs them as two 16-row MMA tiles.
+__global__ void __launch_bounds__(128) k_quad_mean(DevLayout L, double4 trect, int tid, const double4 *__restrict__ gauss,
+                                                   const double4 *__restrict__ sqs, const int *__restrict__ sides,
+                                                   uint32_t Q, const double *__restrict__ pi_exact,
+                                                   const double *__restrict__ wx, const double *__restrict__ wy,
+                                                   double eps, bool exact, const float *__restrict__ p,
+                                                   const __nv_bfloat16 *__restrict__ w1,
+                                                   const __nv_bfloat16 *__restrict__ w2, double *sum) {
+    __shared__ Smem S;
+    __shared__ uint32_t xs[4][32][kIn / 2];
+    load_net(S, p, w1, w2);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, tg = lane & 3;
+    const int64_t n = (int64_t)Q * FRW_NSAMPLE;
     const double4 g4 = gauss[0];
     const double perim = __dadd_rn(__dmul_rn(2.0, __dsub_rn(g4.z, g4.x)), __dmul_rn(2.0, __dsub_rn(g4.w, g4.y)));
-    const double4 s4 = sqs[q];
-    const double s[4] = {s4.x, s4.y, s4.z, s4.w};
-    double x1, y1;
-    point_from_index(s, i, exact, x1, y1);
-    const double a0 = __dsub_rn(s[2], s[0]);
-    const double nx = side == 1 ? 1.0 : (side == 3 ? -1.0 : 0.0);
-    const double ny = side == 2 ? 1.0 : (side == 0 ? -1.0 : 0.0);
-    const double dot = __dadd_rn(__dmul_rn(wx[i], nx), __dmul_rn(wy[i], ny));
-    const double c = __ddiv_rn(__dmul_rn(__dmul_rn(-eps, perim), dot), a0);
-    out[t] = make_double4(x1, y1, a0, c * pi_exact[i] / (double)Q);
+    double acc = 0.0;
+    for (int64_t b = ((int64_t)blockIdx.x * 4 + warp) * 32; b < n; b += (int64_t)gridDim.x * 128) {
+        const int64_t t = b + lane;
+        double wgt = 0.0;
+        float f[kIn];
+#pragma unroll
+        for (int k = 0; k < kIn; k++) f[k] = 0.f;
+        const int side = t < n ? sides[t / FRW_NSAMPLE] : -1;
+        if (side >= 0) {
+            const int i = (int)(t % FRW_NSAMPLE);
+            const double4 s4 = sqs[t / FRW_NSAMPLE];
+            const double sq[4] = {s4.x, s4.y, s4.z, s4.w};
+            double x1, y1;
+            point_from_index(sq, i, exact, x1, y1);
+            const double a0 = __dsub_rn(sq[2], sq[0]);
+            const double nx = side == 1 ? 1.0 : (side == 3 ? -1.0 : 0.0);
+            const double ny = side == 2 ? 1.0 : (side == 0 ? -1.0 : 0.0);
+            const double dot = __dadd_rn(__dmul_rn(wx[i], nx), __dmul_rn(wy[i], ny));
+            const double c = __ddiv_rn(__dmul_rn(__dmul_rn(-eps, perim), dot), a0);
+            wgt = c * pi_exact[i] / (double)Q;
+            edge_feats(x1, y1, trect.x, trect.y, trect.z, trect.w, a0, f);
+            const int k = nearest_other(L, x1, y1, tid);
+            if (k >= 0) {
+                const float4 o = __ldg(L.rects + k);
+                edge_feats(x1, y1, o.x, o.y, o.z, o.w, a0, f + 8);
+            } else {
+#pragma unroll
+                for (int q = 8; q < kIn; q++) f[q] = 16.f;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kIn / 2; k++) xs[warp][lane][k] = pack2(f[2 * k], f[2 * k + 1]);
+        __syncwarp();
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int ra = 16 * h + g, rb = ra + 8;
+            const uint32_t xa[4] = {xs[warp][ra][tg], xs[warp][rb][tg], xs[warp][ra][tg + 4], xs[warp][rb][tg + 4]};
+            float z1[8][4], z2[8][4], og, og8;
+            uint32_t a2[4][4];
+            tile_forward(S, xa, g, tg, z1, z2, a2, og, og8);
+            const double wa = __shfl_sync(kFull, wgt, ra), wb = __shfl_sync(kFull, wgt, rb);
+            if (tg == 0) acc += wa * (double)og + wb * (double)og8;
+        }
+        __syncwarp();
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) atomicAdd(sum, acc);
 }
 
 }  // namespace
@@ -732,25 +764,19 @@ frw_status launch_targets(const int64_t *end, const double4 *rec, int64_t n, int
     return FRW_OK;
 }
 
-frw_status launch_weighted_sum(const double4 *rec, const float *phi, int64_t n, double *sum, cudaStream_t st) {
-    if (n <= 0) return FRW_OK;
-    const int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
-    k_weighted_sum<<<blocks, 256, 0, st>>>(rec, phi, n, sum);
-    FRW_CK(cudaGetLastError());
-    return FRW_OK;
-}
 
-frw_status launch_quad_points(const DevLayout &L, const double4 *gauss, uint32_t Q, const double *pi_exact,
-                              const double *wx, const double *wy, double eps, bool exact, double4 *rec,
-                              cudaStream_t st) {
+frw_status launch_quad_mean(const DevLayout &L, double4 trect, int tid, const double4 *gauss, uint32_t Q,
+                            const double *pi_exact, const double *wx, const double *wy, double eps, bool exact,
+                            const Net &net, double *sum, cudaStream_t st) {
     double4 *sqs;
     int *sides;
     FRW_CK(cudaMallocAsync((void **)&sqs, (size_t)Q * sizeof(double4), st));
     FRW_CK(cudaMallocAsync((void **)&sides, (size_t)Q * sizeof(int), st));
     k_quad_starts<<<(Q + 127) / 128, 128, 0, st>>>(L, gauss, Q, sqs, sides);
     const int64_t n = (int64_t)Q * FRW_NSAMPLE;
-    k_quad_points<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(gauss, sqs, sides, Q, pi_exact, wx, wy, eps, exact,
-                                                               rec);
+    const int blocks = (int)std::min<int64_t>((n + 127) / 128, 148 * 8);
+    k_quad_mean<<<blocks, 128, 0, st>>>(L, trect, tid, gauss, sqs, sides, Q, pi_exact, wx, wy, eps, exact, net.p,
+                                        net.w1, net.w2, sum);
     cudaError_t e = cudaGetLastError();
     cudaFreeAsync(sqs, st);
     cudaFreeAsync(sides, st);

@@ -45,11 +45,10 @@ frw_status launch_adam(const Net &n, float *grad, float *m, float *v, int *step,
 // per walk: z = c (1{end==target} - phi); w = c 1{end==target}; sums of z, z^2, w, w^2
 frw_status launch_cv_reduce(const int64_t *end, const double4 *rec, const float *phi, int64_t n, int target,
                             double *sums /*4*/, cudaStream_t st);
-// exact mean: points and weights of the first-hop distribution on the grid start
-frw_status launch_quad_points(const DevLayout &L, const double4 *gauss, uint32_t Q, const double *pi_exact,
-                              const double *wx, const double *wy, double eps, bool exact_perimeter,
-                              double4 *rec /*Q*200: p1x, p1y, a0, weight*/, cudaStream_t st);
-frw_status launch_weighted_sum(const double4 *rec, const float *phi, int64_t n, double *sum, cudaStream_t st);
+// exact mean E[f] over every (grid start, first-hop bin) pair, accumulated into *sum
+frw_status launch_quad_mean(const DevLayout &L, double4 target_rect, int target_id, const double4 *gauss, uint32_t Q,
+                            const double *pi_exact, const double *wx, const double *wy, double eps,
+                            bool exact_perimeter, const Net &net, double *sum, cudaStream_t st);
 frw_status launch_targets(const int64_t *end, const double4 *rec, int64_t n, int target, float *y, float *wt,
                           double *wsum, cudaStream_t st);
 

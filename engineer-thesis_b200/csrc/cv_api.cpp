@@ -256,17 +256,12 @@ frw_status frw_cv_train(const frw_layout *layout, int64_t target, const frw_opts
         Buf B(st);
         const uint32_t Q = walk_opts->start_grid;
         const int64_t nq = (int64_t)Q * FRW_NSAMPLE;
-        double4 *d_gauss, *d_tgt, *d_q;
-        __nv_bfloat16 *d_xq;
-        float *d_phi;
+        double4 *d_gauss, *d_tgt;
         double *d_pi, *d_mu;
         uint32_t *d_status;
         cudaError_t e = cudaSuccess;
         if (e == cudaSuccess) e = B.get(&d_gauss, 32);
         if (e == cudaSuccess) e = B.get(&d_tgt, 32);
-        if (e == cudaSuccess) e = B.get(&d_q, nq * 32);
-        if (e == cudaSuccess) e = B.get(&d_xq, nq * 32);
-        if (e == cudaSuccess) e = B.get(&d_phi, nq * 4);
         if (e == cudaSuccess) e = B.get(&d_pi, FRW_NSAMPLE * 8);
         if (e == cudaSuccess) e = B.get(&d_mu, 8);
         if (e == cudaSuccess) e = B.get(&d_status, 4);
@@ -280,13 +275,11 @@ frw_status frw_cv_train(const frw_layout *layout, int64_t target, const frw_opts
         cudaMemsetAsync(d_status, 0, 4, st);
         rc = launch_gauss(v.dl, (const double *)d_tgt, 1, walk_opts->gauss_mode, walk_opts->gauss_param,
                           (double *)d_gauss, d_status, st);
-        if (!rc)
-            rc = cv::launch_quad_points(v.dl, d_gauss, Q, d_pi, tables + FRW_NSAMPLE + 1, tables + 2 * FRW_NSAMPLE + 1,
-                                        walk_opts->permittivity, walk_opts->exact_perimeter != 0, d_q, st);
         const double4 trect = make_double4(r[0], r[1], r[2], r[3]);
-        if (!rc) rc = cv::launch_features(v.dl, trect, (int)target, d_q, nq, d_xq, nullptr, st);
-        if (!rc) rc = cv::launch_forward(M->net, d_xq, nq, d_phi, st);
-        if (!rc) rc = cv::launch_weighted_sum(d_q, d_phi, nq, d_mu, st);
+        if (!rc)
+            rc = cv::launch_quad_mean(v.dl, trect, (int)target, d_gauss, Q, d_pi, tables + FRW_NSAMPLE + 1,
+                                      tables + 2 * FRW_NSAMPLE + 1, walk_opts->permittivity,
+                                      walk_opts->exact_perimeter != 0, M->net, d_mu, st);
         if (rc) return fail(rc);
         uint32_t hs = 0;
         e = cudaMemcpyAsync(&M->mean_term, d_mu, 8, cudaMemcpyDeviceToHost, st);

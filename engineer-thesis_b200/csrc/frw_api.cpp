@@ -437,18 +437,18 @@ frw_status frw_layout_create(const float *rects, int64_t n, const double *bounds
     cudaStream_t st = (cudaStream_t)stream;
     float4 *d_in = nullptr;
     auto fail = [&](frw_status r) {
-        if (d_in) cudaFree(d_in);
+        if (d_in) cudaFreeAsync(d_in, st);
         free_tree(&L->T);
         delete L;
         return r;
     };
-    cudaError_t e = cudaMalloc(&d_in, (size_t)n * 16);
-    if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc rects"));
+    cudaError_t e = cudaMallocAsync(&d_in, (size_t)n * 16, st);
+    if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMallocAsync rects"));
     e = cudaMemcpyAsync(d_in, rects, (size_t)n * 16, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return fail(cuda_fail(e, "upload rects"));
     rc = build_tree(d_in, (int32_t)n, L->bounds, L->leaf_max, st, &L->T, &L->build_ms);
     if (rc) return fail(rc);
-    cudaFree(d_in);
+    cudaFreeAsync(d_in, st);
     d_in = nullptr;
     DevLayout &dl = L->dl;
     dl.rects = L->T.rects;

@@ -39,8 +39,8 @@ __global__ void __launch_bounds__(128) k_box(DevLayout L, const double4 *__restr
 
 // RectHost::createGaussianSurface (CPU/rectHost.cpp:84-100).
 __device__ void scale_rect(const double r[4], double fx, double fy, double o[4]) {
-    const double mx = __ddiv_rn(__dadd_rn(r[0], r[2]), 2.0);
-    const double my = __ddiv_rn(__dadd_rn(r[1], r[3]), 2.0);
+    const double mx = __dmul_rn(__dadd_rn(r[0], r[2]), 0.5);
+    const double my = __dmul_rn(__dadd_rn(r[1], r[3]), 0.5);
     const double vx = __dmul_rn(__dsub_rn(r[0], mx), fx);
     const double vy = __dmul_rn(__dsub_rn(r[1], my), fy);
     o[0] = __dadd_rn(mx, vx);
@@ -61,7 +61,7 @@ __device__ double adjusted_factor(const DevLayout &L, const double r[4], double 
         const bool isc = box_collides(L, s, true, r, st);
         if (first && !isc) break;
         if ((isc && !dividing) || (!isc && dividing)) dividing = !dividing;
-        const double mid = __ddiv_rn(__dadd_rn(lb, rb), 2.0);
+        const double mid = __dmul_rn(__dadd_rn(lb, rb), 0.5);
         if (dividing) adj = rb = mid;
         else adj = lb = mid;
         first = false;

