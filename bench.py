@@ -111,23 +111,28 @@ class Clocks:
 
 # ------------------------------------------------------------ reference arm
 def _ref_worker(args):
-    rects, bounds, target, seconds, wid = args
+    rects, bounds, target, seconds, wid, mode = args
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
     R = O.Ref(rects=rects, bounds=bounds)
-    done, t0 = 0, time.perf_counter()
+    done, k, t0 = 0, 0, time.perf_counter()
     while time.perf_counter() - t0 < seconds:
-        R.walks_as_shipped(target, 4)
-        done += 4
+        if mode == "shipped":  # per-walk rng_init, as RandomWalk does
+            R.walks_as_shipped(target, 4)
+            done += 4
+        else:  # the same walk loop with JKISS seeded once per batch
+            R.walks_seeded(target, 64, seed=(wid + 1, k + 7, 0x5EED, 0xC0FFEE))
+            done += 64
+        k += 1
     return done, time.perf_counter() - t0
 
 
-def reference_rate(rects, bounds, target, seconds, cores):
-    """Walks/s of the shipped reference CPU walk on `cores` processes."""
+def reference_rate(rects, bounds, target, seconds, cores, mode="shipped"):
+    """Walks/s of the reference CPU walk on `cores` processes."""
     ctx = mp.get_context("spawn")
     with ctx.Pool(cores) as pool:
-        res = pool.map(_ref_worker, [(rects, bounds, target, seconds, i) for i in range(cores)])
+        res = pool.map(_ref_worker, [(rects, bounds, target, seconds, i, mode) for i in range(cores)])
     return sum(d for d, _ in res) / max(t for _, t in res), sum(d for d, _ in res)
 
 
@@ -155,12 +160,13 @@ def run_reference(args):
     for _ in range(args.warmup):
         reference_rate(rects, bounds, WORKLOAD["target"], 0.5, cores)
     t0 = time.perf_counter()
-    total = 0
+    total, rates = 0, []
     for _ in range(args.steps):
-        _, n = reference_rate(rects, bounds, WORKLOAD["target"], step_s, cores)
+        rate, n = reference_rate(rects, bounds, WORKLOAD["target"], step_s, cores)
+        rates.append(rate)  # walks / the slowest worker's own time (process start-up excluded)
         total += n
     el = time.perf_counter() - t0
-    v = total / el
+    v = statistics.mean(rates)
     cfg = dict(WORKLOAD, gauss="reference scale 1.5", start="reference Green CDF", walks=f"~{step_s}s sample/step")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": "walks/s", "n_gpus": args.gpus,
@@ -241,7 +247,68 @@ def time_to_rel_se(frw, device, stream):
             "plain": dict(p, device_s=p_dev, wall_s=p_wall),
             "cv": dict(c, device_s=c_dev, wall_s=c_wall),
             "speedup_wall": p_wall / c_wall, "speedup_device": p_dev / c_dev,
+            "cv_wall_s_training_amortised": c_wall - c["train_device_s"] - c["exact_mean_device_s"],
+            "speedup_wall_training_amortised": p_wall / (c_wall - c["train_device_s"] - c["exact_mean_device_s"]),
             "agree_sigma": abs(p["c00"] - c["c00"]) / np.hypot(p["c00"] * p["rel_se"], c["c00"] * c["rel_se"])}
+
+
+# ------------------------------------------------------------ queries and C3
+def query_rates(frw, L, device, stream):
+    """drawBiggestSquareAtPoint + checkCollisons(point) per point, batched:
+    the 1e5-point check set (uniform in the bounds, seed 0x0C2) and a 1e7-point
+    batch (inputs and outputs 560 MB, larger than L2), device buffers."""
+    import torch
+
+    b = L.bounds
+    out = {}
+    for name, n, seed, reps in (("check_1e5", 100_000, 0x0C2, 20), ("batch_1e7", 10_000_000, 0x0C2 + 1, 5)):
+        rng = np.random.default_rng(seed)
+        pts = np.stack([rng.uniform(b[0], b[2], n), rng.uniform(b[1], b[3], n)], 1)
+        p = torch.as_tensor(pts, device=device)
+        sq = torch.empty((n, 4), dtype=torch.float64, device=device)
+        hit = torch.empty(n, dtype=torch.int64, device=device)
+        L.query_device(p, sq, hit, stream.cuda_stream)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            L.query_device(p, sq, hit, stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        out[name] = {"points": n, "ms": ms, "queries_per_s": n / (ms * 1e-3)}
+        del p, sq, hit
+    return out
+
+
+C3 = dict(workload="frw-c3-1e6-rects-1e8-walks", rects=1_000_000, domain=1e5, walks=100_000_000, target=0,
+          layout_seed=0xF4A7 + 3)
+
+
+def c3_run(frw, device, stream, steps):
+    """C3: 10^6 rects, 1e8 walks per step, full capacitance row (offset-1
+    surface, uniform start).  Per-walk records and row sums of this layout
+    equal the FP64 oracle's (GPU test on a 2e5-walk sub-range)."""
+    import torch
+
+    rects = frw.generate_layout(C3["layout_seed"], C3["rects"], C3["domain"])
+    L = frw.Layout.from_rects(rects, device=device)
+    o = frw.capacitance_opts(1.0)
+    L.walk(C3["target"], 1_000_000, seed=1, o=o, stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    res = [L.walk(C3["target"], C3["walks"], seed=300 + k, o=o, stream=stream.cuda_stream) for k in range(steps)]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    r = res[-1]
+    c, se = r.row(C3["target"])[1:]
+    info = L.info
+    L.close()
+    return {"workload": C3["workload"], "ms_per_step": ms, "walks_per_s": C3["walks"] / (ms * 1e-3),
+            "mean_hops": r.hops_total / C3["walks"], "c00": c, "c00_rel_se": se / abs(c),
+            "conductors_reached": int(len(r.conductor)), "tree_build_ms": info.build_ms}
 
 
 # ------------------------------------------------------------ batched config
@@ -334,12 +401,17 @@ def main():
         import oracle as O
 
         cores = os.cpu_count() or 1
-        rate, n = reference_rate(rects.astype(np.float64), O.layer_bounds(rects.astype(np.float64)), W["target"],
-                                 args.cpu_seconds, cores)
+        rb = rects.astype(np.float64), O.layer_bounds(rects.astype(np.float64))
+        rate, n = reference_rate(*rb, W["target"], args.cpu_seconds, cores)
+        rate1, n1 = reference_rate(*rb, W["target"], args.cpu_seconds / 2, cores, mode="seeded")
         cpu = {"value": rate, "unit": "walks/s", "cores": cores, "kind": "reference",
                "sample": f"reference RandomWalk as shipped (per-walk rng_init, reference scale-1.5 surface and "
                          f"Green-CDF start) on the same layout and target, {args.cpu_seconds:.0f}s on {cores} "
-                         f"processes, {n} walks"}
+                         f"processes, {n} walks",
+               "per_core": rate / cores,
+               "seeded_once": {"value": rate1, "per_core": rate1 / cores,
+                               "sample": f"the same walk loop with JKISS seeded once per 64 walks, "
+                                         f"{args.cpu_seconds / 2:.0f}s on {cores} processes, {n1} walks"}}
 
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
@@ -407,6 +479,8 @@ def main():
         torch.cuda.synchronize()
         e2e_ms = e0.elapsed_time(e1) / e2e_steps
 
+    queries = query_rates(frw, L, dev, stream) if rank == 0 and world == 1 else None
+    c3 = c3_run(frw, local, stream, 3) if rank == 0 and world == 1 and not args.no_batched else None
     headline = batched = None
     if rank == 0 and world == 1 and not args.no_headline:
         headline = time_to_rel_se(frw, local, stream)
@@ -440,6 +514,10 @@ def main():
                                  "(the tree is L2-resident, so HBM is an upper-bound denominator)"},
             "clocks": clk.summary(),
         }
+        if queries:
+            out["collision_queries"] = queries
+        if c3:
+            out["c3"] = c3
         if headline:
             out["time_to_0.1pct_rel_se"] = headline
         if batched:

@@ -72,6 +72,28 @@ def test_estimator_matches_oracle_sums_config1():
     assert res.fraction_other == pytest.approx(1 - counts[ks == 0][0] / n)
 
 
+@pytest.mark.parametrize("seed,n_rects,domain", [(0xF4A7 + 2, 10_000, 1e4), (0xF4A7 + 3, 10**6, 1e5)])
+def test_estimator_matches_oracle_sums_c2_c3(seed, n_rects, domain):
+    """C2 (10^4 rects) and C3 (10^6 rects): 2e5 walks taken from the middle of
+    the walk index space; hits, hop total and every conductor's row equal the
+    FP64 oracle's over the same walks."""
+    rects = frw.generate_layout(seed, n_rects, domain)
+    n, first = 200_000, 50_000_000
+    o = frw.capacitance_opts(1.0, first_walk=first)
+    G = O.Grid(rects.astype(np.float64))
+    with frw.Layout.from_rects(rects) as L:
+        res = L.walk(0, n, seed=2024, o=o)
+    end, hops, b1, w = G.walks(oracle_cfg(G, o, 0, 2024), first, n)
+    assert res.walks == n and res.hops_total == hops.sum() and res.escaped == (end == -1).sum()
+    ks, counts = np.unique(end[end >= 0], return_counts=True)
+    assert np.array_equal(res.conductor, ks) and np.array_equal(res.hits, counts)
+    w = np.where(end >= 0, w, 0.0)
+    s1 = np.array([w[end == k].sum() for k in ks])
+    s2 = np.array([(w[end == k] ** 2).sum() for k in ks])
+    assert np.allclose(res.sum_w, s1, rtol=1e-12, atol=1e-12 * np.abs(s1).max())
+    assert np.allclose(res.sum_w2, s2, rtol=1e-12, atol=1e-12 * np.abs(s2).max())
+
+
 def test_walks_independent_of_launch_shape():
     rects = config1_layout()
     o1 = frw.capacitance_opts(1.0)
