@@ -1,0 +1,308 @@
+// cell_build.cu -- cell lists: a uniform grid over the layer bounds whose
+// cells list the rects a clearance query from inside the cell can need.
+//
+// For a point p of cell C with centre c and side s,
+//     d*(p) <= d*(c) + |p - c|_inf <= d*(c) + s/2 =: U_C
+// (d* is 1-Lipschitz in the L-inf norm, bounds distance included), and a
+// rect R with gap(R, p) <= d*(p) + 2 delta has L-inf distance to C at most
+// U_C + 2 delta.  So the rects touching C grown by
+//     r_C = max(U_C, 0) + 2 delta + margin
+// are every rect the query at p can find nearest, tied within 2 delta, or
+// containing p (max with 0).  The margin (M * 2^-30, M the layout's
+// coordinate scale) covers the rounding of the cell index of p and of the
+// cell's coordinates, both of order M * 2^-50.  Built from the tree: one
+// clearance query at each cell centre, then a count -> scan -> fill pair of
+// box enumerations.  Cells with more than max_per_cell rects keep count -1
+// and their points use the tree.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "query.cuh"
+
+namespace frw {
+namespace {
+
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+// Visits the tree's rects touching the closed box B, in tree order, until
+// visit() returns false.  Returns false when the traversal stack overflowed
+// (the visit is then incomplete).
+template <typename F>
+__device__ __forceinline__ bool touching(const DevLayout &L, const double B[4], F &&visit) {
+    int stk[kStackMax];
+    int sp = 1;
+    stk[0] = 0;
+    while (sp > 0) {
+        const int nd = stk[--sp];
+        const int4 rf = __ldg(L.nref + nd);
+        const int ref[4] = {rf.x, rf.y, rf.z, rf.w};
+        for (int c = 0; c < 4; c++) {
+            if (ref[c] == kRefEmpty) continue;
+            const float4 b = __ldg(L.nbox + 4 * nd + c);
+            if (!((double)b.z >= B[0] && B[2] >= (double)b.x && (double)b.w >= B[1] && B[3] >= (double)b.y))
+                continue;
+            if (ref[c] >= 0) {
+                if (sp == kStackMax) return false;
+                stk[sp++] = ref[c];
+                continue;
+            }
+            const int f = leaf_first(ref[c]), m = leaf_count(ref[c]);
+            for (int k = f; k < f + m; k++) {
+                const float4 r = __ldg(L.rects + k);
+                if ((double)r.z >= B[0] && B[2] >= (double)r.x && (double)r.w >= B[1] && B[3] >= (double)r.y)
+                    if (!visit(k, r)) return true;
+            }
+        }
+    }
+    return true;
+}
+
+struct Grid {
+    double gx0, gy0, side, margin;
+    int nx, ny;
+};
+
+__device__ __forceinline__ void cell_box(const DevLayout &L, const Grid &G, int64_t c, double B[4]) {
+    const int ix = (int)(c % G.nx), iy = (int)(c / G.nx);
+    const double x0 = G.gx0 + ix * G.side, y0 = G.gy0 + iy * G.side;
+    const double x1 = x0 + G.side, y1 = y0 + G.side;
+    Cands C;
+    int hit;
+    double best;
+    clearance(L, x0 + 0.5 * G.side, y0 + 0.5 * G.side, C, hit, best);  // L has no cells: the tree
+    const double r = fmax(best, 0.0) + 0.5 * G.side + 2.0 * L.delta + G.margin;
+    B[0] = x0 - r;
+    B[1] = y0 - r;
+    B[2] = x1 + r;
+    B[3] = y1 + r;
+}
+
+// Per cell: its list length, or -1 (in cells[c].y) when it exceeds cap or
+// the enumeration was incomplete; cnt[c] = entries to reserve.
+__global__ void k_cell_count(DevLayout L, Grid G, int cap, int64_t *__restrict__ cnt, int2 *__restrict__ cells,
+                             unsigned long long *overflow, int64_t ncells) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncells) return;
+    double B[4];
+    cell_box(L, G, c, B);
+    int n = 0;
+    const bool complete = touching(L, B, [&](int, float4) { return ++n <= cap; });
+    const bool ok = complete && n <= cap;
+    cnt[c] = ok ? n : 0;
+    cells[c] = make_int2(0, ok ? n : -1);
+    if (!ok) atomicAdd(overflow, 1ull);
+}
+
+// Writes the lists of the cells that did not overflow (the enumeration order
+// is deterministic, so it meets the same rects as the count).
+__global__ void k_cell_fill(DevLayout L, Grid G, const int64_t *__restrict__ start, int2 *__restrict__ cells,
+                            float4 *__restrict__ crects, int32_t *__restrict__ cids, int64_t ncells) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncells) return;
+    const int m = cells[c].y;
+    if (m < 0) return;
+    double B[4];
+    cell_box(L, G, c, B);
+    const int64_t s = start[c];
+    int n = 0;
+    touching(L, B, [&](int k, float4 r) {
+        if (n >= m) return false;
+        crects[s + n] = r;
+        cids[s + n] = __ldg(L.ids + k);
+        return ++n < m;
+    });
+    cells[c] = make_int2((int)s, m);
+}
+
+// Exclusive scan of int64 values: tile sums, a one-block scan of the tile
+// sums, then each tile rescanned with its offset.
+__device__ __forceinline__ int64_t block_excl_scan(int64_t v, int64_t *warp_tot, int64_t &total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int64_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int64_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_tot[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int64_t t = lane < kScanThreads / 32 ? warp_tot[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int64_t y = __shfl_up_sync(0xFFFFFFFFu, t, o);
+            if (lane >= o) t += y;
+        }
+        warp_tot[lane] = t;  // inclusive over warps
+    }
+    __syncthreads();
+    total = warp_tot[kScanThreads / 32 - 1];
+    const int64_t before = w ? warp_tot[w - 1] : 0;
+    __syncthreads();
+    return before + x - v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_tile_sums(const int64_t *__restrict__ in, int64_t n,
+                                                          int64_t *__restrict__ sums) {
+    __shared__ int64_t wt[32];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    int64_t s = 0;
+    for (int k = 0; k < kScanItems; k++)
+        if (base + k < n) s += in[base + k];
+    int64_t total;
+    block_excl_scan(s, wt, total);
+    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_sums(int64_t *sums, int64_t n, int64_t *grand) {
+    __shared__ int64_t wt[32];
+    int64_t carry = 0;
+    for (int64_t b = 0; b < n; b += kScanThreads) {
+        const int64_t i = b + threadIdx.x;
+        const int64_t v = i < n ? sums[i] : 0;
+        int64_t total;
+        const int64_t e = block_excl_scan(v, wt, total);
+        if (i < n) sums[i] = carry + e;
+        carry += total;
+    }
+    if (threadIdx.x == 0) *grand = carry;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_tile_scan(const int64_t *__restrict__ in, int64_t n,
+                                                          const int64_t *__restrict__ offs,
+                                                          int64_t *__restrict__ out) {
+    __shared__ int64_t wt[32];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    int64_t v[kScanItems], s = 0;
+    for (int k = 0; k < kScanItems; k++) {
+        v[k] = base + k < n ? in[base + k] : 0;
+        s += v[k];
+    }
+    int64_t total;
+    int64_t run = offs[blockIdx.x] + block_excl_scan(s, wt, total);
+    for (int k = 0; k < kScanItems; k++) {
+        if (base + k < n) out[base + k] = run;
+        run += v[k];
+    }
+}
+
+}  // namespace
+
+void free_cells(CellBuffers *c) {
+    cudaFree(c->cells);
+    cudaFree(c->crects);
+    cudaFree(c->cids);
+    *c = CellBuffers();
+}
+
+void attach_cells(DevLayout &L, const CellBuffers &c) {
+    L.cells = c.cells;
+    L.crects = c.crects;
+    L.cids = c.cids;
+    L.gx0 = c.gx0;
+    L.gy0 = c.gy0;
+    L.ginv = c.ginv;
+    L.gnx = c.nx;
+    L.gny = c.ny;
+}
+
+frw_status build_cells(const DevLayout &Lin, double cells_per_rect, int cap, cudaStream_t st, CellBuffers *out) {
+    *out = CellBuffers();
+    if (!(cells_per_rect > 0) || cap < 1 || cap > (1 << 16)) {
+        set_error("build_cells: cells_per_rect must be > 0 and max_per_cell in [1, 65536]");
+        return FRW_E_ARG;
+    }
+    DevLayout L = Lin;
+    L.cells = nullptr;  // the build queries the tree
+    const double W = L.bx1 - L.bx0, H = L.by1 - L.by0;
+    const double target = std::min((double)kMaxCells, std::max(1.0, cells_per_rect * (double)L.n));
+    double side = std::sqrt(std::max(W * H, 1e-300) / target);
+    if (!(side > 0) || !std::isfinite(side)) side = std::max(std::max(W, H), 1.0);
+    side = std::max(side, std::max(W, H) / 65536.0);  // at most 2^16 cells per axis
+    if (!(side > 0)) side = 1.0;
+    int64_t nx = 0, ny = 0;
+    for (;;) {
+        nx = std::max<int64_t>(1, (int64_t)std::ceil(W / side));
+        ny = std::max<int64_t>(1, (int64_t)std::ceil(H / side));
+        if (nx * ny <= kMaxCells && nx <= 65536 && ny <= 65536) break;
+        side *= 1.25;
+    }
+    const int64_t ncells = nx * ny;
+    const double M = 4.0 * std::max(std::max(std::max(std::fabs(L.bx0), std::fabs(L.by0)),
+                                             std::max(std::fabs(L.bx1), std::fabs(L.by1))),
+                                    std::max(W, H)) +
+                     16.0;
+    Grid G{L.bx0, L.by0, side, std::ldexp(M, -30), (int)nx, (int)ny};
+
+    cudaEvent_t e0, e1;
+    FRW_CK(cudaEventCreate(&e0));
+    FRW_CK(cudaEventCreate(&e1));
+    CellBuffers C;
+    C.ncells = ncells;
+    C.nx = (int)nx;
+    C.ny = (int)ny;
+    C.gx0 = G.gx0;
+    C.gy0 = G.gy0;
+    C.side = side;
+    C.ginv = 1.0 / side;
+    int64_t *cnt = nullptr, *start = nullptr, *sums = nullptr, *grand = nullptr;
+    unsigned long long *ovf = nullptr;
+    const int64_t tiles = (ncells + kScanTile - 1) / kScanTile;
+    frw_status rc = FRW_OK;
+    auto ck = [&](cudaError_t e, const char *what) {
+        if (e != cudaSuccess && rc == FRW_OK) rc = cuda_fail(e, what);
+        return rc == FRW_OK;
+    };
+    do {
+        if (!ck(cudaMalloc(&C.cells, (size_t)ncells * sizeof(int2)), "malloc cells")) break;
+        if (!ck(cudaEventRecord(e0, st), "event")) break;
+        if (!ck(cudaMallocAsync(&cnt, (size_t)ncells * 8, st), "malloc cell counts")) break;
+        if (!ck(cudaMallocAsync(&start, (size_t)ncells * 8, st), "malloc cell starts")) break;
+        if (!ck(cudaMallocAsync(&sums, (size_t)tiles * 8, st), "malloc tile sums")) break;
+        if (!ck(cudaMallocAsync(&grand, 8, st), "malloc total")) break;
+        if (!ck(cudaMallocAsync(&ovf, 8, st), "malloc overflow count")) break;
+        if (!ck(cudaMemsetAsync(ovf, 0, 8, st), "memset")) break;
+        const unsigned blocks = (unsigned)((ncells + 127) / 128);
+        k_cell_count<<<blocks, 128, 0, st>>>(L, G, cap, cnt, C.cells, ovf, ncells);
+        k_tile_sums<<<(unsigned)tiles, kScanThreads, 0, st>>>(cnt, ncells, sums);
+        k_scan_sums<<<1, kScanThreads, 0, st>>>(sums, tiles, grand);
+        k_tile_scan<<<(unsigned)tiles, kScanThreads, 0, st>>>(cnt, ncells, sums, start);
+        if (!ck(cudaGetLastError(), "cell count")) break;
+        int64_t total = 0;
+        unsigned long long novf = 0;
+        if (!ck(cudaMemcpyAsync(&total, grand, 8, cudaMemcpyDeviceToHost, st), "cell total")) break;
+        if (!ck(cudaMemcpyAsync(&novf, ovf, 8, cudaMemcpyDeviceToHost, st), "cell overflow")) break;
+        if (!ck(cudaStreamSynchronize(st), "cell total")) break;
+        if (total > INT32_MAX) {
+            set_error("build_cells: more than 2^31 list entries; use fewer cells per rect");
+            rc = FRW_E_ARG;
+            break;
+        }
+        C.entries = total;
+        C.overflow = (int64_t)novf;
+        if (!ck(cudaMalloc(&C.crects, (size_t)std::max<int64_t>(total, 1) * 16), "malloc cell rects")) break;
+        if (!ck(cudaMalloc(&C.cids, (size_t)std::max<int64_t>(total, 1) * 4), "malloc cell ids")) break;
+        if (total > 0) k_cell_fill<<<blocks, 128, 0, st>>>(L, G, start, C.cells, C.crects, C.cids, ncells);
+        if (!ck(cudaGetLastError(), "cell fill")) break;
+        if (!ck(cudaEventRecord(e1, st), "event")) break;
+        if (!ck(cudaEventSynchronize(e1), "cell sync")) break;
+        cudaEventElapsedTime(&C.build_ms, e0, e1);
+    } while (0);
+    for (void *p : {(void *)cnt, (void *)start, (void *)sums, (void *)grand, (void *)ovf})
+        if (p) cudaFreeAsync(p, st);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != FRW_OK) {
+        free_cells(&C);
+        return rc;
+    }
+    C.bytes = ncells * (int64_t)sizeof(int2) + C.entries * 20;
+    *out = C;
+    return FRW_OK;
+}
+
+}  // namespace frw

@@ -26,6 +26,7 @@ struct frw_layout {
     std::vector<double> rects;  // layer order, as given
     double bounds[4] = {0, 0, 0, 0};
     frw::TreeBuffers T;
+    frw::CellBuffers cells;
     frw::DevLayout dl{};
     float build_ms = 0.f;
     int leaf_max = frw::kDefaultLeafMax;
@@ -439,6 +440,7 @@ frw_status frw_layout_create(const float *rects, int64_t n, const double *bounds
     auto fail = [&](frw_status r) {
         if (d_in) cudaFreeAsync(d_in, st);
         free_tree(&L->T);
+        free_cells(&L->cells);
         delete L;
         return r;
     };
@@ -482,6 +484,9 @@ frw_status frw_layout_create(const float *rects, int64_t n, const double *bounds
     }
     dl.n = (int32_t)n;
     dl.nodes = L->T.nodes;
+    rc = build_cells(dl, kDefaultCellsPerRect, kDefaultCellMax, st, &L->cells);
+    if (rc) return fail(rc);
+    attach_cells(dl, L->cells);
     *out = L;
     return FRW_OK;
 }
@@ -517,6 +522,7 @@ frw_status frw_layout_destroy(frw_layout *L) {
     if (!L) return FRW_OK;
     DeviceGuard g(L->device);
     free_tree(&L->T);
+    free_cells(&L->cells);
     delete L;
     return FRW_OK;
 }
@@ -534,6 +540,51 @@ frw_status frw_layout_info_get(const frw_layout *L, frw_layout_info *info) {
     info->device_bytes = L->T.bytes;
     info->device = L->device;
     info->build_ms = L->build_ms;
+    return FRW_OK;
+}
+
+frw_status frw_layout_set_cells(frw_layout *L, double cells_per_rect, int max_per_cell, void *stream) {
+    if (!L) {
+        set_error("null layout");
+        return FRW_E_ARG;
+    }
+    if (cells_per_rect < 0 || !std::isfinite(cells_per_rect)) {
+        set_error("frw_layout_set_cells: cells_per_rect must be finite and >= 0");
+        return FRW_E_ARG;
+    }
+    DeviceGuard g(L->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    FRW_CK(cudaStreamSynchronize(st));
+    CellBuffers c;
+    if (cells_per_rect > 0) {
+        DevLayout tree_only = L->dl;
+        tree_only.cells = nullptr;
+        frw_status rc = build_cells(tree_only, cells_per_rect, max_per_cell > 0 ? max_per_cell : kDefaultCellMax,
+                                    st, &c);
+        if (rc) return rc;
+    }
+    FRW_CK(cudaDeviceSynchronize());  // no launch may still read the old lists
+    free_cells(&L->cells);
+    L->cells = c;
+    L->dl.cells = nullptr;
+    if (c.cells) attach_cells(L->dl, c);
+    return FRW_OK;
+}
+
+frw_status frw_layout_cells_info(const frw_layout *L, frw_cells_info *info) {
+    if (!L || !info) {
+        set_error("null argument");
+        return FRW_E_ARG;
+    }
+    const CellBuffers &c = L->cells;
+    info->cells = c.ncells;
+    info->nx = c.nx;
+    info->ny = c.ny;
+    info->cell_side = c.side;
+    info->entries = c.entries;
+    info->overflow_cells = c.overflow;
+    info->device_bytes = c.bytes;
+    info->build_ms = c.build_ms;
     return FRW_OK;
 }
 

@@ -42,6 +42,14 @@ struct DevLayout {
     double delta;               // tie window of the clearance replay (see query.cuh)
     float slack;                // FP32 pre-filter margin: 4 ulp_f32(max |bound|)
     int32_t n, nodes;
+    // cell lists (optional, cells == nullptr: tree only): a gnx x gny grid of
+    // side 1/ginv from (gx0, gy0); cell (start, count) into crects / cids,
+    // count < 0 when the cell overflowed and its points use the tree
+    const int2 *cells;
+    const float4 *crects;
+    const int32_t *cids;
+    double gx0, gy0, ginv;
+    int32_t gnx, gny;
 };
 
 // ---- device status word (atomicOr'ed by kernels, read back by the host) ----
@@ -121,6 +129,26 @@ struct TreeBuffers {
 frw_status build_tree(const float4 *d_rects_in, int32_t n, const double bounds[4], int leaf_max,
                       cudaStream_t stream, TreeBuffers *out, float *build_ms);
 void free_tree(TreeBuffers *t);
+
+// Cell lists over a built tree (DevLayout L with cells == nullptr): every
+// rect whose L-inf distance to a cell can be within 2 delta of the clearance
+// of a point of the cell, per cell, at most max_per_cell of them.
+struct CellBuffers {
+    int2 *cells = nullptr;
+    float4 *crects = nullptr;
+    int32_t *cids = nullptr;
+    int64_t ncells = 0, entries = 0, overflow = 0, bytes = 0;
+    double gx0 = 0, gy0 = 0, side = 0, ginv = 0;
+    int32_t nx = 0, ny = 0;
+    float build_ms = 0.f;
+};
+constexpr double kDefaultCellsPerRect = 8.0;
+constexpr int kDefaultCellMax = 32;
+constexpr int64_t kMaxCells = 1ll << 26;
+frw_status build_cells(const DevLayout &L, double cells_per_rect, int max_per_cell, cudaStream_t stream,
+                       CellBuffers *out);
+void free_cells(CellBuffers *c);
+void attach_cells(DevLayout &L, const CellBuffers &c);
 
 // query.cu
 frw_status launch_query(const DevLayout &L, const double *d_pts, int64_t n, double *d_sq,

@@ -31,8 +31,9 @@ constexpr int kNoHit = 0x7FFFFFFF;
 constexpr double kMinDist = (double).095f;  // drawBiggestSquareAtPoint MIN_DIST
 
 struct Cands {
-    int idx[kCandMax];  // Morton positions of the near-tied rects
-    float g[kCandMax];  // their gaps, rounded down (keeping extra entries is harmless)
+    const float4 *base;  // the array idx[] points into: the tree's rects or a cell list
+    int idx[kCandMax];   // positions of the near-tied rects in base
+    float g[kCandMax];   // their gaps, rounded down (keeping extra entries is harmless)
     int n;
 };
 
@@ -41,10 +42,52 @@ __device__ __forceinline__ float lb_box_f(const float4 b, float px, float py) {
     return fmaxf(fmaxf(fmaxf(b.x - px, px - b.z), fmaxf(b.y - py, py - b.w)), 0.f);
 }
 
-// One depth-first, nearest-child-first traversal.  Node boxes and rect gaps
-// are screened in FP32 (errors below L.slack); only rects that can matter --
-// inside the current tie window or containing p -- get the exact FP64 gap.
-// Returns status bits.
+// One rect of a leaf or a cell list: FP32 screen, then the exact FP64 gap;
+// tightens `best`, keeps the near-tie list and the containing rect.
+__device__ __forceinline__ void scan_rect(const float4 r, int k, const int32_t *ids, double px, double py,
+                                          float pxf, float pyf, double r2, float slack, float &limf,
+                                          double &best, int &hit, Cands &C, uint32_t &st) {
+    const float gf = fmaxf(fmaxf(r.x - pxf, pxf - r.z), fmaxf(r.y - pyf, pyf - r.w));
+    if (gf > limf) return;
+    const double x0 = r.x, y0 = r.y, x1 = r.z, y1 = r.w;
+    const double g = fmax(fmax(x0 - px, px - x1), fmax(y0 - py, py - y1));
+    if (g <= 0.0 && px >= x0 && py >= y0 && px <= x1 && py <= y1) {
+        const int id = __ldg(ids + k);
+        hit = id < hit ? id : hit;
+    }
+    if (g < best) {
+        best = g;
+        limf = (float)(fmax(best, 0.0) + r2) + slack;
+        int j = 0;
+        for (int q = 0; q < C.n; q++)
+            if ((double)C.g[q] <= best + r2) {
+                C.idx[j] = C.idx[q];
+                C.g[j] = C.g[q];
+                j++;
+            }
+        C.n = j;
+    }
+    if (g <= best + r2) {
+        if (C.n < kCandMax) {
+            C.idx[C.n] = k;
+            C.g[C.n] = __double2float_rd(g);
+            C.n++;
+        } else {
+            st |= kStCandOverflow;
+        }
+    }
+}
+
+// The clearance of p and its near-tie list.  With cell lists the list of
+// p's cell holds every rect that can come within 2*delta of the clearance of
+// any point of the cell (the cell's radius is bounded by the clearance of
+// its centre plus half a side, with a margin far above the rounding of the
+// cell index), so scanning it gives the same d*, the same containing rect and
+// a superset of the same ties as the whole tree.  Otherwise (no cell lists,
+// or an overflowed cell): one depth-first, nearest-child-first traversal.
+// Node boxes and rect gaps are screened in FP32 (errors below L.slack); only
+// rects that can matter -- inside the current tie window or containing p --
+// get the exact FP64 gap.  Returns status bits.
 __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, double py, Cands &C,
                                               int &hit, double &best) {
     uint32_t st = 0;
@@ -52,11 +95,25 @@ __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, dou
     best = fmin(fmin(px - L.bx0, L.bx1 - px), fmin(py - L.by0, L.by1 - py));
     hit = kNoHit;
     C.n = 0;
+    C.base = L.rects;
     // outside the closed bounds no rect can contain p and p+-1 already
     // leaves the bounds: nothing to look up
     if (!(px >= L.bx0 && py >= L.by0 && px <= L.bx1 && py <= L.by1)) return 0;
     const float pxf = (float)px, pyf = (float)py, slack = L.slack;
     float limf = (float)(fmax(best, 0.0) + r2) + slack;  // screen: FP32 value > limf => exact > limit
+    if (L.cells) {
+        int ix = (int)__dmul_rn(__dsub_rn(px, L.gx0), L.ginv);
+        int iy = (int)__dmul_rn(__dsub_rn(py, L.gy0), L.ginv);
+        ix = ix < 0 ? 0 : (ix >= L.gnx ? L.gnx - 1 : ix);
+        iy = iy < 0 ? 0 : (iy >= L.gny ? L.gny - 1 : iy);
+        const int2 ce = __ldg(L.cells + (int64_t)iy * L.gnx + ix);
+        if (ce.y >= 0) {
+            C.base = L.crects;
+            for (int k = ce.x; k < ce.x + ce.y; k++)
+                scan_rect(__ldg(L.crects + k), k, L.cids, px, py, pxf, pyf, r2, slack, limf, best, hit, C, st);
+            return st;
+        }
+    }
     int stk_node[kStackMax];
     float stk_lb[kStackMax];
     int sp = 0;
@@ -78,38 +135,8 @@ __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, dou
         for (int c = 0; c < 4; c++) {
             if (ref[c] >= kRefEmpty || lb[c] > limf) continue;
             const int f = leaf_first(ref[c]), m = leaf_count(ref[c]);
-            for (int k = f; k < f + m; k++) {
-                const float4 r = __ldg(L.rects + k);
-                const float gf = fmaxf(fmaxf(r.x - pxf, pxf - r.z), fmaxf(r.y - pyf, pyf - r.w));
-                if (gf > limf) continue;
-                const double x0 = r.x, y0 = r.y, x1 = r.z, y1 = r.w;
-                const double g = fmax(fmax(x0 - px, px - x1), fmax(y0 - py, py - y1));
-                if (g <= 0.0 && px >= x0 && py >= y0 && px <= x1 && py <= y1) {
-                    const int id = __ldg(L.ids + k);
-                    hit = id < hit ? id : hit;
-                }
-                if (g < best) {
-                    best = g;
-                    limf = (float)(fmax(best, 0.0) + r2) + slack;
-                    int j = 0;
-                    for (int q = 0; q < C.n; q++)
-                        if ((double)C.g[q] <= best + r2) {
-                            C.idx[j] = C.idx[q];
-                            C.g[j] = C.g[q];
-                            j++;
-                        }
-                    C.n = j;
-                }
-                if (g <= best + r2) {
-                    if (C.n < kCandMax) {
-                        C.idx[C.n] = k;
-                        C.g[C.n] = __double2float_rd(g);
-                        C.n++;
-                    } else {
-                        st |= kStCandOverflow;
-                    }
-                }
-            }
+            for (int k = f; k < f + m; k++)
+                scan_rect(__ldg(L.rects + k), k, L.ids, px, py, pxf, pyf, r2, slack, limf, best, hit, C, st);
         }
         // internal children within reach: visit the nearest next, stack the rest
         int next = -1;
@@ -159,7 +186,7 @@ __device__ __forceinline__ void load_listed(const DevLayout &L, const Cands &C, 
     T.n = C.n;
 #pragma unroll
     for (int q = 0; q < 2; q++) {
-        const float4 r = q < C.n ? __ldg(L.rects + C.idx[q]) : make_float4(1.f, 1.f, 0.f, 0.f);
+        const float4 r = q < C.n ? __ldg(C.base + C.idx[q]) : make_float4(1.f, 1.f, 0.f, 0.f);
         T.x0[q] = r.x;
         T.y0[q] = r.y;
         T.x1[q] = r.z;
@@ -174,7 +201,7 @@ __device__ __forceinline__ bool collides_listed(const DevLayout &L, const Cands 
     for (int q = 0; q < 2; q++)
         if (q < T.n && T.x1[q] >= o[0] && o[2] >= T.x0[q] && T.y1[q] >= o[1] && o[3] >= T.y0[q]) return true;
     for (int q = 2; q < T.n; q++) {
-        const float4 r = __ldg(L.rects + C.idx[q]);
+        const float4 r = __ldg(C.base + C.idx[q]);
         if ((double)r.z >= o[0] && o[2] >= (double)r.x && (double)r.w >= o[1] && o[3] >= (double)r.y)
             return true;
     }

@@ -143,6 +143,19 @@ class LayoutInfo(C.Structure):
     ]
 
 
+class CellsInfo(C.Structure):
+    _fields_ = [
+        ("cells", C.c_int64),
+        ("nx", C.c_int32),
+        ("ny", C.c_int32),
+        ("cell_side", C.c_double),
+        ("entries", C.c_int64),
+        ("overflow_cells", C.c_int64),
+        ("device_bytes", C.c_int64),
+        ("build_ms", C.c_double),
+    ]
+
+
 _D = C.POINTER(C.c_double)
 _F = C.POINTER(C.c_float)
 _I64 = C.POINTER(C.c_int64)
@@ -160,6 +173,8 @@ _SIGS = {
     "frw_layout_destroy": ([_VP], C.c_int),
     "frw_layout_info_get": ([_VP, C.POINTER(LayoutInfo)], C.c_int),
     "frw_layout_rects": ([_VP, _D], C.c_int),
+    "frw_layout_set_cells": ([_VP, C.c_double, C.c_int, _VP], C.c_int),
+    "frw_layout_cells_info": ([_VP, C.POINTER(CellsInfo)], C.c_int),
     "frw_query_batch": ([_VP, _VP, C.c_int64, _VP, _VP, C.c_int, _VP], C.c_int),
     "frw_box_collides_batch": ([_VP, _VP, C.c_int64, _D, _VP, C.c_int, _VP], C.c_int),
     "frw_opts_default": ([C.POINTER(Opts)], None),
@@ -348,6 +363,17 @@ class Layout:
         out = np.zeros((self.n, 4))
         _check(lib().frw_layout_rects(self._h, _ptr(out, _D)))
         return out
+
+    # ---- cell lists
+    def set_cells(self, cells_per_rect: float, max_per_cell: int = 32):
+        """Rebuild the cell lists (0 removes them: queries use the tree alone)."""
+        _check(lib().frw_layout_set_cells(self._h, float(cells_per_rect), int(max_per_cell), None))
+
+    @property
+    def cells(self) -> CellsInfo:
+        i = CellsInfo()
+        _check(lib().frw_layout_cells_info(self._h, C.byref(i)))
+        return i
 
     # ---- queries
     def query(self, pts):

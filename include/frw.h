@@ -96,6 +96,28 @@ typedef struct frw_layout_info {
     double build_ms;       /* device time of the last tree build */
 } frw_layout_info;
 frw_status frw_layout_info_get(const frw_layout *layout, frw_layout_info *info);
+/* Cell lists (no counterpart in the reference, which answers every query
+ * from its quadtree, CPU/quadTree.cpp:148-312): a uniform grid over the
+ * layer bounds whose cells each list every rect that a clearance query from
+ * inside the cell can find nearest, tied or containing the point.  Queries
+ * scan their cell's list instead of descending the tree; cells whose list
+ * would exceed max_per_cell fall back to the tree.  Results are identical
+ * with and without them.  frw_layout_create builds them with 8 cells per rect
+ * and at most 32 rects per cell; frw_layout_set_cells rebuilds them
+ * (cells_per_rect = 0 removes them).  It synchronises the device and must
+ * not run while another call uses the layout, nor while a batch or a control
+ * variate built on it exists. */
+typedef struct frw_cells_info {
+    int64_t cells;           /* nx * ny, 0 when the layout has none */
+    int32_t nx, ny;
+    double cell_side;
+    int64_t entries;         /* list entries in all cells */
+    int64_t overflow_cells;  /* cells answered by the tree */
+    int64_t device_bytes;
+    double build_ms;
+} frw_cells_info;
+frw_status frw_layout_set_cells(frw_layout *layout, double cells_per_rect, int max_per_cell, void *stream);
+frw_status frw_layout_cells_info(const frw_layout *layout, frw_cells_info *info);
 /* Copies the layout's rects (layer order, as doubles) to a host array n*4. */
 frw_status frw_layout_rects(const frw_layout *layout, double *out_xyxy);
 
