@@ -142,7 +142,7 @@ struct CellBuffers {
     int32_t nx = 0, ny = 0;
     float build_ms = 0.f;
 };
-constexpr double kDefaultCellsPerRect = 8.0;
+constexpr double kDefaultCellsPerRect = 16.0;
 constexpr int kDefaultCellMax = 32;
 constexpr int64_t kMaxCells = 1ll << 26;
 frw_status build_cells(const DevLayout &L, double cells_per_rect, int max_per_cell, cudaStream_t stream,

@@ -175,32 +175,12 @@ __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, dou
 }
 
 // Tree::checkCollisions(box) restricted to the near-tie list (exact for the
-// boxes of the replay, see the file comment).  The first two listed rects
-// are held as doubles for the whole replay; further ones (rare) are read back.
-struct Listed {
-    double x0[2], y0[2], x1[2], y1[2];
-    int n;
-};
-
-__device__ __forceinline__ void load_listed(const DevLayout &L, const Cands &C, Listed &T) {
-    T.n = C.n;
-#pragma unroll
-    for (int q = 0; q < 2; q++) {
-        const float4 r = q < C.n ? __ldg(C.base + C.idx[q]) : make_float4(1.f, 1.f, 0.f, 0.f);
-        T.x0[q] = r.x;
-        T.y0[q] = r.y;
-        T.x1[q] = r.z;
-        T.y1[q] = r.w;
-    }
-}
-
-__device__ __forceinline__ bool collides_listed(const DevLayout &L, const Cands &C, const Listed &T,
-                                                const double o[4]) {
+// boxes of the replay, see the file comment).  Only boxes within delta of the
+// clearance get here (rarely), so the listed rects are read back on demand
+// rather than held in registers through the whole replay.
+__device__ __forceinline__ bool collides_listed(const DevLayout &L, const Cands &C, const double o[4]) {
     if (!(o[1] >= L.by0 && o[0] >= L.bx0 && o[3] <= L.by1 && o[2] <= L.bx1)) return true;
-#pragma unroll
-    for (int q = 0; q < 2; q++)
-        if (q < T.n && T.x1[q] >= o[0] && o[2] >= T.x0[q] && T.y1[q] >= o[1] && o[3] >= T.y0[q]) return true;
-    for (int q = 2; q < T.n; q++) {
+    for (int q = 0; q < C.n; q++) {
         const float4 r = __ldg(C.base + C.idx[q]);
         if ((double)r.z >= o[0] && o[2] >= (double)r.x && (double)r.w >= o[1] && o[3] >= (double)r.y)
             return true;
@@ -214,12 +194,12 @@ __device__ __forceinline__ bool collides_listed(const DevLayout &L, const Cands 
 // extents above d* means the nearest obstacle (bounds side or listed rect) is
 // touched; all below means nothing can be.  Only boxes within delta of d*
 // take the exact predicate.
-__device__ __forceinline__ bool collides_box(const DevLayout &L, const Cands &C, const Listed &T,
-                                             const double o[4], double px, double dstar) {
+__device__ __forceinline__ bool collides_box(const DevLayout &L, const Cands &C, const double o[4], double px,
+                                             double dstar) {
     const double e = __dsub_rn(o[2], px);
     if (e > dstar + L.delta) return true;
     if (e < dstar - L.delta) return false;
-    return collides_listed(L, C, T, o);
+    return collides_listed(L, C, o);
 }
 
 // drawBiggestSquareAtPoint replayed on scalars: same operations, same order,
@@ -228,16 +208,14 @@ __device__ __forceinline__ bool collides_box(const DevLayout &L, const Cands &C,
 // results are identical (subnormals included), without the division sequence.
 __device__ __forceinline__ uint32_t replay_square(const DevLayout &L, const Cands &C, double px,
                                                   double py, double dstar, double sq[4]) {
-    Listed T;
-    load_listed(L, C, T);
     double o[4] = {__dsub_rn(px, 1.0), __dsub_rn(py, 1.0), __dadd_rn(px, 1.0), __dadd_rn(py, 1.0)};
-    if (collides_box(L, C, T, o, px, dstar)) {
+    if (collides_box(L, C, o, px, dstar)) {
         sq[0] = o[0]; sq[1] = o[1]; sq[2] = o[2]; sq[3] = o[3];
         return 0;
     }
     const double in2[4] = {__dsub_rn(px, 2.0), __dsub_rn(py, 2.0), __dadd_rn(px, 2.0),
                            __dadd_rn(py, 2.0)};
-    if (collides_box(L, C, T, in2, px, dstar)) {
+    if (collides_box(L, C, in2, px, dstar)) {
         sq[0] = in2[0]; sq[1] = in2[1]; sq[2] = in2[2]; sq[3] = in2[3];
         return 0;
     }
@@ -245,7 +223,7 @@ __device__ __forceinline__ uint32_t replay_square(const DevLayout &L, const Cand
     bool maxReached = false, isc;
     uint32_t st = 0;
     int it = 0;
-    while ((isc = collides_box(L, C, T, o, px, dstar)) || !maxReached || dist > kMinDist) {
+    while ((isc = collides_box(L, C, o, px, dstar)) || !maxReached || dist > kMinDist) {
         if (isc) {
             if (dist > kMinDist) dist = __dmul_rn(dist, 0.5);
             maxReached = true;

@@ -27,6 +27,7 @@ namespace frw {
 namespace {
 
 constexpr int kWalkThreads = 256;
+constexpr int kWalkMinBlocks = 4;  // 64 registers per thread: 4 blocks (32 warps) per SM
 constexpr int kWarpsPerBlock = kWalkThreads / 32;
 constexpr int kTabSlots = 32;  // per warp
 constexpr unsigned long long kEmptyKey = ~0ull;
@@ -149,7 +150,7 @@ __device__ void tab_flush(const WalkParams &P, Slot *tab, int lane) {
 }
 
 template <bool kMulti>
-__global__ void __launch_bounds__(kWalkThreads) k_walk(const WalkParams P) {
+__global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const WalkParams P) {
     __shared__ double s_intg[FRW_NSAMPLE + 1];
     __shared__ double s_wx[FRW_NSAMPLE], s_wy[FRW_NSAMPLE];
     __shared__ Slot s_tab[kWarpsPerBlock][kTabSlots];
@@ -206,14 +207,18 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(const WalkParams P) {
             if (!active) {
                 gw = mine;
                 if (gw < P.total_walks) {
-                    if (kMulti) {
-                        int lo = 0, hi = P.njobs;  // last job with walk_begin <= gw
-                        while (hi - lo > 1) {
-                            const int mid = (lo + hi) >> 1;
-                            if (P.jobs[mid].walk_begin <= gw) lo = mid;
-                            else hi = mid;
+                    if (kMulti) {  // the job whose walk range holds gw
+                        const bool same = gw >= P.jobs[job].walk_begin &&
+                                          (job + 1 == P.njobs || gw < P.jobs[job + 1].walk_begin);
+                        if (!same) {  // walk indices only grow: search above the current job
+                            int lo = gw >= P.jobs[job].walk_begin ? job : 0, hi = P.njobs;
+                            while (hi - lo > 1) {
+                                const int mid = (lo + hi) >> 1;
+                                if (P.jobs[mid].walk_begin <= gw) lo = mid;
+                                else hi = mid;
+                            }
+                            job = lo;
                         }
-                        job = lo;
                     }
                     const WalkJob &J = job_of<kMulti>(P, job);
                     const double4 g4 = P.gauss[job];

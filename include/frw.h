@@ -102,7 +102,7 @@ frw_status frw_layout_info_get(const frw_layout *layout, frw_layout_info *info);
  * inside the cell can find nearest, tied or containing the point.  Queries
  * scan their cell's list instead of descending the tree; cells whose list
  * would exceed max_per_cell fall back to the tree.  Results are identical
- * with and without them.  frw_layout_create builds them with 8 cells per rect
+ * with and without them.  frw_layout_create builds them with 16 cells per rect
  * and at most 32 rects per cell; frw_layout_set_cells rebuilds them
  * (cells_per_rect = 0 removes them).  It synchronises the device and must
  * not run while another call uses the layout, nor while a batch or a control

@@ -72,11 +72,11 @@ def test_cells_any_resolution_and_overflow(cells_per_rect, max_per_cell):
 
 
 def test_cells_c2_lists_are_short():
-    """10^4 rects: 8 cells per rect, a handful of rects per list, no overflow."""
+    """10^4 rects: 16 cells per rect, a handful of rects per list, no overflow."""
     rects = frw.generate_layout(0xF4A7 + 2, 10_000, 1e4)
     with frw.Layout.from_rects(rects) as L:
         ci = L.cells
-    assert ci.cells >= 8 * 10_000 * 0.9
+    assert ci.cells >= 16 * 10_000 * 0.9
     assert ci.entries / ci.cells < 8
     assert ci.overflow_cells == 0
 
