@@ -18,6 +18,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <initializer_list>
 
 #include "query.cuh"
 
@@ -192,10 +193,9 @@ __global__ void __launch_bounds__(kScanThreads) k_tile_scan(const int64_t *__res
 
 }  // namespace
 
-void free_cells(CellBuffers *c) {
-    cudaFree(c->cells);
-    cudaFree(c->crects);
-    cudaFree(c->cids);
+void free_cells(CellBuffers *c, cudaStream_t st) {
+    for (void *p : {(void *)c->cells, (void *)c->crects, (void *)c->cids})
+        if (p) cudaFreeAsync(p, st);
     *c = CellBuffers();
 }
 
@@ -258,8 +258,8 @@ frw_status build_cells(const DevLayout &Lin, double cells_per_rect, int cap, cud
         return rc == FRW_OK;
     };
     do {
-        if (!ck(cudaMalloc(&C.cells, (size_t)ncells * sizeof(int2)), "malloc cells")) break;
         if (!ck(cudaEventRecord(e0, st), "event")) break;
+        if (!ck(cudaMallocAsync(&C.cells, (size_t)ncells * sizeof(int2), st), "malloc cells")) break;
         if (!ck(cudaMallocAsync(&cnt, (size_t)ncells * 8, st), "malloc cell counts")) break;
         if (!ck(cudaMallocAsync(&start, (size_t)ncells * 8, st), "malloc cell starts")) break;
         if (!ck(cudaMallocAsync(&sums, (size_t)tiles * 8, st), "malloc tile sums")) break;
@@ -284,8 +284,8 @@ frw_status build_cells(const DevLayout &Lin, double cells_per_rect, int cap, cud
         }
         C.entries = total;
         C.overflow = (int64_t)novf;
-        if (!ck(cudaMalloc(&C.crects, (size_t)std::max<int64_t>(total, 1) * 16), "malloc cell rects")) break;
-        if (!ck(cudaMalloc(&C.cids, (size_t)std::max<int64_t>(total, 1) * 4), "malloc cell ids")) break;
+        if (!ck(cudaMallocAsync(&C.crects, (size_t)std::max<int64_t>(total, 1) * 16, st), "malloc cell rects")) break;
+        if (!ck(cudaMallocAsync(&C.cids, (size_t)std::max<int64_t>(total, 1) * 4, st), "malloc cell ids")) break;
         if (total > 0) k_cell_fill<<<blocks, 128, 0, st>>>(L, G, start, C.cells, C.crects, C.cids, ncells);
         if (!ck(cudaGetLastError(), "cell fill")) break;
         if (!ck(cudaEventRecord(e1, st), "event")) break;
@@ -297,7 +297,7 @@ frw_status build_cells(const DevLayout &Lin, double cells_per_rect, int cap, cud
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc != FRW_OK) {
-        free_cells(&C);
+        free_cells(&C, st);
         return rc;
     }
     C.bytes = ncells * (int64_t)sizeof(int2) + C.entries * 20;

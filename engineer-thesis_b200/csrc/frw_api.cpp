@@ -439,8 +439,8 @@ frw_status frw_layout_create(const float *rects, int64_t n, const double *bounds
     float4 *d_in = nullptr;
     auto fail = [&](frw_status r) {
         if (d_in) cudaFreeAsync(d_in, st);
-        free_tree(&L->T);
-        free_cells(&L->cells);
+        free_tree(&L->T, st);
+        free_cells(&L->cells, st);
         delete L;
         return r;
     };
@@ -521,9 +521,12 @@ frw_status frw_layout_from_file(const char *path, int layer, int device, frw_lay
 frw_status frw_layout_destroy(frw_layout *L) {
     if (!L) return FRW_OK;
     DeviceGuard g(L->device);
-    free_tree(&L->T);
-    free_cells(&L->cells);
+    // like cudaFree: nothing on the device may still read the layout
+    cudaError_t e = cudaDeviceSynchronize();
+    free_tree(&L->T, nullptr);
+    free_cells(&L->cells, nullptr);
     delete L;
+    FRW_CK(e);
     return FRW_OK;
 }
 
@@ -564,7 +567,7 @@ frw_status frw_layout_set_cells(frw_layout *L, double cells_per_rect, int max_pe
         if (rc) return rc;
     }
     FRW_CK(cudaDeviceSynchronize());  // no launch may still read the old lists
-    free_cells(&L->cells);
+    free_cells(&L->cells, nullptr);
     L->cells = c;
     L->dl.cells = nullptr;
     if (c.cells) attach_cells(L->dl, c);

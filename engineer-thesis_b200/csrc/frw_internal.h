@@ -128,7 +128,10 @@ struct TreeBuffers {
 };
 frw_status build_tree(const float4 *d_rects_in, int32_t n, const double bounds[4], int leaf_max,
                       cudaStream_t stream, TreeBuffers *out, float *build_ms);
-void free_tree(TreeBuffers *t);
+// Layout buffers come from the device's stream-ordered pool; the free calls
+// release them in the order of `stream` (callers make sure nothing still
+// reads them on another stream).
+void free_tree(TreeBuffers *t, cudaStream_t stream);
 
 // Cell lists over a built tree (DevLayout L with cells == nullptr): every
 // rect whose L-inf distance to a cell can be within 2 delta of the clearance
@@ -147,7 +150,7 @@ constexpr int kDefaultCellMax = 32;
 constexpr int64_t kMaxCells = 1ll << 26;
 frw_status build_cells(const DevLayout &L, double cells_per_rect, int max_per_cell, cudaStream_t stream,
                        CellBuffers *out);
-void free_cells(CellBuffers *c);
+void free_cells(CellBuffers *c, cudaStream_t stream);
 void attach_cells(DevLayout &L, const CellBuffers &c);
 
 // query.cu

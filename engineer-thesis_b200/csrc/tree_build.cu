@@ -265,11 +265,9 @@ __global__ void k_refit(const float4 *__restrict__ rects, const int4 *__restrict
 
 }  // namespace
 
-void free_tree(TreeBuffers *t) {
-    cudaFree(t->rects);
-    cudaFree(t->ids);
-    cudaFree(t->nbox);
-    cudaFree(t->nref);
+void free_tree(TreeBuffers *t, cudaStream_t st) {
+    for (void *p : {(void *)t->rects, (void *)t->ids, (void *)t->nbox, (void *)t->nref})
+        if (p) cudaFreeAsync(p, st);
     *t = TreeBuffers();
 }
 
@@ -301,11 +299,11 @@ frw_status build_tree(const float4 *d_rects_in, int32_t n, const double bounds[4
         return rc == FRW_OK;
     };
     do {
-        if (!ck(cudaMalloc(&T.rects, (size_t)n * 16), "malloc rects")) break;
-        if (!ck(cudaMalloc(&T.ids, (size_t)n * 4), "malloc ids")) break;
-        if (!ck(cudaMalloc(&T.nbox, (size_t)cap_nodes * 64), "malloc nbox")) break;
-        if (!ck(cudaMalloc(&T.nref, (size_t)cap_nodes * 16), "malloc nref")) break;
-        if (!ck(cudaEventRecord(e0, st), "event")) break;  // build time excludes the persistent allocations
+        if (!ck(cudaEventRecord(e0, st), "event")) break;
+        if (!ck(cudaMallocAsync(&T.rects, (size_t)n * 16, st), "malloc rects")) break;
+        if (!ck(cudaMallocAsync(&T.ids, (size_t)n * 4, st), "malloc ids")) break;
+        if (!ck(cudaMallocAsync(&T.nbox, (size_t)cap_nodes * 64, st), "malloc nbox")) break;
+        if (!ck(cudaMallocAsync(&T.nref, (size_t)cap_nodes * 16, st), "malloc nref")) break;
         // temporaries from the stream-ordered pool (no device-wide sync)
         if (!ck(cudaMallocAsync(&k0, (size_t)n * 4, st), "malloc keys")) break;
         if (!ck(cudaMallocAsync(&k1, (size_t)n * 4, st), "malloc keys")) break;
@@ -392,7 +390,7 @@ frw_status build_tree(const float4 *d_rects_in, int32_t n, const double bounds[4
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc != FRW_OK) {
-        free_tree(&T);
+        free_tree(&T, st);
         return rc;
     }
     *out = T;
