@@ -8,6 +8,7 @@
 #include <stdio.h>
 
 #include <cmath>
+#include <cstddef>
 #include <string.h>
 #include <time.h>
 
@@ -42,6 +43,7 @@ struct DeviceCtx {
     int sms = 0;
     int cc_major = 0, cc_minor = 0;
     double *tables = nullptr;  // intg[201] | wx[200] | wy[200]
+    int walk_bps = 0;          // resident walk blocks per SM (occupancy query, cached)
 };
 std::mutex g_mu;
 std::map<int, DeviceCtx> g_ctx;
@@ -97,11 +99,8 @@ frw_status device_ctx(int dev, DeviceCtx **out) {
     return FRW_OK;
 }
 
-// Reads the kernel status word (after the stream has drained).
-frw_status check_status(const uint32_t *d_status, cudaStream_t st) {
-    uint32_t h = 0;
-    FRW_CK(cudaMemcpyAsync(&h, d_status, 4, cudaMemcpyDeviceToHost, st));
-    FRW_CK(cudaStreamSynchronize(st));
+// The message of a nonzero kernel status word.
+frw_status status_error(uint32_t h) {
     if (h) {
         std::string m = "kernel reported:";
         if (h & kStCandOverflow) m += " near-tie candidate list overflow;";
@@ -112,6 +111,14 @@ frw_status check_status(const uint32_t *d_status, cudaStream_t st) {
         return FRW_E_KERNEL;
     }
     return FRW_OK;
+}
+
+// Reads the kernel status word (after the stream has drained).
+frw_status check_status(const uint32_t *d_status, cudaStream_t st) {
+    uint32_t h = 0;
+    FRW_CK(cudaMemcpyAsync(&h, d_status, 4, cudaMemcpyDeviceToHost, st));
+    FRW_CK(cudaStreamSynchronize(st));
+    return status_error(h);
 }
 
 bool fp32_exact(double v) { return (double)(float)v == v && fabs(v) < 16777216.0; }
@@ -174,31 +181,32 @@ frw_status run_walks(const frw_layout *lay, int64_t target, uint64_t first_walk,
         set_error("target conductor index out of range");
         return FRW_E_ARG;
     }
-    Scratch S(st);
-    double4 *d_tgt, *d_gauss;
-    uint32_t *d_status;
-    unsigned long long *d_counter, *d_stats, *d_acc_n;
-    double *d_acc_s, *d_acc_s2;
+    // one scratch block: a header cleared with the per-conductor rows in one
+    // memset, read back in one copy; compacted rows after it
+    struct Hdr {
+        double4 gauss;
+        unsigned long long stats[4], counter, cnt;
+        uint32_t status, pad;
+        double4 tgt;
+    };
+    static_assert(sizeof(Hdr) % 16 == 0, "header keeps 16-byte alignment");
     const int64_t rows = lay->n;  // the kernel flushes every conductor it reaches
-    FRW_CK(S.get(&d_tgt, sizeof(double4)));
-    FRW_CK(S.get(&d_gauss, sizeof(double4)));
-    FRW_CK(S.get(&d_status, 4));
-    FRW_CK(S.get(&d_counter, 8));
-    FRW_CK(S.get(&d_stats, 4 * 8));
-    FRW_CK(S.get(&d_acc_n, (size_t)std::max<int64_t>(rows, 1) * 8));
-    FRW_CK(S.get(&d_acc_s, (size_t)std::max<int64_t>(rows, 1) * 8));
-    FRW_CK(S.get(&d_acc_s2, (size_t)std::max<int64_t>(rows, 1) * 8));
+    const size_t R = (size_t)std::max<int64_t>(rows, 1);
+    Scratch S(st);
+    char *blk;
+    FRW_CK(S.get(&blk, sizeof(Hdr) + R * 8 * (out ? 7 : 3)));
+    Hdr *h = reinterpret_cast<Hdr *>(blk);
+    unsigned long long *d_acc_n = reinterpret_cast<unsigned long long *>(blk + sizeof(Hdr));
+    double *d_acc_s = reinterpret_cast<double *>(d_acc_n + R);
+    double *d_acc_s2 = d_acc_s + R;
+    double4 *d_tgt = &h->tgt, *d_gauss = &h->gauss;
+    uint32_t *d_status = &h->status;
+    unsigned long long *d_counter = &h->counter, *d_stats = h->stats;
     const double *r = lay->rects.data() + 4 * target;
     const double tg[4] = {r[0], r[1], r[2], r[3]};
+    FRW_CK(cudaMemsetAsync(blk, 0, offsetof(Hdr, tgt), st));
+    if (rows) FRW_CK(cudaMemsetAsync(d_acc_n, 0, R * 24, st));
     FRW_CK(cudaMemcpyAsync(d_tgt, tg, sizeof(tg), cudaMemcpyHostToDevice, st));
-    FRW_CK(cudaMemsetAsync(d_status, 0, 4, st));
-    FRW_CK(cudaMemsetAsync(d_counter, 0, 8, st));
-    FRW_CK(cudaMemsetAsync(d_stats, 0, 32, st));
-    if (rows) {
-        FRW_CK(cudaMemsetAsync(d_acc_n, 0, rows * 8, st));
-        FRW_CK(cudaMemsetAsync(d_acc_s, 0, rows * 8, st));
-        FRW_CK(cudaMemsetAsync(d_acc_s2, 0, rows * 8, st));
-    }
     rc = launch_gauss(lay->dl, (const double *)d_tgt, 1, o.gauss_mode, o.gauss_param, (double *)d_gauss,
                       d_status, st);
     if (rc) return rc;
@@ -237,7 +245,8 @@ frw_status run_walks(const frw_layout *lay, int64_t target, uint64_t first_walk,
     P.wx = ctx->tables + FRW_NSAMPLE + 1;
     P.wy = ctx->tables + 2 * FRW_NSAMPLE + 1;
     const int threads = 256;
-    int bps = o.blocks_per_sm > 0 ? o.blocks_per_sm : walk_max_blocks_per_sm(threads, false);
+    if (!ctx->walk_bps) ctx->walk_bps = walk_max_blocks_per_sm(threads, false);
+    int bps = o.blocks_per_sm > 0 ? o.blocks_per_sm : ctx->walk_bps;
     if (bps < 1) bps = 1;
     int blocks = ctx->sms * bps;
     const uint64_t need = (walks + threads - 1) / threads;
@@ -249,6 +258,13 @@ frw_status run_walks(const frw_layout *lay, int64_t target, uint64_t first_walk,
         FRW_CK(cudaEventCreate(&e1));
         FRW_CK(cudaEventRecord(e0, st));
     }
+    struct EvGuard {
+        cudaEvent_t a, b;
+        ~EvGuard() {
+            if (a) cudaEventDestroy(a);
+            if (b) cudaEventDestroy(b);
+        }
+    } evg{e0, e1};
     if (walks > 0) {
         rc = launch_walk(P, threads, blocks, st);
         if (rc) return rc;
@@ -259,24 +275,20 @@ frw_status run_walks(const frw_layout *lay, int64_t target, uint64_t first_walk,
         return check_status(d_status, st);
     }
     FRW_CK(cudaEventRecord(e1, st));
-    // compact nonzero rows
-    int64_t *d_row;
-    unsigned long long *d_cn, *d_cnt;
-    double *d_cs, *d_cs2;
-    FRW_CK(S.get(&d_row, (size_t)std::max<int64_t>(rows, 1) * 8));
-    FRW_CK(S.get(&d_cn, (size_t)std::max<int64_t>(rows, 1) * 8));
-    FRW_CK(S.get(&d_cs, (size_t)std::max<int64_t>(rows, 1) * 8));
-    FRW_CK(S.get(&d_cs2, (size_t)std::max<int64_t>(rows, 1) * 8));
-    FRW_CK(S.get(&d_cnt, 8));
-    FRW_CK(cudaMemsetAsync(d_cnt, 0, 8, st));
-    rc = launch_compact(d_acc_n, d_acc_s, d_acc_s2, rows, d_row, d_cn, d_cs, d_cs2, d_cnt, st);
+    // compact nonzero rows (after the accumulators in the same block)
+    int64_t *d_row = reinterpret_cast<int64_t *>(d_acc_s2 + R);
+    unsigned long long *d_cn = reinterpret_cast<unsigned long long *>(d_row + R);
+    double *d_cs = reinterpret_cast<double *>(d_cn + R);
+    double *d_cs2 = d_cs + R;
+    rc = launch_compact(d_acc_n, d_acc_s, d_acc_s2, rows, d_row, d_cn, d_cs, d_cs2, &h->cnt, st);
     if (rc) return rc;
-    unsigned long long h_cnt = 0, h_stats[4];
-    FRW_CK(cudaMemcpyAsync(&h_cnt, d_cnt, 8, cudaMemcpyDeviceToHost, st));
-    FRW_CK(cudaMemcpyAsync(h_stats, d_stats, 32, cudaMemcpyDeviceToHost, st));
-    FRW_CK(cudaMemcpyAsync(out->gauss, d_gauss, 32, cudaMemcpyDeviceToHost, st));
-    rc = check_status(d_status, st);
+    Hdr hh;
+    FRW_CK(cudaMemcpyAsync(&hh, h, offsetof(Hdr, tgt), cudaMemcpyDeviceToHost, st));
+    FRW_CK(cudaStreamSynchronize(st));
+    rc = status_error(hh.status);
     if (rc) return rc;
+    const unsigned long long h_cnt = hh.cnt;
+    memcpy(out->gauss, &hh.gauss, sizeof(out->gauss));
     out->row.resize(h_cnt);
     out->n.resize(h_cnt);
     out->s.resize(h_cnt);
@@ -288,13 +300,11 @@ frw_status run_walks(const frw_layout *lay, int64_t target, uint64_t first_walk,
         FRW_CK(cudaMemcpyAsync(out->s2.data(), d_cs2, h_cnt * 8, cudaMemcpyDeviceToHost, st));
         FRW_CK(cudaStreamSynchronize(st));
     }
-    out->escaped = h_stats[0];
-    out->aborted = h_stats[1];
-    out->hops = h_stats[2];
-    out->done = h_stats[3];
+    out->escaped = hh.stats[0];
+    out->aborted = hh.stats[1];
+    out->hops = hh.stats[2];
+    out->done = hh.stats[3];
     cudaEventElapsedTime(&out->kernel_ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     if (out->done != walks) {
         set_error("walk kernel finished " + std::to_string(out->done) + " of " + std::to_string(walks) +
                   " walks");
