@@ -67,7 +67,8 @@ struct Grid {
     int nx, ny;
 };
 
-__device__ __forceinline__ void cell_box(const DevLayout &L, const Grid &G, int64_t c, double B[4]) {
+// The cell grown by its radius r_C (returned).
+__device__ __forceinline__ double cell_box(const DevLayout &L, const Grid &G, int64_t c, double B[4]) {
     const int ix = (int)(c % G.nx), iy = (int)(c / G.nx);
     const double x0 = G.gx0 + ix * G.side, y0 = G.gy0 + iy * G.side;
     const double x1 = x0 + G.side, y1 = y0 + G.side;
@@ -80,16 +81,20 @@ __device__ __forceinline__ void cell_box(const DevLayout &L, const Grid &G, int6
     B[1] = y0 - r;
     B[2] = x1 + r;
     B[3] = y1 + r;
+    return r;
 }
 
 // Per cell: its list length, or -1 (in cells[c].y) when it exceeds cap or
 // the enumeration was incomplete; cnt[c] = entries to reserve.
 __global__ void k_cell_count(DevLayout L, Grid G, int cap, int64_t *__restrict__ cnt, int2 *__restrict__ cells,
-                             unsigned long long *overflow, int64_t ncells) {
+                             float *__restrict__ crad, unsigned long long *overflow, int64_t ncells) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncells) return;
     double B[4];
-    cell_box(L, G, c, B);
+    const double r = cell_box(L, G, c, B);
+    // a point of the cell lies within margin/2 of it whatever the rounding of
+    // its cell index, so every rect within r - margin of the point is listed
+    crad[c] = __double2float_rd(r - G.margin);
     int n = 0;
     const bool complete = touching(L, B, [&](int, float4) { return ++n <= cap; });
     const bool ok = complete && n <= cap;
@@ -194,7 +199,7 @@ __global__ void __launch_bounds__(kScanThreads) k_tile_scan(const int64_t *__res
 }  // namespace
 
 void free_cells(CellBuffers *c, cudaStream_t st) {
-    for (void *p : {(void *)c->cells, (void *)c->crects, (void *)c->cids})
+    for (void *p : {(void *)c->cells, (void *)c->crects, (void *)c->cids, (void *)c->crad})
         if (p) cudaFreeAsync(p, st);
     *c = CellBuffers();
 }
@@ -203,6 +208,7 @@ void attach_cells(DevLayout &L, const CellBuffers &c) {
     L.cells = c.cells;
     L.crects = c.crects;
     L.cids = c.cids;
+    L.crad = c.crad;
     L.gx0 = c.gx0;
     L.gy0 = c.gy0;
     L.ginv = c.ginv;
@@ -260,6 +266,7 @@ frw_status build_cells(const DevLayout &Lin, double cells_per_rect, int cap, cud
     do {
         if (!ck(cudaEventRecord(e0, st), "event")) break;
         if (!ck(cudaMallocAsync(&C.cells, (size_t)ncells * sizeof(int2), st), "malloc cells")) break;
+        if (!ck(cudaMallocAsync(&C.crad, (size_t)ncells * sizeof(float), st), "malloc cell radii")) break;
         if (!ck(cudaMallocAsync(&cnt, (size_t)ncells * 8, st), "malloc cell counts")) break;
         if (!ck(cudaMallocAsync(&start, (size_t)ncells * 8, st), "malloc cell starts")) break;
         if (!ck(cudaMallocAsync(&sums, (size_t)tiles * 8, st), "malloc tile sums")) break;
@@ -267,7 +274,7 @@ frw_status build_cells(const DevLayout &Lin, double cells_per_rect, int cap, cud
         if (!ck(cudaMallocAsync(&ovf, 8, st), "malloc overflow count")) break;
         if (!ck(cudaMemsetAsync(ovf, 0, 8, st), "memset")) break;
         const unsigned blocks = (unsigned)((ncells + 127) / 128);
-        k_cell_count<<<blocks, 128, 0, st>>>(L, G, cap, cnt, C.cells, ovf, ncells);
+        k_cell_count<<<blocks, 128, 0, st>>>(L, G, cap, cnt, C.cells, C.crad, ovf, ncells);
         k_tile_sums<<<(unsigned)tiles, kScanThreads, 0, st>>>(cnt, ncells, sums);
         k_scan_sums<<<1, kScanThreads, 0, st>>>(sums, tiles, grand);
         k_tile_scan<<<(unsigned)tiles, kScanThreads, 0, st>>>(cnt, ncells, sums, start);
@@ -300,7 +307,7 @@ frw_status build_cells(const DevLayout &Lin, double cells_per_rect, int cap, cud
         free_cells(&C, st);
         return rc;
     }
-    C.bytes = ncells * (int64_t)sizeof(int2) + C.entries * 20;
+    C.bytes = ncells * (int64_t)(sizeof(int2) + sizeof(float)) + C.entries * 20;
     *out = C;
     return FRW_OK;
 }

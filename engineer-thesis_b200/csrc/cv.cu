@@ -8,14 +8,18 @@
 // EXACTLY: with the grid start (Q equal arcs, Q a power of two) the pair
 // (start point, first-hop bin) takes finitely many values with known
 // probabilities (1/Q times the exact bin probability of the 32-bit uniform),
-// so E[f] is a finite sum over Q x 200 first-hop points evaluated with the
-// same feature and MLP kernels as the walks.
+// so E[f] is a finite sum over Q x 200 first-hop points.  The same pass keeps
+// phi of every one of those points in a table: a walk's first-hop point is a
+// function of its (arc, bin), so the walks look their phi up instead of
+// recomputing features and the MLP, and f is exactly the function whose mean
+// was summed.
 //
-// Kernels: feature extraction (one nearest-other-conductor traversal per
-// point), BF16 tensor-core MLP forward (mma.sync m16n8k16, FP32 accumulate,
-// the first layer's accumulators re-packed in registers as the second
-// layer's A operand), fused forward+backward with weight gradients as
-// tensor-core products over 64-row chunks, Adam, and FP64 reductions.
+// Kernels: feature extraction (the nearest other conductor from the cell
+// list, or one tree traversal), BF16 tensor-core MLP forward (mma.sync
+// m16n8k16, FP32 accumulate, the first layer's accumulators re-packed in
+// registers as the second layer's A operand), the fused exact-mean pass,
+// fused forward+backward with weight gradients as tensor-core products over
+// 64-row chunks, Adam, and FP64 reductions.
 #include <cuda_bf16.h>
 
 #include "cv.cuh"
@@ -28,8 +32,9 @@ namespace {
 constexpr unsigned kFull = 0xFFFFFFFFu;
 
 // ---------------------------------------------------------------- features
-__device__ __forceinline__ float feat(double d, double a0) {
-    double v = __ddiv_rn(d, a0);
+// d / a0 as d * (1 / a0) (one division per point), clamped to [-16, 16]
+__device__ __forceinline__ float feat(double d, double inv) {
+    double v = __dmul_rn(d, inv);
     v = fmin(fmax(v, -16.0), 16.0);
     return (float)v;
 }
@@ -40,19 +45,20 @@ __device__ __forceinline__ void edge_feats(double px, double py, double x0, doub
                                            double a0, float *f) {
     const double cx = fmin(fmax(px, x0), x1), cy = fmin(fmax(py, y0), y1);
     const double dcx = __dsub_rn(cx, px), dcy = __dsub_rn(cy, py);
-    f[0] = feat(dcx, a0);
-    f[1] = feat(__dsub_rn(y0, py), a0);
-    f[2] = feat(__dsub_rn(x1, px), a0);
-    f[3] = feat(dcy, a0);
-    f[4] = feat(dcx, a0);
-    f[5] = feat(__dsub_rn(y1, py), a0);
-    f[6] = feat(__dsub_rn(x0, px), a0);
-    f[7] = feat(dcy, a0);
+    const double inv = __ddiv_rn(1.0, a0);
+    f[0] = feat(dcx, inv);
+    f[1] = feat(__dsub_rn(y0, py), inv);
+    f[2] = feat(__dsub_rn(x1, px), inv);
+    f[3] = feat(dcy, inv);
+    f[4] = f[0];
+    f[5] = feat(__dsub_rn(y1, py), inv);
+    f[6] = feat(__dsub_rn(x0, px), inv);
+    f[7] = f[3];
 }
 
 // Nearest rect other than layer index `exclude` (smallest L-inf gap, then
-// smallest layer index); Morton position or -1.
-__device__ int nearest_other(const DevLayout &L, double px, double py, int exclude) {
+// smallest layer index) from the tree; Morton position or -1.
+__device__ int nearest_other_tree(const DevLayout &L, double px, double py, int exclude) {
     const float pxf = (float)px, pyf = (float)py, slack = L.slack;
     double best = 1e300;
     int best_id = 0x7FFFFFFF, best_k = -1;
@@ -108,6 +114,45 @@ __device__ int nearest_other(const DevLayout &L, double px, double py, int exclu
     return best_k;
 }
 
+// The same from p's cell list when it settles the answer: every rect within
+// crad of p is listed, so a listed nearest other within crad is the nearest
+// (ties included); otherwise the tree.  Writes the rect, false when none.
+__device__ __forceinline__ bool nearest_other(const DevLayout &L, double px, double py, int exclude, float4 &o) {
+    if (L.cells && px >= L.bx0 && py >= L.by0 && px <= L.bx1 && py <= L.by1) {
+        int ix = (int)__dmul_rn(__dsub_rn(px, L.gx0), L.ginv);
+        int iy = (int)__dmul_rn(__dsub_rn(py, L.gy0), L.ginv);
+        ix = ix < 0 ? 0 : (ix >= L.gnx ? L.gnx - 1 : ix);
+        iy = iy < 0 ? 0 : (iy >= L.gny ? L.gny - 1 : iy);
+        const int64_t cell = (int64_t)iy * L.gnx + ix;
+        const int2 ce = __ldg(L.cells + cell);
+        if (ce.y >= 0) {
+            double best = 1e300;
+            int best_id = 0x7FFFFFFF;
+            float4 bo = make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int k = ce.x; k < ce.x + ce.y; k++) {
+                const int id = __ldg(L.cids + k);
+                if (id == exclude) continue;
+                const float4 r = __ldg(L.crects + k);
+                const double g =
+                    fmax(fmax((double)r.x - px, px - (double)r.z), fmax((double)r.y - py, py - (double)r.w));
+                if (g < best || (g == best && id < best_id)) {
+                    best = g;
+                    best_id = id;
+                    bo = r;
+                }
+            }
+            if (best <= (double)__ldg(L.crad + cell)) {
+                o = bo;
+                return true;
+            }
+        }
+    }
+    const int k = nearest_other_tree(L, px, py, exclude);
+    if (k < 0) return false;
+    o = __ldg(L.rects + k);
+    return true;
+}
+
 __global__ void k_features(DevLayout L, double4 trect, int tid, const double4 *__restrict__ rec, int64_t n,
                            __nv_bfloat16 *__restrict__ xb, float *__restrict__ xf) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -116,9 +161,8 @@ __global__ void k_features(DevLayout L, double4 trect, int tid, const double4 *_
     float f[16];
     if (r.z > 0.0) {
         edge_feats(r.x, r.y, trect.x, trect.y, trect.z, trect.w, r.z, f);
-        const int k = nearest_other(L, r.x, r.y, tid);
-        if (k >= 0) {
-            const float4 o = __ldg(L.rects + k);
+        float4 o;
+        if (nearest_other(L, r.x, r.y, tid, o)) {
             edge_feats(r.x, r.y, o.x, o.y, o.z, o.w, r.z, f + 8);
         } else {
 #pragma unroll
@@ -160,9 +204,19 @@ __device__ __forceinline__ void mma16816(float d[4], const uint32_t a[4], uint32
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-__device__ __forceinline__ float silu(float z) { return z / (1.f + __expf(-z)); }
+// sigmoid(z) = (1 + tanh(z/2)) / 2 with the hardware tanh (one MUFU op,
+// relative error about 2^-11, below the BF16 rounding of the activations);
+// training and evaluation use the same function, so the control variate
+// stays exactly the function whose mean is summed.
+__device__ __forceinline__ float tanh_hw(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float sigm(float z) { return 0.5f + 0.5f * tanh_hw(0.5f * z); }
+__device__ __forceinline__ float silu(float z) { return z * sigm(z); }
 __device__ __forceinline__ float dsilu(float z) {
-    const float s = 1.f / (1.f + __expf(-z));
+    const float s = sigm(z);
     return s * (1.f + z * (1.f - s));
 }
 
@@ -556,26 +610,6 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-__global__ void k_cv_reduce(const int64_t *__restrict__ end, const double4 *__restrict__ rec,
-                            const float *__restrict__ phi, int64_t n, int target, double *sums) {
-    double s[4] = {0, 0, 0, 0};
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const double c = rec[i].w;
-        const double yv = end[i] == target ? 1.0 : 0.0;
-        const double z = c * (yv - (double)phi[i]);
-        const double w = c * yv;
-        s[0] += z;
-        s[1] += z * z;
-        s[2] += w;
-        s[3] += w * w;
-    }
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-        const double t = warp_sum(s[k]);
-        if ((threadIdx.x & 31) == 0) atomicAdd(&sums[k], t);
-    }
-}
-
 // Training pairs from walk records: y = 1{end == target}, weight c^2.
 __global__ void k_targets(const int64_t *__restrict__ end, const double4 *__restrict__ rec, int64_t n, int target,
                           float *__restrict__ y, float *__restrict__ wt, double *wsum) {
@@ -625,7 +659,8 @@ __global__ void __launch_bounds__(128) k_quad_mean(DevLayout L, double4 trect, i
                                                    const double *__restrict__ wx, const double *__restrict__ wy,
                                                    double eps, bool exact, const float *__restrict__ p,
                                                    const __nv_bfloat16 *__restrict__ w1,
-                                                   const __nv_bfloat16 *__restrict__ w2, double *sum) {
+                                                   const __nv_bfloat16 *__restrict__ w2, double *sum,
+                                                   float *__restrict__ phi_out) {
     __shared__ Smem S;
     __shared__ uint32_t xs[4][32][kIn / 2];
     load_net(S, p, w1, w2);
@@ -655,9 +690,8 @@ __global__ void __launch_bounds__(128) k_quad_mean(DevLayout L, double4 trect, i
             const double c = __ddiv_rn(__dmul_rn(__dmul_rn(-eps, perim), dot), a0);
             wgt = c * pi_exact[i] / (double)Q;
             edge_feats(x1, y1, trect.x, trect.y, trect.z, trect.w, a0, f);
-            const int k = nearest_other(L, x1, y1, tid);
-            if (k >= 0) {
-                const float4 o = __ldg(L.rects + k);
+            float4 o;
+            if (nearest_other(L, x1, y1, tid, o)) {
                 edge_feats(x1, y1, o.x, o.y, o.z, o.w, a0, f + 8);
             } else {
 #pragma unroll
@@ -667,6 +701,8 @@ __global__ void __launch_bounds__(128) k_quad_mean(DevLayout L, double4 trect, i
 #pragma unroll
         for (int k = 0; k < kIn / 2; k++) xs[warp][lane][k] = pack2(f[2 * k], f[2 * k + 1]);
         __syncwarp();
+        float mine = 0.f;
+        const int row = lane & 15, src = 4 * (row & 7);
 #pragma unroll
         for (int h = 0; h < 2; h++) {
             const int ra = 16 * h + g, rb = ra + 8;
@@ -676,11 +712,40 @@ __global__ void __launch_bounds__(128) k_quad_mean(DevLayout L, double4 trect, i
             tile_forward(S, xa, g, tg, z1, z2, a2, og, og8);
             const double wa = __shfl_sync(kFull, wgt, ra), wb = __shfl_sync(kFull, wgt, rb);
             if (tg == 0) acc += wa * (double)og + wb * (double)og8;
+            const float lo = __shfl_sync(kFull, og, src), hi = __shfl_sync(kFull, og8, src);
+            if ((lane >> 4) == h) mine = row < 8 ? lo : hi;
         }
+        if (phi_out && t < n) phi_out[t] = mine;  // the table the walks look phi up in
         __syncwarp();
     }
     acc = warp_sum(acc);
     if (lane == 0) atomicAdd(sum, acc);
+}
+
+// Per walk record of the grid start: f = c * phi[q * 200 + i1] from the
+// quadrature's table (the same function value the exact mean sums), and the
+// sums of z = c (1{end==t} - phi), z^2, w = c 1{end==t}, w^2.
+__global__ void k_cv_gather(const int64_t *__restrict__ end, const double *__restrict__ cw,
+                            const int32_t *__restrict__ qi, const float *__restrict__ phi, int64_t n, int target,
+                            double *sums) {
+    double s[4] = {0, 0, 0, 0};
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double c = cw[i];
+        const int32_t k = qi[i];
+        const double yv = end[i] == target ? 1.0 : 0.0;
+        const double f = k >= 0 ? (double)__ldg(phi + k) : 0.0;
+        const double z = c * (yv - f);
+        const double w = c * yv;
+        s[0] += z;
+        s[1] += z * z;
+        s[2] += w;
+        s[3] += w * w;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const double t = warp_sum(s[k]);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&sums[k], t);
+    }
 }
 
 }  // namespace
@@ -746,11 +811,11 @@ frw_status launch_adam(const Net &n, float *grad, float *m, float *v, int *step,
     return FRW_OK;
 }
 
-frw_status launch_cv_reduce(const int64_t *end, const double4 *rec, const float *phi, int64_t n, int target,
-                            double *sums, cudaStream_t st) {
+frw_status launch_cv_gather(const int64_t *end, const double *cw, const int32_t *qi, const float *phi, int64_t n,
+                            int target, double *sums, cudaStream_t st) {
     if (n <= 0) return FRW_OK;
     const int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
-    k_cv_reduce<<<blocks, 256, 0, st>>>(end, rec, phi, n, target, sums);
+    k_cv_gather<<<blocks, 256, 0, st>>>(end, cw, qi, phi, n, target, sums);
     FRW_CK(cudaGetLastError());
     return FRW_OK;
 }
@@ -767,7 +832,7 @@ frw_status launch_targets(const int64_t *end, const double4 *rec, int64_t n, int
 
 frw_status launch_quad_mean(const DevLayout &L, double4 trect, int tid, const double4 *gauss, uint32_t Q,
                             const double *pi_exact, const double *wx, const double *wy, double eps, bool exact,
-                            const Net &net, double *sum, cudaStream_t st) {
+                            const Net &net, double *sum, float *phi_out, cudaStream_t st) {
     double4 *sqs;
     int *sides;
     FRW_CK(cudaMallocAsync((void **)&sqs, (size_t)Q * sizeof(double4), st));
@@ -776,7 +841,7 @@ frw_status launch_quad_mean(const DevLayout &L, double4 trect, int tid, const do
     const int64_t n = (int64_t)Q * FRW_NSAMPLE;
     const int blocks = (int)std::min<int64_t>((n + 127) / 128, 148 * 8);
     k_quad_mean<<<blocks, 128, 0, st>>>(L, trect, tid, gauss, sqs, sides, Q, pi_exact, wx, wy, eps, exact, net.p,
-                                        net.w1, net.w2, sum);
+                                        net.w1, net.w2, sum, phi_out);
     cudaError_t e = cudaGetLastError();
     cudaFreeAsync(sqs, st);
     cudaFreeAsync(sides, st);

@@ -42,13 +42,16 @@ frw_status launch_forward(const Net &n, const __nv_bfloat16 *x, int64_t rows, fl
 frw_status launch_train_grad(const Net &n, const __nv_bfloat16 *x, const float *y, const float *wt, int64_t rows,
                              float inv_wsum, float *grad, double *loss, cudaStream_t st);
 frw_status launch_adam(const Net &n, float *grad, float *m, float *v, int *step, float lr, cudaStream_t st);
-// per walk: z = c (1{end==target} - phi); w = c 1{end==target}; sums of z, z^2, w, w^2
-frw_status launch_cv_reduce(const int64_t *end, const double4 *rec, const float *phi, int64_t n, int target,
-                            double *sums /*4*/, cudaStream_t st);
 // exact mean E[f] over every (grid start, first-hop bin) pair, accumulated into *sum
 frw_status launch_quad_mean(const DevLayout &L, double4 target_rect, int target_id, const double4 *gauss, uint32_t Q,
                             const double *pi_exact, const double *wx, const double *wy, double eps,
-                            bool exact_perimeter, const Net &net, double *sum, cudaStream_t st);
+                            bool exact_perimeter, const Net &net, double *sum,
+                            float *phi_out /*nullable: Q*200 phi values, item q*200+i*/, cudaStream_t st);
+// per walk record (end, weight factor c, q*200+i1 or -1): the sums of
+// z = c (1{end==target} - phi), z^2, w = c 1{end==target}, w^2 with phi looked
+// up in the quadrature's table
+frw_status launch_cv_gather(const int64_t *end, const double *cw, const int32_t *qi, const float *phi, int64_t n,
+                            int target, double *sums /*4*/, cudaStream_t st);
 frw_status launch_targets(const int64_t *end, const double4 *rec, int64_t n, int target, float *y, float *wt,
                           double *wsum, cudaStream_t st);
 

@@ -26,6 +26,7 @@ struct frw_cv {
     double mean_term = 0.0, train_loss = 0.0, train_ms = 0.0, quad_ms = 0.0;
     uint64_t train_walks = 0;
     uint32_t quad_points = 0;
+    float *phi = nullptr;  // phi at every (grid arc, first-hop bin): Q x 200
 };
 
 namespace frw {
@@ -89,8 +90,8 @@ void init_params(uint64_t seed, float *p) {
 frw_status check_cv_walk_opts(const frw_opts &o) {
     frw_status rc = check_opts(&o);
     if (rc) return rc;
-    if (o.start_mode != FRW_START_UNIFORM || !pow2(o.start_grid) || o.hop_cap < 2) {
-        set_error("control variate: needs FRW_START_UNIFORM, start_grid a power of two and hop_cap >= 2");
+    if (o.start_mode != FRW_START_UNIFORM || !pow2(o.start_grid) || o.start_grid > (1u << 23) || o.hop_cap < 2) {
+        set_error("control variate: needs FRW_START_UNIFORM, start_grid a power of two <= 2^23 and hop_cap >= 2");
         return FRW_E_ARG;
     }
     return FRW_OK;
@@ -151,6 +152,7 @@ frw_status frw_cv_train(const frw_layout *layout, int64_t target, const frw_opts
     M->train_walks = co.train_walks;
     auto fail = [&](frw_status r) {
         cv::net_free(&M->net);
+        if (M->phi) cudaFreeAsync(M->phi, st);
         delete M;
         return r;
     };
@@ -276,10 +278,14 @@ frw_status frw_cv_train(const frw_layout *layout, int64_t target, const frw_opts
         rc = launch_gauss(v.dl, (const double *)d_tgt, 1, walk_opts->gauss_mode, walk_opts->gauss_param,
                           (double *)d_gauss, d_status, st);
         const double4 trect = make_double4(r[0], r[1], r[2], r[3]);
+        if (!rc) {
+            e = cudaMallocAsync(&M->phi, (size_t)nq * sizeof(float), st);
+            if (e != cudaSuccess) return fail(cuda_fail(e, "frw_cv_train: phi table"));
+        }
         if (!rc)
             rc = cv::launch_quad_mean(v.dl, trect, (int)target, d_gauss, Q, d_pi, tables + FRW_NSAMPLE + 1,
                                       tables + 2 * FRW_NSAMPLE + 1, walk_opts->permittivity,
-                                      walk_opts->exact_perimeter != 0, M->net, d_mu, st);
+                                      walk_opts->exact_perimeter != 0, M->net, d_mu, M->phi, st);
         if (rc) return fail(rc);
         uint32_t hs = 0;
         e = cudaMemcpyAsync(&M->mean_term, d_mu, 8, cudaMemcpyDeviceToHost, st);
@@ -329,15 +335,13 @@ frw_status frw_cv_walk(const frw_cv *M, uint64_t walks, uint64_t seed, frw_cv_re
     const uint64_t chunk = std::min<uint64_t>(walks, 1ull << 23);
     Buf B(st);
     int64_t *d_end;
-    double4 *d_rec;
-    __nv_bfloat16 *d_x;
-    float *d_phi;
+    double *d_w;
+    int32_t *d_q;
     double *d_sums;
     cudaError_t e = cudaSuccess;
     if (e == cudaSuccess) e = B.get(&d_end, chunk * 8);
-    if (e == cudaSuccess) e = B.get(&d_rec, chunk * 32);
-    if (e == cudaSuccess) e = B.get(&d_x, chunk * 32);
-    if (e == cudaSuccess) e = B.get(&d_phi, chunk * 4);
+    if (e == cudaSuccess) e = B.get(&d_w, chunk * 8);
+    if (e == cudaSuccess) e = B.get(&d_q, chunk * 4);
     if (e == cudaSuccess) e = B.get(&d_sums, 32);
     if (e != cudaSuccess) return cuda_fail(e, "frw_cv_walk: allocation");
     cudaMemsetAsync(d_sums, 0, 32, st);
@@ -345,15 +349,11 @@ frw_status frw_cv_walk(const frw_cv *M, uint64_t walks, uint64_t seed, frw_cv_re
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, st);
-    const double *r = M->view.rects + 4 * M->target;
-    const double4 trect = make_double4(r[0], r[1], r[2], r[3]);
     frw_status rc = FRW_OK;
     for (uint64_t first = 0; first < walks && !rc; first += chunk) {
         const uint64_t n = std::min<uint64_t>(chunk, walks - first);
-        rc = walk_records(M->layout, M->target, first, n, seed, M->opts, st, d_end, d_rec);
-        if (!rc) rc = cv::launch_features(M->view.dl, trect, (int)M->target, d_rec, (int64_t)n, d_x, nullptr, st);
-        if (!rc) rc = cv::launch_forward(M->net, d_x, (int64_t)n, d_phi, st);
-        if (!rc) rc = cv::launch_cv_reduce(d_end, d_rec, d_phi, (int64_t)n, (int)M->target, d_sums, st);
+        rc = walk_records(M->layout, M->target, first, n, seed, M->opts, st, d_end, nullptr, d_w, d_q);
+        if (!rc) rc = cv::launch_cv_gather(d_end, d_w, d_q, M->phi, (int64_t)n, (int)M->target, d_sums, st);
     }
     cudaEventRecord(e1, st);
     double h[4] = {0, 0, 0, 0};
@@ -383,8 +383,11 @@ frw_status frw_cv_walk(const frw_cv *M, uint64_t walks, uint64_t seed, frw_cv_re
 frw_status frw_cv_destroy(frw_cv *M) {
     if (!M) return FRW_OK;
     SetDevice sd(M->view.device);
+    cudaError_t e = cudaDeviceSynchronize();  // nothing may still read the table
     cv::net_free(&M->net);
+    if (M->phi) cudaFreeAsync(M->phi, nullptr);
     delete M;
+    FRW_CK(e);
     return FRW_OK;
 }
 

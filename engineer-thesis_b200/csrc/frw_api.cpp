@@ -173,7 +173,8 @@ struct WalkRun {
 // One job on one layout; records optional; host results optional.
 frw_status run_walks(const frw_layout *lay, int64_t target, uint64_t first_walk, uint64_t walks,
                      uint64_t seed, const frw_opts &o, cudaStream_t st, int64_t *rec_end, int32_t *rec_hops,
-                     int32_t *rec_bin, double *rec_w, WalkRun *out, double4 *rec_cv = nullptr) {
+                     int32_t *rec_bin, double *rec_w, WalkRun *out, double4 *rec_cv = nullptr,
+                     int32_t *rec_q = nullptr) {
     DeviceCtx *ctx;
     frw_status rc = device_ctx(lay->device, &ctx);
     if (rc) return rc;
@@ -241,6 +242,7 @@ frw_status run_walks(const frw_layout *lay, int64_t target, uint64_t first_walk,
     P.rec_bin = rec_bin;
     P.rec_w = rec_w;
     P.rec_cv = rec_cv;
+    P.rec_q = rec_q;
     P.intg = ctx->tables;
     P.wx = ctx->tables + FRW_NSAMPLE + 1;
     P.wy = ctx->tables + 2 * FRW_NSAMPLE + 1;
@@ -341,14 +343,10 @@ frw_status device_tables(int device, const double **tables, int *sms) {
 frw_status check_opts(const frw_opts *o) { return validate_opts(o); }
 
 frw_status walk_records(const frw_layout *L, int64_t target, uint64_t first_walk, uint64_t walks, uint64_t seed,
-                        const frw_opts &o, cudaStream_t st, int64_t *rec_end, double4 *rec_cv) {
-    Scratch S(st);
-    int32_t *dh, *db;
-    double *dw;
-    FRW_CK(S.get(&dh, walks * 4));
-    FRW_CK(S.get(&db, walks * 4));
-    FRW_CK(S.get(&dw, walks * 8));
-    return run_walks(L, target, first_walk, walks, seed, o, st, rec_end, dh, db, dw, nullptr, rec_cv);
+                        const frw_opts &o, cudaStream_t st, int64_t *rec_end, double4 *rec_cv, double *rec_w,
+                        int32_t *rec_q) {
+    return run_walks(L, target, first_walk, walks, seed, o, st, rec_end, nullptr, nullptr, rec_w, nullptr, rec_cv,
+                     rec_q);
 }
 
 frw_status cuda_fail(cudaError_t e, const char *what) {

@@ -48,6 +48,7 @@ struct DevLayout {
     const int2 *cells;
     const float4 *crects;
     const int32_t *cids;
+    const float *crad;  // per cell: every rect within this L-inf distance of any point of the cell is listed
     double gx0, gy0, ginv;
     int32_t gnx, gny;
 };
@@ -100,6 +101,7 @@ struct WalkParams {
     int32_t *rec_hops;
     int32_t *rec_bin;
     double *rec_w;
+    int32_t *rec_q;   // optional: first-hop cell q * 200 + bin of the grid start (-1: no first hop)
     double4 *rec_cv;  // optional: (first-hop point x, y, first square side a0, weight factor c)
     // tables
     const double *intg;  // [201]
@@ -140,6 +142,7 @@ struct CellBuffers {
     int2 *cells = nullptr;
     float4 *crects = nullptr;
     int32_t *cids = nullptr;
+    float *crad = nullptr;
     int64_t ncells = 0, entries = 0, overflow = 0, bytes = 0;
     double gx0 = 0, gy0 = 0, side = 0, ginv = 0;
     int32_t nx = 0, ny = 0;
@@ -189,6 +192,7 @@ frw_status device_tables(int device, const double **tables, int *sms);
 frw_status check_opts(const frw_opts *opts);
 // walks with per-walk end and (first-hop point, a0, weight factor) records (device arrays)
 frw_status walk_records(const frw_layout *layout, int64_t target, uint64_t first_walk, uint64_t walks,
-                        uint64_t seed, const frw_opts &o, cudaStream_t st, int64_t *rec_end, double4 *rec_cv);
+                        uint64_t seed, const frw_opts &o, cudaStream_t st, int64_t *rec_end, double4 *rec_cv,
+                        double *rec_w = nullptr, int32_t *rec_q = nullptr);
 
 }  // namespace frw

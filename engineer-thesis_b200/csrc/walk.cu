@@ -235,6 +235,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
                     if (P.start_grid) {  // midpoint of arc floor(u*Q) of Q equal arcs
                         const uint32_t q = (uint32_t)__dmul_rn(u, (double)P.start_grid);
                         u = __ddiv_rn(__dadd_rn((double)q, 0.5), (double)P.start_grid);
+                        if (P.rec_q) bin1 = -2 - (int)q;  // the arc rides in bin1 until the first hop
                     }
                     if (uniform_start) {
                         side = perimeter_point(G, u, px, py);
@@ -269,6 +270,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
                     const int bin = bin_of(s_intg, word_u(rnd, hop));
                     point_from_index(sq, bin, exact, px, py);
                     if (hop == 1) {
+                        if (P.rec_q) P.rec_q[gw] = (-2 - bin1) * FRW_NSAMPLE + bin;
                         bin1 = bin;
                         a0 = __dsub_rn(sq[2], sq[0]);
                         if (P.rec_cv) *reinterpret_cast<double2 *>(&P.rec_cv[gw]) = make_double2(px, py);
@@ -289,12 +291,11 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
                 c = __ddiv_rn(__dmul_rn(__dmul_rn(-P.permittivity, perim), dot), a0);
             }
             if (code >= 0) wgt = c;
-            if (P.rec_end) {
-                P.rec_end[gw] = code;
-                P.rec_hops[gw] = hops;
-                P.rec_bin[gw] = bin1;
-                P.rec_w[gw] = c;
-            }
+            if (P.rec_end) P.rec_end[gw] = code;
+            if (P.rec_hops) P.rec_hops[gw] = hops;
+            if (P.rec_bin) P.rec_bin[gw] = bin1 < 0 ? -1 : bin1;
+            if (P.rec_w) P.rec_w[gw] = c;
+            if (P.rec_q && bin1 < 0) P.rec_q[gw] = -1;
             if (P.rec_cv) {  // first-hop point written at hop 1 (zero when there was none)
                 if (bin1 < 0) *reinterpret_cast<double2 *>(&P.rec_cv[gw]) = make_double2(0.0, 0.0);
                 reinterpret_cast<double2 *>(&P.rec_cv[gw])[1] = make_double2(a0, c);

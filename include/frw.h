@@ -279,7 +279,10 @@ frw_status frw_batch_destroy(frw_batch *batch);
  * and E[f] is summed exactly over the start grid (opts.start_grid = Q, a
  * power of two) x the 200 first-hop bins, so  mean(w - f) + E[f]  is an
  * unbiased estimate of C_tt; frw_cv_walk reports it next to the plain
- * estimate from the same walks. */
+ * estimate from the same walks.  On the grid start the first-hop point is a
+ * function of (arc, bin), so the exact-mean pass keeps phi of all Q x 200
+ * points in a table (4 bytes each) and frw_cv_walk looks each walk's phi up
+ * there: its walks cost about what plain walks cost. */
 typedef struct frw_cv frw_cv;
 typedef struct frw_cv_opts {
     uint32_t struct_size;  /* sizeof(frw_cv_opts) */
@@ -303,9 +306,9 @@ typedef struct frw_cv_result {
     double plain, plain_se;  /* C_tt from the plain estimator */
     double cv, cv_se;        /* C_tt with the control variate */
     double variance_ratio;   /* plain variance / control-variate variance */
-    double kernel_ms;        /* device time of walks + features + inference + sums */
+    double kernel_ms;        /* device time of walks + phi look-up + sums */
 } frw_cv_result;
-/* walk_opts must use FRW_START_UNIFORM with start_grid a power of two. */
+/* walk_opts must use FRW_START_UNIFORM with start_grid a power of two <= 2^23. */
 frw_status frw_cv_train(const frw_layout *layout, int64_t target, const frw_opts *walk_opts,
                         const frw_cv_opts *cv_opts, frw_cv **out, void *stream);
 frw_status frw_cv_info_get(const frw_cv *cv, frw_cv_info *info);

@@ -853,22 +853,24 @@ int64_t oc_walk_stream(const oc_grid *g, const oc_rtree *t, int defect, const do
 /* ------------------------------------------------------------------------ */
 /* Control-variate features (brute force over all rects)                    */
 /* ------------------------------------------------------------------------ */
-static float cv_feat(double d, double a0) {
-    double v = d / a0;
+/* d / a0 as d * (1 / a0), clamped to [-16, 16] */
+static float cv_feat(double d, double inv) {
+    double v = d * inv;
     v = fmin(fmax(v, -16.0), 16.0);
     return (float)v;
 }
 
 static void cv_edges(double px, double py, const double *r, double a0, float *f) {
     double cx = fmin(fmax(px, r[0]), r[2]), cy = fmin(fmax(py, r[1]), r[3]);
-    f[0] = cv_feat(cx - px, a0);
-    f[1] = cv_feat(r[1] - py, a0);
-    f[2] = cv_feat(r[2] - px, a0);
-    f[3] = cv_feat(cy - py, a0);
-    f[4] = cv_feat(cx - px, a0);
-    f[5] = cv_feat(r[3] - py, a0);
-    f[6] = cv_feat(r[0] - px, a0);
-    f[7] = cv_feat(cy - py, a0);
+    double inv = 1.0 / a0;
+    f[0] = cv_feat(cx - px, inv);
+    f[1] = cv_feat(r[1] - py, inv);
+    f[2] = cv_feat(r[2] - px, inv);
+    f[3] = cv_feat(cy - py, inv);
+    f[4] = f[0];
+    f[5] = cv_feat(r[3] - py, inv);
+    f[6] = cv_feat(r[0] - px, inv);
+    f[7] = f[3];
 }
 
 void oc_cv_features(const double *rects, int64_t n, int64_t target, const double *rec4, int64_t m,

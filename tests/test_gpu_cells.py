@@ -92,3 +92,28 @@ def test_walks_identical_with_and_without_cells(golden):
         c = L.walk_trace(17, 0, 20_000, seed=5, o=o)
     for x, y, z in zip(a, b, c):
         assert np.array_equal(x, y) and np.array_equal(x, z)
+
+
+def test_cv_features_equal_with_and_without_cells():
+    """The nearest-other-conductor lookup of the control-variate features
+    answers from the cell list when the list settles it and from the tree
+    otherwise; both give the oracle's features bit for bit."""
+    rects = frw.generate_layout(0xF4A7 + 2, 10_000, 1e4)
+    rng = np.random.default_rng(3)
+    n = 30_000
+    rec = np.zeros((n, 4))
+    t = 0
+    r = rects[t].astype(np.float64)
+    rec[: n // 2, 0] = rng.uniform(r[0] - 60, r[2] + 60, n // 2)
+    rec[: n // 2, 1] = rng.uniform(r[1] - 60, r[3] + 60, n // 2)
+    with frw.Layout.from_rects(rects) as L:
+        b = L.bounds
+        rec[n // 2:, 0] = rng.uniform(b[0], b[2], n - n // 2)
+        rec[n // 2:, 1] = rng.uniform(b[1], b[3], n - n // 2)
+        rec[:, 2] = rng.choice([1.0, 2.5, 7.0], n)
+        f_cells = L.cv_features(t, rec)
+        L.set_cells(0)
+        f_tree = L.cv_features(t, rec)
+    assert np.array_equal(f_cells, f_tree)
+    want = O.cv_features(rects.astype(np.float64), t, rec[::10])
+    assert np.array_equal(f_cells[::10], want)
