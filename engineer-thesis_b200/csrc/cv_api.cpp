@@ -110,8 +110,8 @@ void frw_cv_opts_default(frw_cv_opts *o) {
     o->train_walks = 1000000;
     o->train_seed = 0x7E57C0DEull;
     o->epochs = 4;
-    o->batch = 8192;
-    o->lr = 3e-3f;
+    o->batch = 32768;
+    o->lr = 6e-3f;
 }
 
 frw_status frw_cv_train(const frw_layout *layout, int64_t target, const frw_opts *walk_opts,

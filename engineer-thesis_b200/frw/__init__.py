@@ -519,7 +519,7 @@ class Batch:
             pass
 
 
-def cv_opts(train_walks=1_000_000, train_seed=0x7E57C0DE, epochs=4, batch=8192, lr=3e-3) -> CvOpts:
+def cv_opts(train_walks=1_000_000, train_seed=0x7E57C0DE, epochs=4, batch=32768, lr=6e-3) -> CvOpts:
     o = CvOpts()
     lib().frw_cv_opts_default(C.byref(o))
     o.train_walks, o.train_seed, o.epochs, o.batch, o.lr = train_walks, train_seed, epochs, batch, lr

@@ -289,8 +289,8 @@ typedef struct frw_cv_opts {
     uint64_t train_walks;  /* walks generating training pairs (default 1e6) */
     uint64_t train_seed;   /* independent of the estimation seed */
     int32_t epochs;        /* passes over the training pairs (default 4) */
-    int32_t batch;         /* rows per Adam step, a multiple of 64 (default 8192) */
-    float lr;              /* Adam step size (default 3e-3) */
+    int32_t batch;         /* rows per Adam step, a multiple of 64 (default 32768) */
+    float lr;              /* Adam step size (default 6e-3) */
 } frw_cv_opts;
 void frw_cv_opts_default(frw_cv_opts *opts);
 typedef struct frw_cv_info {

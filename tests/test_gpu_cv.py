@@ -75,7 +75,7 @@ def test_cv_unbiased_and_reduces_variance():
     rects = config1()
     o = frw.capacitance_opts(1.0, start_grid=4096)
     with frw.Layout.from_rects(rects) as L:
-        cv = frw.ControlVariate(L, 0, o, frw.cv_opts(train_walks=200_000, epochs=6, batch=4096))
+        cv = frw.ControlVariate(L, 0, o, frw.cv_opts(train_walks=200_000, epochs=6, batch=4096, lr=3e-3))
         info = cv.info
         r = cv.walk(2_000_000, seed=99)
         ref = L.walk(0, 20_000_000, seed=12345, o=o)  # independent plain run
@@ -92,7 +92,7 @@ def test_cv_mean_term_is_the_mean_of_f():
     rects = config1()
     o = frw.capacitance_opts(1.0, start_grid=1024)
     with frw.Layout.from_rects(rects) as L:
-        cv = frw.ControlVariate(L, 0, o, frw.cv_opts(train_walks=100_000, epochs=3, batch=4096))
+        cv = frw.ControlVariate(L, 0, o, frw.cv_opts(train_walks=100_000, epochs=3, batch=4096, lr=3e-3))
         mu = cv.info.mean_term
         r = cv.walk(8_000_000, seed=7)
         cv.close()
@@ -124,7 +124,7 @@ def test_cv_exact_mean_equals_enumeration():
     Q = 256
     o = frw.capacitance_opts(1.0, start_grid=Q)
     with frw.Layout.from_rects(rects) as L:
-        cv = frw.ControlVariate(L, 0, o, frw.cv_opts(train_walks=50_000, epochs=2, batch=4096))
+        cv = frw.ControlVariate(L, 0, o, frw.cv_opts(train_walks=50_000, epochs=2, batch=4096, lr=3e-3))
         mu = cv.info.mean_term
         params = cv.params()
         cv.close()
