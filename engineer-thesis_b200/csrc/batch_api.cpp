@@ -69,6 +69,7 @@ WalkParams params_for(const frw_batch *B, const WalkJob *jobs, const WalkJob &jo
     P.exact_perimeter = B->opts.exact_perimeter;
     P.refill_min = t.refill_min > 0 ? t.refill_min : 1;
     P.start_grid = B->opts.start_grid;
+    P.start_strata = B->opts.start_strata;
     P.hop_cap = B->opts.hop_cap;
     P.permittivity = B->opts.permittivity;
     P.seed_dev = B->d_seed;

@@ -141,6 +141,10 @@ frw_status validate_opts(const frw_opts *o) {
         set_error("frw_opts.gauss_param / hop_cap");
         return FRW_E_ARG;
     }
+    if (o->start_grid && o->start_mode != FRW_START_UNIFORM) {
+        set_error("frw_opts.start_grid needs FRW_START_UNIFORM");
+        return FRW_E_ARG;
+    }
     return FRW_OK;
 }
 
@@ -227,6 +231,7 @@ frw_status run_walks(const frw_layout *lay, int64_t target, uint64_t first_walk,
     P.exact_perimeter = o.exact_perimeter;
     P.refill_min = o.refill_min > 0 ? o.refill_min : 1;
     P.start_grid = o.start_grid;
+    P.start_strata = o.start_strata;
     P.hop_cap = o.hop_cap;
     P.permittivity = o.permittivity;
     P.seed = seed;

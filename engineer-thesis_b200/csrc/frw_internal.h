@@ -82,6 +82,7 @@ struct WalkParams {
     int32_t exact_perimeter;
     int32_t refill_min;
     uint32_t start_grid;   // 0: continuous uniform start; Q: midpoints of Q equal arcs
+    uint32_t start_strata; // 0: off; S: walk w draws its start in stratum w mod S
     int64_t hop_cap;
     double permittivity;
     uint64_t seed;

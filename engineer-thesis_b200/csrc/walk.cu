@@ -232,6 +232,10 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
                     a0 = 0.0;
                     rnd = draw_block(seed, stream, pw, 0);
                     double u = word_u(rnd, 0);
+                    if (P.start_strata) {  // stratum pw mod S of the start distribution
+                        const double s = (double)(uint32_t)(pw % P.start_strata);
+                        u = __ddiv_rn(__dadd_rn(s, u), (double)P.start_strata);
+                    }
                     if (P.start_grid) {  // midpoint of arc floor(u*Q) of Q equal arcs
                         const uint32_t q = (uint32_t)__dmul_rn(u, (double)P.start_grid);
                         u = __ddiv_rn(__dadd_rn((double)q, 0.5), (double)P.start_grid);

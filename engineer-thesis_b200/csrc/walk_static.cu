@@ -114,6 +114,7 @@ extern "C" frw_status frw_walk_trace_static(const frw_layout *layout, int64_t ta
         P.exact_perimeter = o.exact_perimeter;
         P.refill_min = o.refill_min > 0 ? o.refill_min : 1;
         P.start_grid = o.start_grid;
+        P.start_strata = o.start_strata;
         P.hop_cap = o.hop_cap;
         P.permittivity = o.permittivity;
         P.seed = seed;

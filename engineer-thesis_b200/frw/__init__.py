@@ -59,6 +59,7 @@ class Opts(C.Structure):
         ("refill_min", C.c_int32),
         ("start_grid", C.c_uint32),
         ("first_walk", C.c_uint64),
+        ("start_strata", C.c_uint32),
     ]
 
 
@@ -250,7 +251,7 @@ def green_table():
 
 def opts(gauss_mode=GAUSS_SCALE, gauss_param=1.5, start_mode=START_GREEN, exact_perimeter=False,
          hop_cap=100000, stream_id=0, blocks_per_sm=0, refill_min=1, permittivity=PERMITTIVITY,
-         start_grid=0, first_walk=0) -> Opts:
+         start_grid=0, first_walk=0, start_strata=0) -> Opts:
     o = Opts()
     lib().frw_opts_default(C.byref(o))
     o.gauss_mode = gauss_mode
@@ -264,6 +265,7 @@ def opts(gauss_mode=GAUSS_SCALE, gauss_param=1.5, start_mode=START_GREEN, exact_
     o.permittivity = permittivity
     o.start_grid = start_grid
     o.first_walk = first_walk
+    o.start_strata = start_strata
     return o
 
 

@@ -167,6 +167,11 @@ typedef struct frw_opts {
                                 ranges are independent and their rows (hits, sum_w, sum_w2) add up
                                 exactly to one run over the union: a run can be checkpointed as
                                 (seed, stream_id, next first_walk, rows) and resumed. */
+    uint32_t start_strata;   /* 0 = off; S > 0: walk w starts in stratum w mod S of the start
+                                distribution, u = (w mod S + U) / S (U the walk's first uniform),
+                                for either start mode.  Unbiased when the walk range covers every
+                                stratum equally (walks and first_walk multiples of S); the reported
+                                standard error stays the i.i.d. one, an upper bound. */
 } frw_opts;
 void frw_opts_default(frw_opts *opts);
 

@@ -779,6 +779,7 @@ int oc_walk_run(const oc_grid *g, const double *rects, const oc_walk_cfg *cfg, u
         double u0, p[2], nrm[2] = {0, 0}, sq[4];
         uint32_t hop = 0;
         u0 = draw(cfg->seed, cfg->stream, w, hop);
+        if (cfg->start_strata) u0 = ((double)(uint32_t)(w % cfg->start_strata) + u0) / (double)cfg->start_strata;
         if (cfg->start_mode == OC_START_UNIFORM) {
             if (cfg->start_grid) {
                 uint32_t q = (uint32_t)(u0 * (double)cfg->start_grid);

@@ -137,6 +137,7 @@ typedef struct oc_walk_cfg {
     uint64_t seed;
     uint32_t stream;       /* Philox counter word 3 */
     uint32_t start_grid;   /* uniform start: 0 continuous, Q = midpoints of Q equal arcs */
+    uint32_t start_strata; /* 0 off; S: walk w starts in stratum w mod S, u = (w mod S + u) / S */
 } oc_walk_cfg;
 
 /* Gaussian surface of cfg->target (complete semantics). */

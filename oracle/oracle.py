@@ -55,6 +55,7 @@ class WalkCfg(C.Structure):
         ("seed", C.c_uint64),
         ("stream", C.c_uint32),
         ("start_grid", C.c_uint32),
+        ("start_strata", C.c_uint32),
     ]
 
 
@@ -202,9 +203,9 @@ class Grid:
         return o
 
     def walk_cfg(self, target=0, gauss_mode=GAUSS_OFFSET, gauss_param=1.0, start_mode=START_UNIFORM,
-                 exact_perimeter=False, hop_cap=100000, seed=1, stream=0, start_grid=0):
+                 exact_perimeter=False, hop_cap=100000, seed=1, stream=0, start_grid=0, start_strata=0):
         return WalkCfg(target, gauss_mode, gauss_param, start_mode, int(exact_perimeter), hop_cap,
-                       PERMITTIVITY, seed, stream, start_grid)
+                       PERMITTIVITY, seed, stream, start_grid, start_strata)
 
     def gauss_surface(self, cfg: WalkCfg):
         o = np.zeros(4)

@@ -13,7 +13,7 @@ pytestmark = pytest.mark.gpu
 def oracle_cfg(G, o: frw.Opts, target, seed):
     return G.walk_cfg(target=target, gauss_mode=o.gauss_mode, gauss_param=o.gauss_param,
                       start_mode=o.start_mode, exact_perimeter=bool(o.exact_perimeter), hop_cap=o.hop_cap,
-                      seed=seed, stream=o.stream_id, start_grid=o.start_grid)
+                      seed=seed, stream=o.stream_id, start_grid=o.start_grid, start_strata=o.start_strata)
 
 
 CASES = [
@@ -26,6 +26,11 @@ CASES = [
                           stream_id=3)),
     ("test100", 5, dict(gauss_mode=frw.GAUSS_OFFSET, gauss_param=1.0, start_mode=frw.START_UNIFORM,
                         start_grid=4096)),
+    ("test100", 7, dict(gauss_mode=frw.GAUSS_OFFSET, gauss_param=1.0, start_mode=frw.START_UNIFORM,
+                        start_strata=64)),
+    ("test2", 10, dict(start_strata=7)),  # Green-CDF start, stratified
+    ("test100", 5, dict(gauss_mode=frw.GAUSS_OFFSET, gauss_param=1.0, start_mode=frw.START_UNIFORM,
+                        start_grid=4096, start_strata=256)),
 ]
 
 
@@ -207,3 +212,24 @@ def test_multilayer_file_and_layer_flag(tmp_path):
         assert np.array_equal(L.rects(), b.astype(np.float64))
     with pytest.raises(frw.FrwError):
         frw.Layout.from_file(p, layer=2)
+
+
+def test_stratified_start_unbiased_and_not_worse():
+    """C1 with the start stratified into 1024 strata: the row agrees with an
+    unstratified run within errors, and the spread of C_00 over independent
+    seeds is no larger than without strata."""
+    rects = config1_layout()
+    n, S = 1 << 17, 1024
+    o0 = frw.capacitance_opts(1.0)
+    o1 = frw.capacitance_opts(1.0, start_strata=S)
+    with frw.Layout.from_rects(rects) as L:
+        plain = np.array([L.walk(0, n, seed=100 + k, o=o0).row(0)[1] for k in range(24)])
+        strat = np.array([L.walk(0, n, seed=100 + k, o=o1).row(0)[1] for k in range(24)])
+    assert abs(plain.mean() - strat.mean()) <= 4 * np.hypot(plain.std(ddof=1), strat.std(ddof=1)) / np.sqrt(24)
+    assert strat.std(ddof=1) <= 1.25 * plain.std(ddof=1)
+
+
+def test_start_grid_needs_uniform_start():
+    with frw.Layout.from_rects(config1_layout()) as L:
+        with pytest.raises(frw.FrwError, match="start_grid"):
+            L.walk(0, 1000, seed=1, o=frw.opts(start_grid=64))
