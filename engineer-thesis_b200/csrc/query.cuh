@@ -222,7 +222,13 @@ __device__ __forceinline__ uint32_t replay_square(const DevLayout &L, const Cand
     double dist = L.dist0;
     bool maxReached = false, isc;
     uint32_t st = 0;
-    int it = 0;
+    // the loop's first box is p +- 1 again, already found free: its step (grow
+    // by dist, no halving before the first collision) is taken directly
+    o[0] = __dsub_rn(o[0], dist);
+    o[1] = __dsub_rn(o[1], dist);
+    o[2] = __dadd_rn(o[2], dist);
+    o[3] = __dadd_rn(o[3], dist);
+    int it = 1;
     while ((isc = collides_box(L, C, o, px, dstar)) || !maxReached || dist > kMinDist) {
         if (isc) {
             if (dist > kMinDist) dist = __dmul_rn(dist, 0.5);

@@ -66,7 +66,9 @@ __device__ __forceinline__ double word_u(const uint4 &b, uint32_t hop) {
     return (double)x * 0x1p-32;
 }
 
-__device__ __forceinline__ int bin_of(const double *s_intg, double u) {
+// The last bin lo in [0, 200) with intg[lo] <= u (intg nondecreasing,
+// intg[0] = 0), by binary search.
+__device__ __forceinline__ int bin_search(const double *s_intg, double u) {
     int lo = 0, hi = FRW_NSAMPLE;  // intg[lo] <= u
 #pragma unroll
     for (int k = 0; k < 8; k++) {
@@ -76,6 +78,15 @@ __device__ __forceinline__ int bin_of(const double *s_intg, double u) {
             else hi = mid;
         }
     }
+    return lo;
+}
+
+// The same bin from a guide table: guide[k] = bin_search(k / 256), so the
+// bin of u in [k/256, (k+1)/256) is guide[k] or one of the next few.
+constexpr int kGuide = 256;
+__device__ __forceinline__ int bin_of(const double *s_intg, const uint8_t *guide, double u) {
+    int lo = guide[(int)__dmul_rn(u, (double)kGuide)];
+    while (lo < FRW_NSAMPLE - 1 && s_intg[lo + 1] <= u) lo++;
     return lo;
 }
 
@@ -184,6 +195,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
     __shared__ double s_intg[FRW_NSAMPLE + 1];
     __shared__ double s_wx[FRW_NSAMPLE], s_wy[FRW_NSAMPLE];
     __shared__ Slot s_tab[kWarpsPerBlock][kTabSlots];
+    __shared__ uint8_t s_guide[kGuide];
 
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     for (int i = threadIdx.x; i <= FRW_NSAMPLE; i += blockDim.x) s_intg[i] = P.intg[i];
@@ -193,6 +205,9 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
     }
     Slot *tab = s_tab[wib];
     for (int q = lane; q < kTabSlots; q += 32) tab[q].key = kEmptyKey;
+    __syncthreads();
+    for (int k = threadIdx.x; k < kGuide; k += blockDim.x)
+        s_guide[k] = (uint8_t)bin_search(s_intg, (double)k * (1.0 / kGuide));
     __syncthreads();
 
     const uint32_t lt = (1u << lane) - 1u;
@@ -284,7 +299,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
                     if (uniform_start) {
                         side = perimeter_point(G, u, px, py);
                     } else {
-                        point_from_index(G, bin_of(s_intg, u), exact, px, py);
+                        point_from_index(G, bin_of(s_intg, s_guide, u), exact, px, py);
                     }
                     active = true;
                 }
@@ -321,7 +336,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
                 else {
                     hop++;
                     if ((hop & 3) == 0) rnd = draw_block(seed, stream, pw, hop);
-                    const int bin = bin_of(s_intg, word_u(rnd, hop));
+                    const int bin = bin_of(s_intg, s_guide, word_u(rnd, hop));
                     point_from_index(sq, bin, exact, px, py);
                     if (hop == 1) {
                         if (P.rec_q) P.rec_q[gw] = (-2 - bin1) * FRW_NSAMPLE + bin;
