@@ -196,6 +196,8 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
     __shared__ double s_wx[FRW_NSAMPLE], s_wy[FRW_NSAMPLE];
     __shared__ Slot s_tab[kWarpsPerBlock][kTabSlots];
     __shared__ uint8_t s_guide[kGuide];
+    __shared__ unsigned long long s_chunk[kWarpsPerBlock][2];  // per warp: unclaimed part of its walk chunk
+    __shared__ unsigned long long s_lhops[kWalkThreads];       // per lane: hops of its walks (current job)
 
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     for (int i = threadIdx.x; i <= FRW_NSAMPLE; i += blockDim.x) s_intg[i] = P.intg[i];
@@ -205,6 +207,8 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
     }
     Slot *tab = s_tab[wib];
     for (int q = lane; q < kTabSlots; q += 32) tab[q].key = kEmptyKey;
+    if (lane == 0) s_chunk[wib][0] = s_chunk[wib][1] = 0;
+    s_lhops[threadIdx.x] = 0;
     __syncthreads();
     for (int k = threadIdx.x; k < kGuide; k += blockDim.x)
         s_guide[k] = (uint8_t)bin_search(s_intg, (double)k * (1.0 / kGuide));
@@ -218,9 +222,8 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
     const uint64_t kChunk = P.chunk ? (uint64_t)P.chunk : kChunkDefault;
 
     bool active = false, exhausted = false;
-    uint64_t chunk_next = 0, chunk_end = 0;  // warp-uniform: unclaimed part of this warp's walk chunk
     int job = 0;
-    uint64_t gw = 0, pw = 0;
+    uint64_t pw = 0;
     uint32_t hop = 0, stream = 0;
     uint4 rnd = make_uint4(0, 0, 0, 0);  // uniforms of hops (hop & ~3) .. +3
     int32_t hops = 0, bin1 = -1;
@@ -232,9 +235,13 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
     // 10k-rect layout) are counted and summed in registers and reach the
     // table in one insertion when the lane changes job and at exit; the hops
     // of all its walks likewise go to the job's totals then.
-    unsigned long long pn = 0, lane_hops = 0;
+    uint32_t pn = 0;
     double ps = 0.0, ps2 = 0.0;
     int pjob = 0;
+    auto walk_index = [&]() {  // record index of the lane's walk
+        const WalkJob &J = job_of<kMulti>(P, job);
+        return J.walk_begin + (pw - J.first_walk);
+    };
     auto target_key = [&](int j) {
         return ((unsigned long long)j << 32) | (uint32_t)(job_of<kMulti>(P, j).target + 2);
     };
@@ -243,6 +250,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
         // ---- refill idle lanes from the warp's chunk of the walk counter ----
         const unsigned idle = __ballot_sync(kFull, !active);
         if (!exhausted && __popc(idle) >= refill_min) {
+            uint64_t chunk_next = s_chunk[wib][0], chunk_end = s_chunk[wib][1];
             const uint64_t need = (uint64_t)__popc(idle), avail = chunk_end - chunk_next;
             const uint64_t r = (uint64_t)__popc(idle & lt);
             uint64_t mine;
@@ -259,8 +267,14 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
                 chunk_end = nb + kChunk;
             }
             if (chunk_end >= P.total_walks && chunk_next >= P.total_walks) exhausted = true;
+            __syncwarp();
+            if (lane == 0) {
+                s_chunk[wib][0] = chunk_next;
+                s_chunk[wib][1] = chunk_end;
+            }
+            __syncwarp();
             if (!active) {
-                gw = mine;
+                const uint64_t gw = mine;
                 if (gw < P.total_walks) {
                     if (kMulti) {  // the job whose walk range holds gw
                         const bool same = gw >= P.jobs[job].walk_begin &&
@@ -308,8 +322,10 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
                 const bool moved = job != pjob;
                 tab_round<kMulti>(P, tab, lane, lt, moved && pn > 0, target_key(pjob), pn, ps, ps2);
                 if (moved) {
-                    if (lane_hops) atomicAdd(P.job_stats + 4 * pjob + 2, lane_hops);
-                    pn = lane_hops = 0;
+                    const unsigned long long lh = s_lhops[threadIdx.x];
+                    if (lh) atomicAdd(P.job_stats + 4 * pjob + 2, lh);
+                    s_lhops[threadIdx.x] = 0;
+                    pn = 0;
                     ps = ps2 = 0.0;
                     pjob = job;
                 }
@@ -339,10 +355,10 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
                     const int bin = bin_of(s_intg, s_guide, word_u(rnd, hop));
                     point_from_index(sq, bin, exact, px, py);
                     if (hop == 1) {
-                        if (P.rec_q) P.rec_q[gw] = (-2 - bin1) * FRW_NSAMPLE + bin;
+                        if (P.rec_q) P.rec_q[walk_index()] = (-2 - bin1) * FRW_NSAMPLE + bin;
                         bin1 = bin;
                         a0 = __dsub_rn(sq[2], sq[0]);
-                        if (P.rec_cv) *reinterpret_cast<double2 *>(&P.rec_cv[gw]) = make_double2(px, py);
+                        if (P.rec_cv) *reinterpret_cast<double2 *>(&P.rec_cv[walk_index()]) = make_double2(px, py);
                     }
                 }
             }
@@ -362,6 +378,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
                 c = __ddiv_rn(__dmul_rn(__dmul_rn(-P.permittivity, perim), dot), a0);
             }
             if (code >= 0) wgt = c;
+            const uint64_t gw = walk_index();
             if (P.rec_end) P.rec_end[gw] = code;
             if (P.rec_hops) P.rec_hops[gw] = hops;
             if (P.rec_bin) P.rec_bin[gw] = bin1 < 0 ? -1 : bin1;
@@ -372,7 +389,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
                 reinterpret_cast<double2 *>(&P.rec_cv[gw])[1] = make_double2(a0, c);
             }
             active = false;
-            lane_hops += (unsigned long long)hops;
+            s_lhops[threadIdx.x] += (unsigned long long)hops;
             if ((int64_t)code == job_of<kMulti>(P, job).target) {
                 pn++;
                 ps = __dadd_rn(ps, wgt);
@@ -386,7 +403,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
     }
     __syncwarp();
     tab_round<kMulti>(P, tab, lane, lt, pn > 0, target_key(pjob), pn, ps, ps2);
-    if (lane_hops) atomicAdd(P.job_stats + 4 * pjob + 2, lane_hops);
+    if (s_lhops[threadIdx.x]) atomicAdd(P.job_stats + 4 * pjob + 2, s_lhops[threadIdx.x]);
     tab_flush<kMulti>(P, tab, lane);
     if (st) atomicOr(P.status, st);
 }
