@@ -180,10 +180,8 @@ __device__ __forceinline__ void child_bounds(const uint32_t *keys, int level, in
 }
 
 // Per frontier entry: (new nodes << 32) | (next-frontier entries).
-__global__ void k_split_count(const uint32_t *__restrict__ keys, Frontier fr, int nfr, int leaf_max,
-                              unsigned long long *__restrict__ cnt) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nfr) return;
+__device__ __forceinline__ unsigned long long split_count_one(const uint32_t *keys, const Frontier &fr, int i,
+                                                              int leaf_max) {
     int b[5];
     int level = fr.level[i];
     child_bounds(keys, level, fr.start[i], fr.end[i], b);
@@ -193,17 +191,22 @@ __global__ void k_split_count(const uint32_t *__restrict__ keys, Frontier fr, in
         nonempty += m > 0;
         big += m > leaf_max;
     }
-    unsigned long long v;
-    if (nonempty == 1 && level < 16 && big == 1) v = 1ull;  // compress: re-split one level down
-    else v = ((unsigned long long)big << 32) | (unsigned long long)big;
-    cnt[i] = v;
+    if (nonempty == 1 && level < 16 && big == 1) return 1ull;  // compress: re-split one level down
+    return ((unsigned long long)big << 32) | (unsigned long long)big;
 }
 
-__global__ void k_split_emit(const uint32_t *__restrict__ keys, Frontier fr, int nfr, int leaf_max,
-                             const unsigned long long *__restrict__ off, int node_base,
-                             int4 *__restrict__ nref, Frontier nx) {
+__global__ void k_split_count(const uint32_t *__restrict__ keys, Frontier fr, int nfr, int leaf_max,
+                              unsigned long long *__restrict__ cnt) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nfr) return;
+    cnt[i] = split_count_one(keys, fr, i, leaf_max);
+}
+
+// Per frontier entry with its scanned offsets: the node's child references
+// and the next frontier's entries.
+__device__ __forceinline__ void split_emit_one(const uint32_t *keys, const Frontier &fr, int i, int leaf_max,
+                                               unsigned long long o, int node_base, int4 *nref,
+                                               const Frontier &nx) {
     int b[5];
     int level = fr.level[i], node = fr.node[i];
     child_bounds(keys, level, fr.start[i], fr.end[i], b);
@@ -213,7 +216,6 @@ __global__ void k_split_emit(const uint32_t *__restrict__ keys, Frontier fr, int
         nonempty += m > 0;
         big += m > leaf_max;
     }
-    unsigned long long o = off[i];
     int onode = (int)(o >> 32), onext = (int)(o & 0xFFFFFFFFull);
     if (nonempty == 1 && level < 16 && big == 1) {
         nx.node[onext] = node;
@@ -241,15 +243,20 @@ __global__ void k_split_emit(const uint32_t *__restrict__ keys, Frontier fr, int
     nref[node] = make_int4(ref[0], ref[1], ref[2], ref[3]);
 }
 
+__global__ void k_split_emit(const uint32_t *__restrict__ keys, Frontier fr, int nfr, int leaf_max,
+                             const unsigned long long *__restrict__ off, int node_base,
+                             int4 *__restrict__ nref, Frontier nx) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nfr) return;
+    split_emit_one(keys, fr, i, leaf_max, off[i], node_base, nref, nx);
+}
+
 __device__ __forceinline__ float4 box_union(float4 a, float4 b) {
     return make_float4(fminf(a.x, b.x), fminf(a.y, b.y), fmaxf(a.z, b.z), fmaxf(a.w, b.w));
 }
 
-__global__ void k_refit(const float4 *__restrict__ rects, const int4 *__restrict__ nref,
-                        float4 *__restrict__ nbox, int a, int b) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    int node = a + (t >> 2), c = t & 3;
-    if (node >= b) return;
+// Child box c of `node`: the union of its child's boxes or of its leaf's rects.
+__device__ __forceinline__ void refit_one(const float4 *rects, const int4 *nref, float4 *nbox, int node, int c) {
     int4 r4 = nref[node];
     int ref = c == 0 ? r4.x : c == 1 ? r4.y : c == 2 ? r4.z : r4.w;
     const float inf = __int_as_float(0x7f800000);
@@ -261,6 +268,125 @@ __global__ void k_refit(const float4 *__restrict__ rects, const int4 *__restrict
         for (int k = 0; k < m; k++) box = box_union(box, rects[f + k]);
     }
     nbox[4 * node + c] = box;
+}
+
+__global__ void k_refit(const float4 *__restrict__ rects, const int4 *__restrict__ nref,
+                        float4 *__restrict__ nbox, int a, int b) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int node = a + (t >> 2), c = t & 3;
+    if (node >= b) return;
+    refit_one(rects, nref, nbox, node, c);
+}
+
+// Exclusive scan over one block of 1024 threads; every thread gets the total.
+__device__ __forceinline__ unsigned long long block_scan_u64(unsigned long long v, unsigned long long *wt,
+                                                             unsigned long long &total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    unsigned long long x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wt[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        unsigned long long t = wt[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(0xFFFFFFFFu, t, o);
+            if (lane >= o) t += y;
+        }
+        wt[lane] = t;
+    }
+    __syncthreads();
+    total = wt[31];
+    const unsigned long long before = w ? wt[w - 1] : 0ull;
+    __syncthreads();
+    return before + x - v;
+}
+
+constexpr int kSmallBuild = 1 << 16;  // layouts up to this many rects split and refit in one block
+constexpr int kMaxLevels = 64;
+
+// The whole level-synchronous split and the bottom-up refit of a small
+// layout in one block of 1024 threads: the same count -> scan -> emit steps
+// as the multi-kernel path (so the same node numbering), with the frontier
+// sizes kept on the device instead of read back per level.  out[0] nodes,
+// out[1] depth, out[2] 1 when the level bound was hit.
+__global__ void __launch_bounds__(1024) k_build_small(const uint32_t *__restrict__ keys, int n, Frontier fa,
+                                                      Frontier fb, int leaf_max, unsigned long long *cnt,
+                                                      int4 *nref, const float4 *__restrict__ rects,
+                                                      float4 *nbox, int *out) {
+    __shared__ unsigned long long wt[32];
+    __shared__ int s_nfr, s_nodes, s_depth, s_nb, s_over;
+    __shared__ int s_batch[kMaxLevels + 4];
+    const int t = threadIdx.x;
+    if (t == 0) {
+        s_nodes = 1;
+        s_depth = 0;
+        s_over = 0;
+        s_batch[0] = 0;
+        s_batch[1] = 1;
+        s_nb = 2;
+        if (n <= leaf_max) {  // a layout of <= leaf_max rects still gets one internal root node
+            nref[0] = make_int4(leaf_ref(0, n), kRefEmpty, kRefEmpty, kRefEmpty);
+            s_nfr = 0;
+        } else {
+            fa.node[0] = 0;
+            fa.level[0] = 0;
+            fa.start[0] = 0;
+            fa.end[0] = n;
+            s_nfr = 1;
+        }
+    }
+    __syncthreads();
+    for (int iter = 0;; iter++) {
+        const int nfr = s_nfr;
+        if (nfr == 0) break;
+        if (iter > kMaxLevels) {
+            if (t == 0) s_over = 1;
+            break;
+        }
+        for (int i = t; i < nfr; i += 1024) cnt[i] = split_count_one(keys, fa, i, leaf_max);
+        __syncthreads();
+        unsigned long long carry = 0;
+        for (int b0 = 0; b0 < nfr; b0 += 1024) {
+            const int i = b0 + t;
+            const unsigned long long v = i < nfr ? cnt[i] : 0ull;
+            unsigned long long total;
+            const unsigned long long e = block_scan_u64(v, wt, total);
+            if (i < nfr) cnt[i] = carry + e;
+            carry += total;
+        }
+        __syncthreads();
+        const int node_base = s_nodes;
+        for (int i = t; i < nfr; i += 1024) split_emit_one(keys, fa, i, leaf_max, cnt[i], node_base, nref, fb);
+        __syncthreads();
+        if (t == 0) {
+            const int new_nodes = (int)(carry >> 32);
+            if (new_nodes > 0) {
+                s_nodes += new_nodes;
+                s_batch[s_nb++] = s_nodes;
+                s_depth++;
+            }
+            s_nfr = (int)(carry & 0xFFFFFFFFull);
+        }
+        const Frontier tmp = fa;
+        fa = fb;
+        fb = tmp;
+        __syncthreads();
+    }
+    for (int k = s_nb - 1; k > 0; k--) {
+        const int a = s_batch[k - 1], b = s_batch[k];
+        for (int q = t; q < 4 * (b - a); q += 1024) refit_one(rects, nref, nbox, a + (q >> 2), q & 3);
+        __syncthreads();
+    }
+    if (t == 0) {
+        out[0] = s_nodes;
+        out[1] = s_depth;
+        out[2] = s_over;
+    }
 }
 
 }  // namespace
@@ -311,7 +437,7 @@ frw_status build_tree(const float4 *d_rects_in, int32_t n, const double bounds[4
         if (!ck(cudaMallocAsync(&v1, (size_t)n * 4, st), "malloc vals")) break;
         if (!ck(cudaMallocAsync(&hist, (size_t)256 * nblk * 4, st), "malloc hist")) break;
         if (!ck(cudaMallocAsync(&cnt, (size_t)cap_nodes * 8, st), "malloc cnt")) break;
-        if (!ck(cudaMallocAsync(&tot, 8, st), "malloc tot")) break;
+        if (!ck(cudaMallocAsync(&tot, 16, st), "malloc tot")) break;  // scan total, or the small build's result
         if (!ck(cudaMallocAsync(&frb, (size_t)cap_nodes * 8 * 4, st), "malloc frontier")) break;
 
         double W = bounds[2] - bounds[0], H = bounds[3] - bounds[1];
@@ -333,21 +459,36 @@ frw_status build_tree(const float4 *d_rects_in, int32_t n, const double bounds[4
         // level-synchronous split
         Frontier fa{frb, frb + cap_nodes, frb + 2 * cap_nodes, frb + 3 * cap_nodes};
         Frontier fb{frb + 4 * cap_nodes, frb + 5 * cap_nodes, frb + 6 * cap_nodes, frb + 7 * cap_nodes};
+        if (n <= kSmallBuild) {  // one block: no host round trip per level
+            k_build_small<<<1, 1024, 0, st>>>(k0, n, fa, fb, leaf_max, cnt, T.nref, T.rects, T.nbox,
+                                              reinterpret_cast<int *>(tot));
+            if (!ck(cudaGetLastError(), "split")) break;
+            int h[4] = {0, 0, 0, 0};
+            if (!ck(cudaMemcpyAsync(h, tot, 16, cudaMemcpyDeviceToHost, st), "split result")) break;
+            if (!ck(cudaEventRecord(e1, st), "event")) break;
+            if (!ck(cudaEventSynchronize(e1), "build sync")) break;
+            if (h[2]) {
+                set_error("build_tree: too many levels");
+                rc = FRW_E_KERNEL;
+                break;
+            }
+            T.nodes = h[0];
+            T.depth = h[1];
+            T.bytes = (int64_t)n * 20 + (int64_t)T.nodes * 80;
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (build_ms) *build_ms = ms;
+            break;
+        }
         int32_t root[4] = {0, 0, 0, n};
         if (!ck(cudaMemcpyAsync(fa.node, &root[0], 4, cudaMemcpyHostToDevice, st), "root")) break;
         if (!ck(cudaMemcpyAsync(fa.level, &root[1], 4, cudaMemcpyHostToDevice, st), "root")) break;
         if (!ck(cudaMemcpyAsync(fa.start, &root[2], 4, cudaMemcpyHostToDevice, st), "root")) break;
         if (!ck(cudaMemcpyAsync(fa.end, &root[3], 4, cudaMemcpyHostToDevice, st), "root")) break;
-        // a layout of <= leaf_max rects still gets one internal root node
         int nodes = 1, nfr = 1, depth = 0;
         std::vector<int> batch = {0, 1};
-        if (n <= leaf_max) {
-            int4 r = make_int4(leaf_ref(0, n), kRefEmpty, kRefEmpty, kRefEmpty);
-            if (!ck(cudaMemcpyAsync(T.nref, &r, 16, cudaMemcpyHostToDevice, st), "root ref")) break;
-            nfr = 0;
-        }
         for (int iter = 0; nfr > 0; iter++) {
-            if (iter > 64) {
+            if (iter > kMaxLevels) {
                 set_error("build_tree: too many levels");
                 rc = FRW_E_KERNEL;
                 break;
