@@ -185,7 +185,11 @@ frw_status frw_cv_train(const frw_layout *layout, int64_t target, const frw_opts
         if (e == cudaSuccess) e = B.get(&d_step, 4);
         if (e != cudaSuccess) return fail(cuda_fail(e, "frw_cv_train: allocation"));
         cudaEventRecord(e0, st);
-        rc = walk_records(layout, target, 0, (uint64_t)N, co.train_seed, *walk_opts, st, d_end, d_rec);
+        // training walks start anywhere on the surface: a stratified start
+        // with more strata than training walks would cover only part of it
+        frw_opts train_opts = *walk_opts;
+        train_opts.start_strata = 0;
+        rc = walk_records(layout, target, 0, (uint64_t)N, co.train_seed, train_opts, st, d_end, d_rec);
         if (rc) return fail(rc);
         const double *r = v.rects + 4 * target;
         const double4 trect = make_double4(r[0], r[1], r[2], r[3]);
