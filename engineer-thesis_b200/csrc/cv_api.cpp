@@ -4,9 +4,10 @@
 // (features of the first-hop point, 1{walk ends on the target}, weight c^2);
 // the MLP is fitted on the device (fused forward+backward + Adam, the whole
 // loop captured once in a CUDA graph); then the exact mean E[c*phi] is summed
-// over the grid start x first-hop bins.  frw_cv_walk: walks + features +
-// inference + reduction, giving the plain and the control-variate estimate of
-// C_tt side by side from the same walks.
+// over the grid start x first-hop bins, keeping phi of every (arc, bin) in a
+// table.  frw_cv_walk: walks recording (end, weight factor, arc * 200 + bin),
+// phi looked up in the table, reduction -- the plain and the control-variate
+// estimate of C_tt side by side from the same walks.
 #include <math.h>
 #include <string.h>
 
