@@ -112,3 +112,31 @@ def test_layout_info_and_tree_shape():
         info = L.info
         assert info.n_rects == 50_000 and 0 < info.n_nodes < 50_000 and info.depth >= 4
         assert np.array_equal(L.rects(), rects.astype(np.float64))
+
+
+@pytest.mark.parametrize("n", [1, 2, 8, 9, 33, 65_536, 65_537])
+def test_tiny_and_threshold_layouts_match_oracle(n):
+    """Layouts around the tree builder's special sizes: a root leaf (n <= 8),
+    the first split, and both sides of the one-block build's 65,536-rect
+    limit; queries and walk records equal the oracle's."""
+    dom = max(200.0, float(np.sqrt(n)) * 100.0)
+    rects = frw.generate_layout(0xA11 + n, n, dom)
+    G = O.Grid(rects.astype(np.float64))
+    rng = np.random.default_rng(n)
+    with frw.Layout.from_rects(rects) as L:
+        b = L.bounds
+        pts = np.stack([rng.uniform(b[0], b[2], 4000), rng.uniform(b[1], b[3], 4000)], 1)
+        pts[:200] = rects[rng.integers(0, n, 200), :2]  # rect corners
+        sq, hit = L.query(pts)
+        o = frw.capacitance_opts(1.0)
+        end, hops, b1, w = L.walk_trace(0, 0, 2000, seed=9, o=o)
+        for cells in (0.0, 16.0):  # the tree alone, then with cell lists again
+            L.set_cells(cells)
+            sq2, hit2 = L.query(pts)
+            assert np.array_equal(sq2, sq) and np.array_equal(hit2, hit)
+    sq_o, hit_o = G.query_batch(pts)
+    assert np.array_equal(sq, sq_o) and np.array_equal(hit, hit_o)
+    cfg = G.walk_cfg(target=0, gauss_mode=o.gauss_mode, gauss_param=o.gauss_param, start_mode=o.start_mode, seed=9)
+    end_o, hops_o, b1_o, w_o = G.walks(cfg, 0, 2000)
+    assert np.array_equal(end, end_o) and np.array_equal(hops, hops_o)
+    assert np.array_equal(b1, b1_o) and np.array_equal(w, w_o)
