@@ -2,8 +2,8 @@
 //
 // frw_cv_train: walks from an independent seed give training pairs
 // (features of the first-hop point, 1{walk ends on the target}, weight c^2);
-// the MLP is fitted on the device (fused forward+backward + Adam, the whole
-// loop captured once in a CUDA graph); then the exact mean E[c*phi] is summed
+// the MLP is fitted on the device (fused forward+backward + Adam per step);
+// then the exact mean E[c*phi] is summed
 // over the grid start x first-hop bins, keeping phi of every (arc, bin) in a
 // table.  frw_cv_walk: walks recording (end, weight factor, arc * 200 + bin),
 // phi looked up in the table, reduction -- the plain and the control-variate
@@ -218,37 +218,19 @@ frw_status frw_cv_train(const frw_layout *layout, int64_t target, const frw_opts
         cudaMemsetAsync(d_v, 0, cv::kParams * 4, st);
         cudaMemsetAsync(d_loss, 0, (size_t)steps * 8, st);
         cudaMemsetAsync(d_step, 0, 4, st);
-        // the training loop, captured once and replayed as one graph
-        cudaStream_t cs;
-        e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
-        if (e != cudaSuccess) return fail(cuda_fail(e, "stream"));
-        cudaEvent_t ready;
-        cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
-        cudaEventRecord(ready, st);
-        cudaStreamWaitEvent(cs, ready, 0);
-        e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        // the training loop: a few hundred launches, enqueued directly (the
+        // host stays ahead of the device; instantiating a graph of them would
+        // cost more host time than it saves)
         const double scale = (double)N / wsum;  // per-batch normalisation of the weighted MSE
-        for (int s = 0; s < steps && e == cudaSuccess && !rc; s++) {
+        for (int s = 0; s < steps && !rc; s++) {
             const int64_t start = (int64_t)(s % steps_per_epoch) * co.batch;
             const int64_t rows = std::min<int64_t>(co.batch, N - start);
             const float inv = (float)(scale / (double)rows);
             rc = cv::launch_train_grad(M->net, d_x + 16 * start, d_y + start, d_wt + start, rows, inv, d_grad,
-                                       d_loss + s, cs);
-            if (!rc) rc = cv::launch_adam(M->net, d_grad, d_m, d_v, d_step, co.lr, cs);
+                                       d_loss + s, st);
+            if (!rc) rc = cv::launch_adam(M->net, d_grad, d_m, d_v, d_step, co.lr, st);
         }
-        cudaGraph_t graph = nullptr;
-        cudaError_t e2c = cudaStreamEndCapture(cs, &graph);
-        if (e == cudaSuccess) e = e2c;
-        cudaGraphExec_t exec = nullptr;
-        if (e == cudaSuccess && !rc) e = cudaGraphInstantiate(&exec, graph, 0);
-        if (e == cudaSuccess && !rc) e = cudaGraphLaunch(exec, cs);
-        if (e == cudaSuccess && !rc) e = cudaStreamSynchronize(cs);
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
-        cudaStreamDestroy(cs);
-        cudaEventDestroy(ready);
         if (rc) return fail(rc);
-        if (e != cudaSuccess) return fail(cuda_fail(e, "frw_cv_train: training graph"));
         cudaEventRecord(e1, st);
         std::vector<double> losses(steps);
         e = cudaMemcpyAsync(losses.data(), d_loss, (size_t)steps * 8, cudaMemcpyDeviceToHost, st);
