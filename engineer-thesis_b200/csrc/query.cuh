@@ -193,29 +193,49 @@ __device__ __forceinline__ bool collides_listed(const DevLayout &L, const Cands 
 // with the clearance d* settles every box farther than delta from d*: all
 // extents above d* means the nearest obstacle (bounds side or listed rect) is
 // touched; all below means nothing can be.  Only boxes within delta of d*
-// take the exact predicate.
-__device__ __forceinline__ bool collides_box(const DevLayout &L, const Cands &C, const double o[4], double px,
-                                             double dstar) {
-    const double e = __dsub_rn(o[2], px);
-    if (e > dstar + L.delta) return true;
-    if (e < dstar - L.delta) return false;
+// take the exact predicate.  The extent is compared as a coordinate: the x1
+// side against p.x + (d* +- delta), both rounded once per query -- a shift of
+// the window by an ulp of p.x, far inside the 32x margin of delta over eps.
+struct Window {
+    double hi, lo;  // x1 beyond hi: collides; below lo: free
+};
+
+__device__ __forceinline__ Window replay_window(const DevLayout &L, double px, double dstar) {
+    return Window{__dadd_rn(px, __dadd_rn(dstar, L.delta)), __dadd_rn(px, __dsub_rn(dstar, L.delta))};
+}
+
+__device__ __forceinline__ bool collides_box(const DevLayout &L, const Cands &C, const double o[4],
+                                             const Window &W) {
+    if (o[2] > W.hi) return true;
+    if (o[2] < W.lo) return false;
     return collides_listed(L, C, o);
 }
 
+// dist / 2 for the replay's step sizes (normal, positive, above MIN_DIST/2):
+// one less in the exponent field is exactly the correctly rounded half, so
+// the integer pipe does it.  A positive double's bit pattern orders like its
+// value, so the MIN_DIST test is an integer compare too.
+__device__ __forceinline__ double half_of(double d) {
+    return __longlong_as_double(__double_as_longlong(d) - 0x0010000000000000ll);
+}
+__device__ __forceinline__ bool above_min(double d) {
+    return __double_as_longlong(d) > __double_as_longlong(kMinDist);
+}
+
 // drawBiggestSquareAtPoint replayed on scalars: same operations, same order,
-// explicit round-to-nearest intrinsics (no contraction).  A halving x / 2 is
-// computed as x * 0.5: both are the exact real x/2 correctly rounded, so the
-// results are identical (subnormals included), without the division sequence.
+// explicit round-to-nearest intrinsics (no contraction); the halvings as
+// above.
 __device__ __forceinline__ uint32_t replay_square(const DevLayout &L, const Cands &C, double px,
                                                   double py, double dstar, double sq[4]) {
+    const Window W = replay_window(L, px, dstar);
     double o[4] = {__dsub_rn(px, 1.0), __dsub_rn(py, 1.0), __dadd_rn(px, 1.0), __dadd_rn(py, 1.0)};
-    if (collides_box(L, C, o, px, dstar)) {
+    if (collides_box(L, C, o, W)) {
         sq[0] = o[0]; sq[1] = o[1]; sq[2] = o[2]; sq[3] = o[3];
         return 0;
     }
     const double in2[4] = {__dsub_rn(px, 2.0), __dsub_rn(py, 2.0), __dadd_rn(px, 2.0),
                            __dadd_rn(py, 2.0)};
-    if (collides_box(L, C, in2, px, dstar)) {
+    if (collides_box(L, C, in2, W)) {
         sq[0] = in2[0]; sq[1] = in2[1]; sq[2] = in2[2]; sq[3] = in2[3];
         return 0;
     }
@@ -229,16 +249,16 @@ __device__ __forceinline__ uint32_t replay_square(const DevLayout &L, const Cand
     o[2] = __dadd_rn(o[2], dist);
     o[3] = __dadd_rn(o[3], dist);
     int it = 1;
-    while ((isc = collides_box(L, C, o, px, dstar)) || !maxReached || dist > kMinDist) {
+    while ((isc = collides_box(L, C, o, W)) || !maxReached || above_min(dist)) {
         if (isc) {
-            if (dist > kMinDist) dist = __dmul_rn(dist, 0.5);
+            if (above_min(dist)) dist = half_of(dist);
             maxReached = true;
             o[0] = __dadd_rn(o[0], dist);
             o[1] = __dadd_rn(o[1], dist);
             o[2] = __dsub_rn(o[2], dist);
             o[3] = __dsub_rn(o[3], dist);
         } else {
-            if (maxReached) dist = __dmul_rn(dist, 0.5);
+            if (maxReached) dist = half_of(dist);
             o[0] = __dsub_rn(o[0], dist);
             o[1] = __dsub_rn(o[1], dist);
             o[2] = __dadd_rn(o[2], dist);

@@ -233,3 +233,24 @@ def test_start_grid_needs_uniform_start():
     with frw.Layout.from_rects(config1_layout()) as L:
         with pytest.raises(frw.FrwError, match="start_grid"):
             L.walk(0, 1000, seed=1, o=frw.opts(start_grid=64))
+
+
+def test_full_size_c3_counts_and_signs():
+    """C3 at its full size (10^6 rects, 1e8 walks): every walk is accounted
+    for (hits + escapes + aborts), the self-capacitance is positive and no
+    coupling is significantly positive; a second run over the next 1e8 walk
+    indices agrees within the combined errors."""
+    rects = frw.generate_layout(0xF4A7 + 3, 10**6, 1e5)
+    n = 100_000_000
+    with frw.Layout.from_rects(rects) as L:
+        a = L.walk(0, n, seed=77, o=frw.capacitance_opts(1.0))
+        b = L.walk(0, n, seed=77, o=frw.capacitance_opts(1.0, first_walk=n))
+    for r in (a, b):
+        assert r.walks == n and int(r.hits.sum()) + r.escaped + r.aborted == n
+        i0 = np.searchsorted(r.conductor, 0)
+        assert r.conductor[i0] == 0 and r.cap[i0] > 0
+        others = np.delete(np.arange(len(r.conductor)), i0)
+        assert (r.cap[others] <= 5 * r.cap_se[others]).all()
+    ca, sa = a.row(0)[1:]
+    cb, sb = b.row(0)[1:]
+    assert abs(ca - cb) <= 5 * np.hypot(sa, sb)
