@@ -285,12 +285,19 @@ frw_status frw_batch_tune(frw_batch *B, uint64_t trial_walks, frw_tuning *chosen
     }
     WalkJob *d_tj = nullptr;
     FRW_CK(cudaMalloc(&d_tj, sizeof(WalkJob) * B->njobs));
+    struct Free {
+        void *p;
+        ~Free() { cudaFree(p); }
+    } free_tj{d_tj};
     FRW_CK(cudaMemcpy(d_tj, jobs.data(), sizeof(WalkJob) * B->njobs, cudaMemcpyHostToDevice));
     const uint64_t seed = 0x5EEDull;
     FRW_CK(cudaMemcpy(B->d_seed, &seed, 8, cudaMemcpyHostToDevice));
-    cudaEvent_t k0, k1;
-    cudaEventCreate(&k0);
-    cudaEventCreate(&k1);
+    Events ev(2);
+    if (!ev.ok(2)) {
+        set_error("frw_batch_tune: cudaEventCreate failed");
+        return FRW_E_CUDA;
+    }
+    cudaEvent_t k0 = ev[0], k1 = ev[1];
     const int maxb = std::max(1, walk_max_blocks_per_sm(256, true));
     const int refills[] = {1, 4, 16};
     const int chunks[] = {32, 128, 512};
@@ -316,9 +323,6 @@ frw_status frw_batch_tune(frw_batch *B, uint64_t trial_walks, frw_tuning *chosen
                     best.ms = ms;
                 }
             }
-    cudaEventDestroy(k0);
-    cudaEventDestroy(k1);
-    cudaFree(d_tj);
     if (rc) {
         if (rc == FRW_E_CUDA) set_error("frw_batch_tune: trial launch failed");
         return rc;
@@ -335,15 +339,16 @@ frw_status frw_batch_run(frw_batch *B, uint64_t seed, frw_result *results, void 
     }
     SetDev sd(B->device);
     cudaStream_t us = (cudaStream_t)stream;
-    cudaEvent_t ev;
-    FRW_CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    Events evs(3);
+    if (!evs.ok(3)) {
+        set_error("frw_batch_run: cudaEventCreate failed");
+        return FRW_E_CUDA;
+    }
+    cudaEvent_t ev = evs[0], t0 = evs[1], t1 = evs[2];
     // order after the caller's stream, run on the batch stream
     FRW_CK(cudaEventRecord(ev, us));
     FRW_CK(cudaStreamWaitEvent(B->cs, ev, 0));
     FRW_CK(cudaMemcpyAsync(B->d_seed, &seed, 8, cudaMemcpyHostToDevice, B->cs));
-    cudaEvent_t t0, t1;
-    cudaEventCreate(&t0);
-    cudaEventCreate(&t1);
     cudaEventRecord(t0, B->cs);
     FRW_CK(cudaGraphLaunch(B->exec, B->cs));
     cudaEventRecord(t1, B->cs);
@@ -368,9 +373,6 @@ frw_status frw_batch_run(frw_batch *B, uint64_t seed, frw_result *results, void 
     }
     float ms = 0.f;
     cudaEventElapsedTime(&ms, t0, t1);
-    cudaEventDestroy(t0);
-    cudaEventDestroy(t1);
-    cudaEventDestroy(ev);
     if (status) {
         set_error("frw_batch_run: a kernel reported an internal limit");
         return FRW_E_KERNEL;

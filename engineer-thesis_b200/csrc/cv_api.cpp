@@ -157,10 +157,9 @@ frw_status frw_cv_train(const frw_layout *layout, int64_t target, const frw_opts
         delete M;
         return r;
     };
-    cudaEvent_t e0, e1, e2;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaEventCreate(&e2);
+    Events ev(3);
+    if (!ev.ok(3)) return fail(cuda_fail(cudaErrorUnknown, "frw_cv_train: cudaEventCreate"));
+    cudaEvent_t e0 = ev[0], e1 = ev[1], e2 = ev[2];
     const int64_t N = (int64_t)co.train_walks;
     {
         Buf B(st);
@@ -291,9 +290,7 @@ frw_status frw_cv_train(const frw_layout *layout, int64_t target, const frw_opts
     cudaEventElapsedTime(&b, e1, e2);
     M->train_ms = a;
     M->quad_ms = b;
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    cudaEventDestroy(e2);
+
     *out = M;
     return FRW_OK;
 }
@@ -332,9 +329,9 @@ frw_status frw_cv_walk(const frw_cv *M, uint64_t walks, uint64_t seed, frw_cv_re
     if (e == cudaSuccess) e = B.get(&d_sums, 32);
     if (e != cudaSuccess) return cuda_fail(e, "frw_cv_walk: allocation");
     cudaMemsetAsync(d_sums, 0, 32, st);
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
+    Events ev(2);
+    if (!ev.ok(2)) return cuda_fail(cudaErrorUnknown, "frw_cv_walk: cudaEventCreate");
+    cudaEvent_t e0 = ev[0], e1 = ev[1];
     cudaEventRecord(e0, st);
     frw_status rc = FRW_OK;
     for (uint64_t first = 0; first < walks && !rc; first += chunk) {
@@ -351,8 +348,6 @@ frw_status frw_cv_walk(const frw_cv *M, uint64_t walks, uint64_t seed, frw_cv_re
     }
     float ms = 0;
     if (!rc) cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     if (rc) return rc;
     const double N = (double)walks;
     const double mz = h[0] / N, vz = std::max(h[1] / N - mz * mz, 0.0) * N / (N - 1);

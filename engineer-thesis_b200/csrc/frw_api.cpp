@@ -259,19 +259,12 @@ frw_status run_walks(const frw_layout *lay, int64_t target, uint64_t first_walk,
     const uint64_t need = (walks + threads - 1) / threads;
     if ((uint64_t)blocks > need) blocks = (int)std::max<uint64_t>(need, 1);
 
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    Events ev(out ? 2 : 0);
+    cudaEvent_t e0 = ev[0], e1 = ev[1];
     if (out) {
-        FRW_CK(cudaEventCreate(&e0));
-        FRW_CK(cudaEventCreate(&e1));
+        if (!ev.ok(2)) return cuda_fail(cudaErrorUnknown, "cudaEventCreate");
         FRW_CK(cudaEventRecord(e0, st));
     }
-    struct EvGuard {
-        cudaEvent_t a, b;
-        ~EvGuard() {
-            if (a) cudaEventDestroy(a);
-            if (b) cudaEventDestroy(b);
-        }
-    } evg{e0, e1};
     if (walks > 0) {
         rc = launch_walk(P, threads, blocks, st);
         if (rc) return rc;

@@ -114,6 +114,27 @@ struct WalkParams {
 void set_error(const std::string &msg);
 frw_status cuda_fail(cudaError_t e, const char *what);
 
+// CUDA events destroyed at scope exit, error paths included.
+struct Events {
+    cudaEvent_t e[4] = {nullptr, nullptr, nullptr, nullptr};
+    explicit Events(int n, unsigned flags = cudaEventDefault) {
+        for (int i = 0; i < n && i < 4; i++)
+            if (cudaEventCreateWithFlags(&e[i], flags) != cudaSuccess) e[i] = nullptr;
+    }
+    bool ok(int n) const {
+        for (int i = 0; i < n; i++)
+            if (!e[i]) return false;
+        return true;
+    }
+    cudaEvent_t operator[](int i) const { return e[i]; }
+    ~Events() {
+        for (cudaEvent_t x : e)
+            if (x) cudaEventDestroy(x);
+    }
+    Events(const Events &) = delete;
+    Events &operator=(const Events &) = delete;
+};
+
 #define FRW_CK(call)                                          \
     do {                                                      \
         cudaError_t e__ = (call);                             \
