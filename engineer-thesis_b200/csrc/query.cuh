@@ -316,6 +316,18 @@ __device__ __forceinline__ bool box_collides(const DevLayout &L, const double B[
     return false;
 }
 
+// x / 200 for an integer-valued x in [0, 2^31), correctly rounded without the
+// division sequence: q0 = x * RN(1/200), then one fused correction with the
+// exact residual x - q0 * 200 (Markstein's quotient refinement).  Checked
+// against IEEE division for every integer in the range.
+static_assert(FRW_NSAMPLE == 200, "div200 is for the 200-bin perimeter");
+__device__ __forceinline__ double div200(double x) {
+    constexpr double r = 1.0 / 200.0;
+    const double q0 = __dmul_rn(x, r);
+    const double res = __fma_rn(-q0, 200.0, x);
+    return __fma_rn(res, r, q0);
+}
+
 // RectHost::getPointFromNindex (CPU/rectHost.cpp:107-161; GPU twin
 // Cuda/d_Rect.cu:34-101): branch structure and operand order kept because
 // they decide ties; the perimeter is truncated to int unless `exact`.
@@ -323,7 +335,7 @@ __device__ __forceinline__ void point_from_index(const double s[4], int index, b
                                                  double &oy) {
     const double per2 = __dadd_rn(__dmul_rn(2.0, __dsub_rn(s[2], s[0])), __dmul_rn(2.0, __dsub_rn(s[3], s[1])));
     const double perim = exact ? per2 : (double)__double2int_rz(per2);
-    const double v = __ddiv_rn(perim, (double)FRW_NSAMPLE);
+    const double v = exact ? __ddiv_rn(perim, (double)FRW_NSAMPLE) : div200(perim);
     const double h = __dsub_rn(s[3], s[1]);
     const double w = __dsub_rn(s[2], s[0]);
     const double iv = __dmul_rn((double)index, v), jv = __dmul_rn((double)(index - 1), v);
