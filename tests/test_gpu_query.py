@@ -140,3 +140,30 @@ def test_tiny_and_threshold_layouts_match_oracle(n):
     end_o, hops_o, b1_o, w_o = G.walks(cfg, 0, 2000)
     assert np.array_equal(end, end_o) and np.array_equal(hops, hops_o)
     assert np.array_equal(b1, b1_o) and np.array_equal(w, w_o)
+
+
+def test_degenerate_and_equal_key_layouts_match_oracle():
+    """A layout of one point-sized rect (zero-area bounds), and 40 nested
+    rects sharing one centre (equal Morton keys: the tree splits them by
+    index); queries and walks equal the oracle's."""
+    cases = [
+        np.array([[50, 50, 50, 50]], dtype=np.float32),
+        np.array([[100 - k, 100 - k, 100 + k, 100 + k] for k in range(1, 41)], dtype=np.float32),
+    ]
+    rng = np.random.default_rng(4)
+    for rects in cases:
+        G = O.Grid(rects.astype(np.float64))
+        b = G.bounds
+        pts = np.stack([rng.uniform(b[0] - 1, b[2] + 1, 3000), rng.uniform(b[1] - 1, b[3] + 1, 3000)], 1)
+        pts[:40] = rects[: min(40, len(rects)), :2]
+        with frw.Layout.from_rects(rects) as L:
+            sq, hit = L.query(pts)
+            o = frw.capacitance_opts(1.0)
+            end, hops, b1, w = L.walk_trace(0, 0, 500, seed=3, o=o)
+        sq_o, hit_o = G.query_batch(pts)
+        assert np.array_equal(sq, sq_o) and np.array_equal(hit, hit_o)
+        cfg = G.walk_cfg(target=0, gauss_mode=o.gauss_mode, gauss_param=o.gauss_param, start_mode=o.start_mode,
+                         seed=3)
+        end_o, hops_o, b1_o, w_o = G.walks(cfg, 0, 500)
+        assert np.array_equal(end, end_o) and np.array_equal(hops, hops_o)
+        assert np.array_equal(b1, b1_o) and np.array_equal(w, w_o)
