@@ -2,9 +2,10 @@
 //
 // A batch is a job table (one job = layout, target conductor, walk count)
 // walked by ONE launch of the multi-job walk kernel: every warp lane picks
-// its next walk from a single global counter and finds the walk's job by
-// binary search over the jobs' first walk indices, so jobs of very uneven
-// size share the whole GPU without tail effects.  The device work of a run
+// its next walk from a single global counter and keeps its job while the
+// walk index stays inside the job's range (a binary search over the jobs'
+// first walk indices otherwise), so jobs of very uneven size share the whole
+// GPU without per-job tail effects.  The device work of a run
 // (clears, the Gaussian surfaces of all jobs, the walk launch and the row
 // compaction) is captured once into a CUDA graph; a run writes the seed into
 // device memory and replays the graph.  Launch parameters (resident blocks
