@@ -254,3 +254,20 @@ def test_full_size_c3_counts_and_signs():
     ca, sa = a.row(0)[1:]
     cb, sb = b.row(0)[1:]
     assert abs(ca - cb) <= 5 * np.hypot(sa, sb)
+
+
+def test_walk_argument_errors_and_empty_runs():
+    """Bad targets and options are rejected with FRW_E_ARG and a message; a run
+    of zero walks returns an empty row."""
+    with frw.Layout.from_rects(config1_layout()) as L:
+        for bad in (-1, L.n):
+            with pytest.raises(frw.FrwError, match="target"):
+                L.walk(bad, 1000, seed=1, o=frw.capacitance_opts(1.0))
+        o = frw.capacitance_opts(1.0)
+        o.struct_size = 8
+        with pytest.raises(frw.FrwError, match="struct_size"):
+            L.walk(0, 1000, seed=1, o=o)
+        with pytest.raises(frw.FrwError, match="hop_cap"):
+            L.walk(0, 1000, seed=1, o=frw.capacitance_opts(1.0, hop_cap=0))
+        r = L.walk(0, 0, seed=1, o=frw.capacitance_opts(1.0))
+        assert r.walks == 0 and len(r.conductor) == 0
