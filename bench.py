@@ -10,7 +10,8 @@ suite.  Under torchrun every rank runs its own 1e7 walks (Philox stream =
 rank; weak scaling) and the per-conductor rows are summed with one NCCL
 all-reduce inside the step.
 
-`value`  : walks/s with the layout resident in HBM (device events, max over ranks).
+`value`  : walks/s with the layout resident in HBM and the rows left on the
+           device (frw_walk_device; device events, max over ranks).
 `e2e`    : walks/s through the public C ABI from pinned host rects: layout
            upload + tree build + walks + result rows back, every step.
 `--impl reference`: the reference's own CPU walk (RandomWalk as shipped,
@@ -422,11 +423,25 @@ def main():
     L = frw.Layout.from_rects(rects, device=local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
 
-    def step(seed):
-        r = L.walk(W["target"], W["walks"], seed, o, stream=stream.cuda_stream)
-        if dist is not None:  # the one exchange: sum of the packed rows (NCCL)
-            shard.all_reduce_rows(torch.as_tensor(shard.result_rows(r, L.n), device=dev))
-        return r
+    # the step's rows stay on the device: hits | stats (int64) and sum_w | sum_w2
+    # (float64), cleared per step, summed over ranks by the one exchange
+    n = L.n
+    rows_i = torch.zeros(n + 4, dtype=torch.int64, device=dev)
+    rows_f = torch.zeros(2 * n, dtype=torch.float64, device=dev)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+
+    def step(seed, kev=None):
+        rows_i.zero_()
+        rows_f.zero_()
+        if kev:
+            kev[0].record(stream)
+        L.walk_device(W["target"], W["walks"], seed, o, rows_i[:n], rows_f[:n], rows_f[n:], rows_i[n:], status,
+                      stream.cuda_stream)
+        if kev:
+            kev[1].record(stream)
+        if dist is not None:  # the one exchange: the rows summed over ranks (NCCL)
+            dist.all_reduce(rows_i)
+            dist.all_reduce(rows_f)
 
     for i in range(args.warmup):
         step(1000 + i)
@@ -434,24 +449,27 @@ def main():
     if dist is not None:
         dist.barrier()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    kern_ms, hops, results = [], 0, []
+    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     with Clocks(local) as clk:
         for i in range(args.steps):
             flush.zero_()
             ev[i][0].record(stream)
-            r = step(i)
+            step(i, kev[i])
             ev[i][1].record(stream)
-            kern_ms.append(r.kernel_ms)
-            hops += r.hops_total
-            results.append(r)
         torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
+    if int(status.item()) != 0:
+        raise RuntimeError(f"walk kernel reported status {int(status.item()):#x}")
+    kern_ms = [a.elapsed_time(b) for a, b in kev]
     t_ms = sum(a.elapsed_time(b) for a, b in ev)
     if dist is not None:
         t = torch.tensor([t_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_ms = float(t.item())
+    last_i, last_f = rows_i.cpu().numpy(), rows_f.cpu().numpy()  # the last step, all ranks
+    stats = last_i[n:]
+    assert int(stats[3]) == W["walks"] * world, stats
     walks_total = W["walks"] * args.steps * world
     value = walks_total / (t_ms * 1e-3)
 
@@ -491,10 +509,11 @@ def main():
         batched = batched_run(frw, local, stream, 3)
 
     if rank == 0:
-        last = results[-1]
-        i0 = int(np.searchsorted(last.conductor, W["target"]))
-        rel_se = float(last.cap_se[i0] / abs(last.cap[i0]))
-        hbar = hops / (W["walks"] * args.steps)
+        nw = float(W["walks"] * world)
+        m1 = last_f[W["target"]] / nw
+        var = max(last_f[n + W["target"]] / nw - m1 * m1, 0.0) * nw / (nw - 1.0)
+        rel_se = float(np.sqrt(var / nw) / abs(m1))
+        hbar = float(stats[2]) / float(stats[3])
         bq = algorithmic_bytes_per_query(W["rects"])
         kms = statistics.median(kern_ms)
         achieved = W["walks"] * hbar * bq / (kms * 1e-3) / 1e9
@@ -510,11 +529,12 @@ def main():
             "e2e": {"value": W["walks"] / (e2e_ms * 1e-3), "unit": "walks/s",
                     "h2d_bytes_per_step": W["rects"] * 16 + 32,
                     "d2h_bytes_per_step": nrows * 32 + 64},
-            "gpu_launches": 3 * args.steps,
+            "gpu_launches": 2 * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "note": f"walk kernel; algorithmic {bq} B/query x {hbar:.2f} queries/walk; peak {peak_kind} "
-                                 "(the tree is L2-resident, so HBM is an upper-bound denominator)"},
+                         "note": f"walk kernel; algorithmic {bq} B/query (the tree query's bytes) x {hbar:.2f} "
+                                 f"queries/walk; peak {peak_kind} (cell lists and tree are L2-resident, so HBM is an "
+                                 "upper-bound denominator)"},
             "clocks": clk.summary(),
         }
         if queries:

@@ -752,6 +752,73 @@ frw_status frw_walk(const frw_layout *L, int64_t target, uint64_t walks, uint64_
     return FRW_OK;
 }
 
+frw_status frw_walk_device(const frw_layout *L, int64_t target, uint64_t walks, uint64_t seed, const frw_opts *opts,
+                           uint64_t *hits, double *sum_w, double *sum_w2, uint64_t *stats, uint32_t *status,
+                           void *stream) {
+    frw_opts o;
+    frw_opts_default(&o);
+    if (opts) o = *opts;
+    frw_status rc = validate_opts(&o);
+    if (rc) return rc;
+    if (!L || !hits || !sum_w || !sum_w2 || !stats || !status) {
+        set_error("frw_walk_device: null argument");
+        return FRW_E_ARG;
+    }
+    if (target < 0 || target >= L->n) {
+        set_error("target conductor index out of range");
+        return FRW_E_ARG;
+    }
+    DeviceGuard g(L->device);
+    DeviceCtx *ctx;
+    rc = device_ctx(L->device, &ctx);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    Scratch S(st);
+    char *blk;
+    FRW_CK(S.get(&blk, 64 + 32));  // counter, then the target rect (32 B) and its Gaussian surface
+    unsigned long long *d_counter = reinterpret_cast<unsigned long long *>(blk);
+    double4 *d_tgt = reinterpret_cast<double4 *>(blk + 32);
+    double4 *d_gauss = reinterpret_cast<double4 *>(blk + 64);
+    const double *r = L->rects.data() + 4 * target;
+    const double tg[4] = {r[0], r[1], r[2], r[3]};
+    FRW_CK(cudaMemsetAsync(d_counter, 0, 8, st));
+    FRW_CK(cudaMemcpyAsync(d_tgt, tg, sizeof(tg), cudaMemcpyHostToDevice, st));
+    rc = launch_gauss(L->dl, (const double *)d_tgt, 1, o.gauss_mode, o.gauss_param, (double *)d_gauss, status, st);
+    if (rc || walks == 0) return rc;
+    WalkParams P{};
+    P.job0.L = L->dl;
+    P.job0.target = target;
+    P.job0.walks = walks;
+    P.job0.first_walk = o.first_walk;
+    P.job0.stream_id = o.stream_id;
+    P.gauss = d_gauss;
+    P.njobs = 1;
+    P.start_mode = o.start_mode;
+    P.exact_perimeter = o.exact_perimeter;
+    P.refill_min = o.refill_min > 0 ? o.refill_min : 1;
+    P.start_grid = o.start_grid;
+    P.start_strata = o.start_strata;
+    P.hop_cap = o.hop_cap;
+    P.permittivity = o.permittivity;
+    P.seed = seed;
+    P.total_walks = walks;
+    P.counter = d_counter;
+    P.acc_n = reinterpret_cast<unsigned long long *>(hits);
+    P.acc_s = sum_w;
+    P.acc_s2 = sum_w2;
+    P.job_stats = reinterpret_cast<unsigned long long *>(stats);
+    P.status = status;
+    P.intg = ctx->tables;
+    P.wx = ctx->tables + FRW_NSAMPLE + 1;
+    P.wy = ctx->tables + 2 * FRW_NSAMPLE + 1;
+    if (!ctx->walk_bps) ctx->walk_bps = walk_max_blocks_per_sm(256, false);
+    int bps = o.blocks_per_sm > 0 ? o.blocks_per_sm : std::max(ctx->walk_bps, 1);
+    int blocks = ctx->sms * bps;
+    const uint64_t need = (walks + 255) / 256;
+    if ((uint64_t)blocks > need) blocks = (int)std::max<uint64_t>(need, 1);
+    return launch_walk(P, 256, blocks, st);
+}
+
 frw_status frw_walk_trace(const frw_layout *L, int64_t target, uint64_t first_walk, uint64_t walks, uint64_t seed,
                           const frw_opts *opts, int64_t *end, int32_t *hops, int32_t *bin1, double *weight,
                           int mem, void *stream) {

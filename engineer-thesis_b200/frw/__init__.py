@@ -180,6 +180,8 @@ _SIGS = {
     "frw_box_collides_batch": ([_VP, _VP, C.c_int64, _D, _VP, C.c_int, _VP], C.c_int),
     "frw_opts_default": ([C.POINTER(Opts)], None),
     "frw_walk": ([_VP, C.c_int64, C.c_uint64, C.c_uint64, C.POINTER(Opts), C.POINTER(Result), _VP], C.c_int),
+    "frw_walk_device": ([_VP, C.c_int64, C.c_uint64, C.c_uint64, C.POINTER(Opts), _VP, _VP, _VP, _VP, _VP, _VP],
+                        C.c_int),
     "frw_walk_trace": ([_VP, C.c_int64, C.c_uint64, C.c_uint64, C.c_uint64, C.POINTER(Opts), _VP, _VP, _VP,
                         _VP, C.c_int, _VP], C.c_int),
     "frw_gauss_surface": ([_VP, C.c_int64, C.POINTER(Opts), _D, _VP], C.c_int),
@@ -432,6 +434,15 @@ class Layout:
         m = min(r.n_entries, cap)
         return WalkResult(r.walks, r.escaped, r.aborted, r.hops_total, np.array(r.gauss[:]), r.fraction_other,
                           r.kernel_ms, cond[:m], hits[:m], c[:m], se[:m], s1[:m], s2[:m])
+
+    def walk_device(self, target: int, walks: int, seed: int, o: Opts | None, hits, sum_w, sum_w2, stats, status,
+                    stream: int = 0):
+        """frw_walk_device on torch CUDA tensors (uint64/float64 rows of n
+        entries, uint64 stats[4], int32 status[1]); stream-ordered, no sync."""
+        _check(lib().frw_walk_device(self._h, target, walks, seed, C.byref(o) if o else None,
+                                     C.c_void_p(hits.data_ptr()), C.c_void_p(sum_w.data_ptr()),
+                                     C.c_void_p(sum_w2.data_ptr()), C.c_void_p(stats.data_ptr()),
+                                     C.c_void_p(status.data_ptr()), stream or None))
 
     def cv_features(self, target: int, rec4) -> np.ndarray:
         q = np.ascontiguousarray(rec4, dtype=np.float64).reshape(-1, 4)

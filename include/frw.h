@@ -203,6 +203,20 @@ typedef struct frw_result {
 frw_status frw_walk(const frw_layout *layout, int64_t target, uint64_t walks, uint64_t seed,
                     const frw_opts *opts, frw_result *result, void *stream);
 
+/* The same walks accumulated into caller-owned DEVICE arrays, stream-ordered,
+ * without host synchronisation (the reference's randomWalkCudaWrapper,
+ * Cuda/mainkernels.h:9, leaves its outputs on the device the same way):
+ * for every conductor k (layer index, arrays of layout->n entries)
+ * hits[k] += walks ending on k, sum_w[k] += their weights, sum_w2[k] += the
+ * squared weights; stats[0..3] += escaped, aborted, hops, walks done;
+ * *status |= kernel limit bits (nonzero: see frw_walk's FRW_E_KERNEL).  The
+ * caller clears the arrays once; runs over disjoint walk ranges add up, and
+ * so do the arrays of several devices (one all-reduce).  Scratch comes from
+ * the device's stream-ordered memory pool. */
+frw_status frw_walk_device(const frw_layout *layout, int64_t target, uint64_t walks, uint64_t seed,
+                           const frw_opts *opts, uint64_t *hits, double *sum_w, double *sum_w2,
+                           uint64_t *stats, uint32_t *status, void *stream);
+
 /* Same walks with per-walk records (device or host arrays of `walks`
  * entries; any may be NULL): end conductor (layer index, -1 escaped,
  * -2 aborted), hop count, first-hop bin and the walk's capacitance weight

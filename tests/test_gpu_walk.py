@@ -271,3 +271,31 @@ def test_walk_argument_errors_and_empty_runs():
             L.walk(0, 1000, seed=1, o=frw.capacitance_opts(1.0, hop_cap=0))
         r = L.walk(0, 0, seed=1, o=frw.capacitance_opts(1.0))
         assert r.walks == 0 and len(r.conductor) == 0
+
+
+def test_walk_device_rows_match_frw_walk():
+    """frw_walk_device accumulates the same rows into device arrays without a
+    host sync: two runs over disjoint walk ranges equal one frw_walk run over
+    their union (hits exactly, sums to 1e-12), and the stats add up."""
+    import torch
+
+    rects = config1_layout()
+    n = 300_000
+    dev = torch.device("cuda", 0)
+    with frw.Layout.from_rects(rects) as L:
+        ref = L.walk(0, 2 * n, seed=31, o=frw.capacitance_opts(1.0))
+        hits = torch.zeros(L.n, dtype=torch.int64, device=dev)
+        s1 = torch.zeros(L.n, dtype=torch.float64, device=dev)
+        s2 = torch.zeros(L.n, dtype=torch.float64, device=dev)
+        stats = torch.zeros(4, dtype=torch.int64, device=dev)
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        for first in (0, n):
+            L.walk_device(0, n, 31, frw.capacitance_opts(1.0, first_walk=first), hits, s1, s2, stats, status)
+        torch.cuda.synchronize()
+    h, a, b, st = hits.cpu().numpy(), s1.cpu().numpy(), s2.cpu().numpy(), stats.cpu().numpy()
+    assert int(status.item()) == 0
+    assert st[3] == 2 * n and st[0] == ref.escaped and st[1] == ref.aborted and st[2] == ref.hops_total
+    k = np.flatnonzero(h)
+    assert np.array_equal(k, ref.conductor) and np.array_equal(h[k], ref.hits)
+    np.testing.assert_allclose(a[k], ref.sum_w, rtol=1e-12, atol=1e-12 * np.abs(ref.sum_w).max())
+    np.testing.assert_allclose(b[k], ref.sum_w2, rtol=1e-12, atol=1e-12 * np.abs(ref.sum_w2).max())
