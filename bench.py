@@ -129,6 +129,31 @@ def _ref_worker(args):
     return done, time.perf_counter() - t0
 
 
+def _port_worker(args):
+    rects, bounds, target, seconds, wid = args
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    G = O.Grid(rects, bounds)
+    cfg = G.walk_cfg(target=target, gauss_mode=O.GAUSS_OFFSET, gauss_param=1.0, start_mode=O.START_UNIFORM,
+                     seed=7, stream=wid)
+    done, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        G.walks(cfg, done, 2048)
+        done += 2048
+    return done, time.perf_counter() - t0
+
+
+def port_rate(rects, bounds, target, seconds, cores):
+    """Walks/s of the FP64 CPU restatement (the oracle, uniform grid index,
+    the benchmark's own offset-1 surface and capacitance weights) on `cores`
+    processes."""
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        res = pool.map(_port_worker, [(rects, bounds, target, seconds, i) for i in range(cores)])
+    return sum(d for d, _ in res) / max(t for _, t in res), sum(d for d, _ in res)
+
+
 def reference_rate(rects, bounds, target, seconds, cores, mode="shipped"):
     """Walks/s of the reference CPU walk on `cores` processes."""
     ctx = mp.get_context("spawn")
@@ -408,6 +433,7 @@ def main():
         rb = rects.astype(np.float64), O.layer_bounds(rects.astype(np.float64))
         rate, n = reference_rate(*rb, W["target"], args.cpu_seconds, cores)
         rate1, n1 = reference_rate(*rb, W["target"], args.cpu_seconds / 2, cores, mode="seeded")
+        rate2, n2 = port_rate(*rb, W["target"], args.cpu_seconds / 4, cores)
         cpu = {"value": rate, "unit": "walks/s", "cores": cores, "kind": "reference",
                "sample": f"reference RandomWalk as shipped (per-walk rng_init, reference scale-1.5 surface and "
                          f"Green-CDF start) on the same layout and target, {args.cpu_seconds:.0f}s on {cores} "
@@ -415,7 +441,11 @@ def main():
                "per_core": rate / cores,
                "seeded_once": {"value": rate1, "per_core": rate1 / cores,
                                "sample": f"the same walk loop with JKISS seeded once per 64 walks, "
-                                         f"{args.cpu_seconds / 2:.0f}s on {cores} processes, {n1} walks"}}
+                                         f"{args.cpu_seconds / 2:.0f}s on {cores} processes, {n1} walks"},
+               "port": {"value": rate2, "per_core": rate2 / cores,
+                        "sample": f"the FP64 CPU restatement (oracle/, uniform grid index, offset-1 surface, "
+                                  f"capacitance weights), {args.cpu_seconds / 4:.1f}s on {cores} processes, "
+                                  f"{n2} walks"}}
 
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
