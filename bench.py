@@ -16,6 +16,9 @@ all-reduce inside the step.
            upload + tree build + walks + result rows back, every step.
 `--impl reference`: the reference's own CPU walk (RandomWalk as shipped,
            compiled from its sources into oracle/_ref) on all host cores.
+`walk3d` : the 3-D walk over box conductors with the reference's unit-cube
+           Green's function (10^4 boxes, 1e7 walks per step), its clearance
+           queries, its e2e rate and its CPU restatement's rate.
 """
 from __future__ import annotations
 
@@ -340,6 +343,91 @@ def c3_run(frw, device, stream, steps):
             "cell_build_ms": L_cells_ms}
 
 
+# ------------------------------------------------------------ 3-D path
+W3D = dict(workload="frw3-1e4-boxes-1e7-walks", boxes=10_000, domain=2000.0, zdomain=400.0, edges="5-50 (z 5-20)",
+           gap=2, walks=10_000_000, target=0, gauss_offset=1.0, nsample=50, layout_seed=0xF4A7 + 6)
+
+
+def _port3_worker(args):
+    boxes, target, seconds, wid = args
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    B = O.Boxes3(boxes, grid=True)
+    cfg = B.cfg(target=target, offset=W3D["gauss_offset"], seed=11, stream=wid, nsample=W3D["nsample"])
+    done, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        B.walks(cfg, done, 512)
+        done += 512
+    return done, time.perf_counter() - t0
+
+
+def walk3d_run(frw, device, stream, steps, cpu_seconds, cores):
+    """The 3-D walk (box conductors, cube transition domains from the
+    reference's unit-cube Green's function): 10^4 boxes, 1e7 walks per step,
+    capacitance row of box 0.  Per-walk records equal the FP64 oracle's
+    (GPU tests); e2e includes the box upload and grid build every step."""
+    import torch
+
+    b = frw.generate_layout3(W3D["layout_seed"], W3D["boxes"], W3D["domain"], W3D["zdomain"], 5, 50, 5, 20,
+                             W3D["gap"])
+    o = frw.opts3(gauss_offset=W3D["gauss_offset"], nsample=W3D["nsample"])
+    L = frw.Layout3.from_boxes(b, device=device)
+    L.walk(W3D["target"], 1_000_000, 1, o, stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    res = [L.walk(W3D["target"], W3D["walks"], 300 + k, o, stream=stream.cuda_stream) for k in range(steps)]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    kms = statistics.median(r.kernel_ms for r in res)
+    r = res[-1]
+    c, se = r.row(W3D["target"])[1:]
+    info = L.info
+    # clearance queries, 1e7 uniform points (inputs + outputs 400 MB, larger than L2)
+    rng = np.random.default_rng(0x3D)
+    bd = L.bounds
+    pts = torch.as_tensor(bd[:3] + rng.random((10_000_000, 3)) * (bd[3:] - bd[:3]), device=device)
+    d = torch.empty(len(pts), dtype=torch.float64, device=device)
+    k = torch.empty(len(pts), dtype=torch.int64, device=device)
+    L.query_device(pts, d, k, stream.cuda_stream)
+    e0.record(stream)
+    for _ in range(5):
+        L.query_device(pts, d, k, stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    qms = e0.elapsed_time(e1) / 5
+    del pts, d, k
+    L.close()
+    # end to end: boxes from the host, grid build, walks, rows back, every step
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(steps):
+        with frw.Layout3.from_boxes(b, device=device) as Le:
+            Le.walk(W3D["target"], W3D["walks"], 500 + i, o, stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / steps
+    out = {"workload": W3D["workload"], "config": W3D, "ms_per_step": ms, "walks_per_s": W3D["walks"] / (ms * 1e-3),
+           "kernel_ms": kms, "kernel_walks_per_s": W3D["walks"] / (kms * 1e-3),
+           "hops_per_s": r.hops_total / (kms * 1e-3), "mean_hops": r.hops_total / W3D["walks"],
+           "escaped": int(r.escaped), "c00": c, "c00_rel_se": se / abs(c), "conductors_reached": int(len(r.conductor)),
+           "grid": list(info.grid), "grid_build_ms": info.build_ms, "mean_list": info.mean_list,
+           "max_list": info.max_list,
+           "queries_1e7": {"ms": qms, "queries_per_s": 1e7 / (qms * 1e-3)},
+           "e2e": {"value": W3D["walks"] / e2e_s, "unit": "walks/s", "h2d_bytes_per_step": W3D["boxes"] * 24,
+                   "d2h_bytes_per_step": (5 + 3 * W3D["boxes"]) * 8}}
+    if cpu_seconds > 0 and cores > 0:
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(cores) as pool:
+            rs = pool.map(_port3_worker, [(b, W3D["target"], cpu_seconds, i) for i in range(cores)])
+        done = sum(x for x, _ in rs)
+        out["cpu_port"] = {"value": done / max(t for _, t in rs), "unit": "walks/s", "cores": cores, "kind": "port",
+                           "sample": f"the FP64 CPU restatement of the 3-D walk (oracle/frwcpu3d.c, cell grid), "
+                                     f"{cpu_seconds:g}s on {cores} processes, {done} walks"}
+    return out
+
+
 # ------------------------------------------------------------ batched config
 BATCHED = dict(workload="frw-c4-256-layouts-1e8-walks", layouts=256, min_rects=100, max_rects=100_000,
                total_walks=100_000_000, layout_seed=0x0C4, tune_walks=5_000_000)
@@ -399,6 +487,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-headline", action="store_true", help="skip the time-to-0.1%% plain vs CV runs")
     ap.add_argument("--no-batched", action="store_true", help="skip the 256-layout batched runs")
+    ap.add_argument("--no-3d", action="store_true", help="skip the 3-D walk runs")
     args = ap.parse_args()
     if args.walks:
         WORKLOAD["walks"] = args.walks
@@ -537,6 +626,10 @@ def main():
         headline = time_to_rel_se(frw, local, stream)
     if rank == 0 and world == 1 and not args.no_batched:
         batched = batched_run(frw, local, stream, 3)
+    walk3d = None
+    if rank == 0 and world == 1 and not args.no_3d:
+        walk3d = walk3d_run(frw, local, stream, 3, 0.0 if args.no_cpu_baseline else 2.0,
+                            min(os.cpu_count() or 1, 16))
 
     if rank == 0:
         nw = float(W["walks"] * world)
@@ -575,6 +668,8 @@ def main():
             out["time_to_0.1pct_rel_se"] = headline
         if batched:
             out["batched"] = batched
+        if walk3d:
+            out["walk3d"] = walk3d
         if cpu:
             out["cpu_baseline"] = cpu
         print(json.dumps(out))

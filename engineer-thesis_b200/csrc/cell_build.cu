@@ -312,4 +312,13 @@ frw_status build_cells(const DevLayout &Lin, double cells_per_rect, int cap, cud
     return FRW_OK;
 }
 
+int64_t scan_i64_tiles(int64_t n) { return (n + kScanTile - 1) / kScanTile; }
+
+void launch_scan_i64(const int64_t *in, int64_t n, int64_t *out, int64_t *sums, int64_t *grand, cudaStream_t st) {
+    const int64_t tiles = scan_i64_tiles(n);
+    k_tile_sums<<<(unsigned)tiles, kScanThreads, 0, st>>>(in, n, sums);
+    k_scan_sums<<<1, kScanThreads, 0, st>>>(sums, tiles, grand);
+    k_tile_scan<<<(unsigned)tiles, kScanThreads, 0, st>>>(in, n, sums, out);
+}
+
 }  // namespace frw

@@ -1,0 +1,101 @@
+// frw3d_internal.h -- declarations of the 3-D walk path (host + device).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/frw3d.h"
+#include "frw_internal.h"
+
+namespace frw {
+
+// ---- cell grid in HBM ----------------------------------------------------------
+// Cubic cells of side s over the bounds.  Cell c lists every box whose
+// L-infinity distance from the cell centre is at most D_c + 2 h + margin
+// (D_c = distance from the centre to its nearest box, h = s/2): the nearest
+// box of any point of the cell is among them.  Entries are copies of the
+// boxes, two float4 each: (x0, y0, z0, id bits) and (x1, y1, z1, 0), so a
+// query reads one 8-byte cell record and 32 bytes per candidate.
+struct Dev3Layout {
+    const uint2 *cells;    // [ncells] (first entry, entry count)
+    const float4 *lists;   // [2 * entries]
+    double g0x, g0y, g0z;  // grid origin
+    double ginv;           // 1 / cell side
+    int nx, ny, nz;
+    double b[6];           // bounds (x0,y0,z0,x1,y1,z1), open
+};
+
+struct Grid3Buffers {
+    uint2 *cells = nullptr;
+    float4 *lists = nullptr;
+    int64_t ncells = 0, entries = 0;
+    int nx = 0, ny = 0, nz = 0;
+    double g0[3] = {0, 0, 0};
+    double side = 0;
+    int32_t max_list = 0;
+    float build_ms = 0;
+};
+
+// Device copy of the cube table for one resolution n: CDF thresholds as
+// 32-bit integers (bin b is chosen for a Philox word x iff thr[b] <= x <
+// thr[b+1], thr[b] = ceil(intg[b] * 2^32) -- the same bin as comparing
+// x * 2^-32 with intg in FP64), a guide over the top 14 bits of x, the
+// first-hop weight vectors and the landing offsets (2 i + 1 - n) / n.
+constexpr int kGuide3Bits = 14;
+struct Cube3Tables {
+    int n = 0, nb = 0;
+    uint32_t *thr = nullptr;    // [nb]
+    uint16_t *guide = nullptr;  // [1 << kGuide3Bits]
+    double *w = nullptr;        // [3 nb]
+    double *offs = nullptr;     // [n]
+};
+
+struct Walk3Params {
+    Dev3Layout L;
+    const uint32_t *thr;
+    const uint16_t *guide;
+    const double *w;
+    const double *offs;
+    int n, nb;
+    double G[6];  // Gaussian box
+    double S;     // its area
+    int64_t target;
+    double shell;
+    int64_t hop_cap;
+    double perm;
+    uint64_t seed;
+    uint32_t stream;
+    uint64_t first, walks;
+    unsigned long long *counter;  // walks claimed (cleared by the caller)
+    // rows (capacitance mode): per box, plus stats[4] = escaped, aborted, hops, walks
+    unsigned long long *hits;
+    double *sum_w, *sum_w2;
+    unsigned long long *stats;
+    // records (trace mode), indexed by walk - first
+    int64_t *rec_end;
+    int32_t *rec_hops, *rec_bin;
+    double *rec_w;
+};
+
+// host_cube_green.cpp
+// Cube table of resolution n (6 n^2 bins), bit-identical to the reference's
+// precompute_unit_cube_green; computed once per n and cached.  Any output
+// may be NULL.  Returns false for n outside [1, FRW3_NSAMPLE_MAX].
+bool cube_green_table(int n, double *g, double *dgdx, double *dgdy, double *dgdz, double *intg);
+double cube_green_point(double a, double eta, double dzeta);
+void cube_deriv_point(double *dg, double a, double eta, double dzeta);
+// Host images of the device tables (thresholds, guide, weights, offsets).
+bool cube_walk_tables(int n, uint32_t *thr, uint16_t *guide, double *w, double *offs);
+
+// walk3d.cu
+frw_status build_grid3(const float *d_boxes, int64_t n, const double bounds[6], double cells_per_box,
+                       cudaStream_t stream, Grid3Buffers *out);
+void free_grid3(Grid3Buffers *g, cudaStream_t stream);
+void attach_grid3(Dev3Layout &L, const Grid3Buffers &g, const double bounds[6]);
+frw_status launch_query3(const Dev3Layout &L, const double *d_pts, int64_t n, double *d_clear,
+                         int64_t *d_nearest, cudaStream_t stream);
+frw_status launch_walk3(const Walk3Params &P, int blocks, cudaStream_t stream);
+int walk3_max_blocks_per_sm();
+int walk3_threads();
+
+}  // namespace frw

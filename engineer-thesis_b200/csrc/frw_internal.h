@@ -176,6 +176,10 @@ constexpr int64_t kMaxCells = 1ll << 26;
 frw_status build_cells(const DevLayout &L, double cells_per_rect, int max_per_cell, cudaStream_t stream,
                        CellBuffers *out);
 void free_cells(CellBuffers *c, cudaStream_t stream);
+// Exclusive scan of n int64 values into out (in and out must not alias);
+// sums holds scan_i64_tiles(n) tile totals, *grand receives the total.
+int64_t scan_i64_tiles(int64_t n);
+void launch_scan_i64(const int64_t *in, int64_t n, int64_t *out, int64_t *sums, int64_t *grand, cudaStream_t stream);
 void attach_cells(DevLayout &L, const CellBuffers &c);
 
 // query.cu

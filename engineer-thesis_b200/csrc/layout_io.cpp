@@ -157,6 +157,69 @@ frw_status generate_layout(uint64_t seed, int64_t n, double domain, int wmin, in
     return FRW_OK;
 }
 
+// The 3-D variant: integer corners uniform in [0, D)^2 x [0, Dz), edges
+// uniform in [wmin, wmax] (z: [zmin, zmax]), accepted when the L-infinity gap
+// to every accepted box is at least `gap` (a hash grid of cubes of side
+// max edge + gap + 1 finds the neighbours).
+frw_status generate_layout3(uint64_t seed, int64_t n, double domain, double zdomain, int wmin, int wmax, int zmin,
+                            int zmax, double gap, float *out) {
+    if (n <= 0 || n > INT32_MAX || wmin < 1 || wmax < wmin || zmin < 1 || zmax < zmin || domain < wmax ||
+        zdomain < zmax || gap < 0 || domain >= 16777216.0 || zdomain >= 16777216.0) {
+        set_error("frw3_generate_layout: bad arguments");
+        return FRW_E_ARG;
+    }
+    const int64_t D = (int64_t)floor(domain), Dz = (int64_t)floor(zdomain);
+    const int64_t emax = std::max(wmax, zmax);
+    const double cs = emax + ceil(gap) + 1.0;
+    const int64_t nc = (int64_t)(D / cs) + 1, ncz = (int64_t)(Dz / cs) + 1;
+    if (nc * nc * ncz > (1ll << 26)) {
+        set_error("frw3_generate_layout: domain too large for the rejection grid");
+        return FRW_E_ARG;
+    }
+    std::vector<int32_t> head((size_t)(nc * nc * ncz), -1), link((size_t)n, -1);
+    SplitMix rng{seed};
+    int64_t got = 0, tries = 0;
+    while (got < n) {
+        if (++tries > 64 * n + 1000) {
+            set_error("frw3_generate_layout: domain too crowded for the requested count");
+            return FRW_E_ARG;
+        }
+        const int64_t w = rng.range(wmin, wmax), h = rng.range(wmin, wmax), d = rng.range(zmin, zmax);
+        const int64_t x0 = rng.range(0, D - w), y0 = rng.range(0, D - h), z0 = rng.range(0, Dz - d);
+        const int64_t lo[3] = {x0, y0, z0}, hi[3] = {x0 + w, y0 + h, z0 + d}, ncs[3] = {nc, nc, ncz};
+        int64_t c0[3], c1[3];
+        for (int c = 0; c < 3; c++) {
+            c0[c] = std::max<int64_t>(0, (int64_t)((lo[c] - emax - gap) / cs) - 1);
+            c1[c] = std::min<int64_t>(ncs[c] - 1, (int64_t)((hi[c] + gap) / cs) + 1);
+        }
+        bool ok = true;
+        for (int64_t cz = c0[2]; cz <= c1[2] && ok; cz++)
+            for (int64_t cy = c0[1]; cy <= c1[1] && ok; cy++)
+                for (int64_t cx = c0[0]; cx <= c1[0] && ok; cx++)
+                    for (int32_t j = head[(size_t)((cz * nc + cy) * nc + cx)]; j >= 0; j = link[(size_t)j]) {
+                        const float *q = out + 6 * (int64_t)j;
+                        double g = -INFINITY;
+                        for (int c = 0; c < 3; c++)
+                            g = std::max(g, std::max(q[c] - (double)hi[c], (double)lo[c] - q[3 + c]));
+                        if (g < gap) {
+                            ok = false;
+                            break;
+                        }
+                    }
+        if (!ok) continue;
+        float *o = out + 6 * got;
+        for (int c = 0; c < 3; c++) {
+            o[c] = (float)lo[c];
+            o[3 + c] = (float)hi[c];
+        }
+        const size_t cell = (size_t)(((int64_t)(z0 / cs) * nc + (int64_t)(y0 / cs)) * nc + (int64_t)(x0 / cs));
+        link[(size_t)got] = head[cell];
+        head[cell] = (int32_t)got;
+        got++;
+    }
+    return FRW_OK;
+}
+
 frw_status write_layout(const char *path, const float *r, int64_t n, const char *name) {
     FILE *f = fopen(path, "w");
     if (!f) {

@@ -1,0 +1,608 @@
+// walk3d.cu -- 3-D floating random walk on box conductors: cell-grid build,
+// clearance queries and the persistent walk kernel.
+//
+// The reference has no 3-D walk (its cube Green's function, green/green.cpp:
+// 232-431, is never called); this is its 2-D walk (CPU/mainFunctions.cpp:
+// 48-90) lifted to cubes, written for B200 the way the 2-D kernels are:
+//   * the clearance query reads one cell record and a short list of box
+//     copies (32 bytes each) -- no tree descent and no stack;
+//   * the cell lists are built on the device: boxes binned by overlap
+//     (count -> scan -> fill), then for every cell a ring search for the
+//     nearest box to its centre and a count -> scan -> fill of the boxes
+//     within that distance plus a cell diagonal;
+//   * the walk kernel is persistent (SM count x resident blocks); a warp
+//     claims walks in chunks from one global counter and refills each idle
+//     lane before every hop, so lanes stay busy while walks of very different
+//     lengths finish;
+//   * random numbers are Philox4x32-10 words keyed by (seed) with counter
+//     (t / 4, walk, stream): the trajectory of a walk depends only on its
+//     index, so the CPU oracle replays every walk bit for bit;
+//   * the landing bin comes from a 2^14-entry guide in shared memory and the
+//     32-bit CDF thresholds (L1-resident) -- one or two compares;
+//   * FP64 geometry with explicitly rounded operations (no contraction):
+//     exactly the oracle's arithmetic.
+#include <math.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "frw3d_internal.h"
+
+namespace frw {
+namespace {
+
+constexpr int kW3Threads = 256;
+constexpr int kW3MinBlocks = 4;
+constexpr unsigned kFull = 0xFFFFFFFFu;
+constexpr uint64_t kW3Chunk = 128;  // walks a warp claims at a time
+constexpr int64_t kMaxCells3 = int64_t(1) << 26;
+constexpr int kMaxAxisCells3 = 1 << 14;
+
+// ---- grid ------------------------------------------------------------------
+struct Grid3 {
+    double o[3];   // origin
+    double side, inv, h, margin;
+    int n[3];
+};
+
+__device__ __forceinline__ int cell_axis(double v, double o, double inv, int n) {
+    const double t = floor(__dmul_rn(__dsub_rn(v, o), inv));
+    if (!(t >= 0.0)) return 0;
+    if (t >= (double)n) return n - 1;
+    return (int)t;
+}
+
+// L-infinity distance from p to the box (x0,y0,z0,x1,y1,z1): the largest
+// per-axis gap, 0 inside.
+__device__ __forceinline__ double box_dist(double px, double py, double pz, float4 lo, float4 hi) {
+    double d = 0.0;
+    d = fmax(d, __dsub_rn((double)lo.x, px));
+    d = fmax(d, __dsub_rn(px, (double)hi.x));
+    d = fmax(d, __dsub_rn((double)lo.y, py));
+    d = fmax(d, __dsub_rn(py, (double)hi.y));
+    d = fmax(d, __dsub_rn((double)lo.z, pz));
+    d = fmax(d, __dsub_rn(pz, (double)hi.z));
+    return d;
+}
+
+__device__ __forceinline__ void load_box(const float *__restrict__ boxes, int64_t i, float4 &lo, float4 &hi) {
+    const float *b = boxes + 6 * i;
+    lo = make_float4(__ldg(b), __ldg(b + 1), __ldg(b + 2), __int_as_float((int)i));
+    hi = make_float4(__ldg(b + 3), __ldg(b + 4), __ldg(b + 5), 0.0f);
+}
+
+__global__ void k3_bin_count(const float *__restrict__ boxes, int64_t n, Grid3 G,
+                             unsigned long long *__restrict__ cnt) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float *b = boxes + 6 * i;
+    int lo[3], hi[3];
+    for (int c = 0; c < 3; c++) {
+        lo[c] = cell_axis((double)b[c], G.o[c], G.inv, G.n[c]);
+        hi[c] = cell_axis((double)b[3 + c], G.o[c], G.inv, G.n[c]);
+    }
+    for (int z = lo[2]; z <= hi[2]; z++)
+        for (int y = lo[1]; y <= hi[1]; y++)
+            for (int x = lo[0]; x <= hi[0]; x++)
+                atomicAdd(cnt + ((int64_t)z * G.n[1] + y) * G.n[0] + x, 1ull);
+}
+
+__global__ void k3_bin_fill(const float *__restrict__ boxes, int64_t n, Grid3 G,
+                            unsigned long long *__restrict__ cursor, int32_t *__restrict__ items) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float *b = boxes + 6 * i;
+    int lo[3], hi[3];
+    for (int c = 0; c < 3; c++) {
+        lo[c] = cell_axis((double)b[c], G.o[c], G.inv, G.n[c]);
+        hi[c] = cell_axis((double)b[3 + c], G.o[c], G.inv, G.n[c]);
+    }
+    for (int z = lo[2]; z <= hi[2]; z++)
+        for (int y = lo[1]; y <= hi[1]; y++)
+            for (int x = lo[0]; x <= hi[0]; x++)
+                items[atomicAdd(cursor + ((int64_t)z * G.n[1] + y) * G.n[0] + x, 1ull)] = (int32_t)i;
+}
+
+// Visits the cells of Chebyshev ring r around (cx, cy, cz) inside the grid:
+// the full x range on the ring's z and y faces, else its two x ends.
+template <class F>
+__device__ __forceinline__ void for_ring(const Grid3 &G, int cx, int cy, int cz, int r, F &&f) {
+    const int z0 = max(cz - r, 0), z1 = min(cz + r, G.n[2] - 1);
+    const int y0 = max(cy - r, 0), y1 = min(cy + r, G.n[1] - 1);
+    const int x0 = max(cx - r, 0), x1 = min(cx + r, G.n[0] - 1);
+    for (int z = z0; z <= z1; z++)
+        for (int y = y0; y <= y1; y++) {
+            const int64_t row = ((int64_t)z * G.n[1] + y) * G.n[0];
+            if (z == cz - r || z == cz + r || y == cy - r || y == cy + r) {
+                for (int x = x0; x <= x1; x++) f(row + x);
+            } else {
+                if (cx - r >= 0) f(row + cx - r);
+                if (r > 0 && cx + r < G.n[0]) f(row + cx + r);
+            }
+        }
+}
+
+// Per cell: the nearest-box distance D of its centre (ring search over the
+// bins: boxes in ring r are at least (2r - 1) h away), then every box within
+// R = D + 2h + margin, each counted once (in the first cell, in index order,
+// where its cell range meets the search cube) -- counted (kFill = false) or
+// written (kFill = true).
+template <bool kFill>
+__global__ void k3_cell_lists(const float *__restrict__ boxes, Grid3 G, const int64_t *__restrict__ bstart,
+                              const int32_t *__restrict__ items, int64_t ncells, int64_t *__restrict__ cnt,
+                              const int64_t *__restrict__ lstart, float4 *__restrict__ lists) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncells) return;
+    const int cx = (int)(c % G.n[0]), cy = (int)((c / G.n[0]) % G.n[1]), cz = (int)(c / ((int64_t)G.n[0] * G.n[1]));
+    const double px = __dadd_rn(G.o[0], __dmul_rn((double)cx + 0.5, G.side));
+    const double py = __dadd_rn(G.o[1], __dmul_rn((double)cy + 0.5, G.side));
+    const double pz = __dadd_rn(G.o[2], __dmul_rn((double)cz + 0.5, G.side));
+    const int rlim = max(G.n[0], max(G.n[1], G.n[2]));
+    double best = INFINITY;
+    for (int r = 0; r <= rlim; r++) {
+        if (r > 0 && __dmul_rn((double)(2 * r - 1), G.h) > __dadd_rn(best, G.margin)) break;
+        for_ring(G, cx, cy, cz, r, [&](int64_t q) {
+            for (int64_t k = bstart[q]; k < bstart[q + 1]; k++) {
+                float4 lo, hi;
+                load_box(boxes, items[k], lo, hi);
+                best = fmin(best, box_dist(px, py, pz, lo, hi));
+            }
+        });
+    }
+    const double R = __dadd_rn(__dadd_rn(best, __dmul_rn(2.0, G.h)), G.margin);
+    int rmax = 0;
+    while (rmax < rlim && __dmul_rn((double)(2 * rmax + 1), G.h) <= R) rmax++;
+    const int s0[3] = {max(cx - rmax, 0), max(cy - rmax, 0), max(cz - rmax, 0)};
+    const int s1[3] = {min(cx + rmax, G.n[0] - 1), min(cy + rmax, G.n[1] - 1), min(cz + rmax, G.n[2] - 1)};
+    int64_t m = 0, out = kFill ? lstart[c] : 0;
+    for (int z = s0[2]; z <= s1[2]; z++)
+        for (int y = s0[1]; y <= s1[1]; y++)
+            for (int x = s0[0]; x <= s1[0]; x++) {
+                const int64_t q = ((int64_t)z * G.n[1] + y) * G.n[0] + x;
+                for (int64_t k = bstart[q]; k < bstart[q + 1]; k++) {
+                    const int32_t i = items[k];
+                    float4 lo, hi;
+                    load_box(boxes, i, lo, hi);
+                    // the box's first cell inside the search cube
+                    const int fx = max(cell_axis((double)lo.x, G.o[0], G.inv, G.n[0]), s0[0]);
+                    const int fy = max(cell_axis((double)lo.y, G.o[1], G.inv, G.n[1]), s0[1]);
+                    const int fz = max(cell_axis((double)lo.z, G.o[2], G.inv, G.n[2]), s0[2]);
+                    if (fx != x || fy != y || fz != z) continue;
+                    if (box_dist(px, py, pz, lo, hi) > R) continue;
+                    if (kFill) {
+                        lists[2 * (out + m)] = lo;
+                        lists[2 * (out + m) + 1] = hi;
+                    }
+                    m++;
+                }
+            }
+    if (!kFill) cnt[c] = m;
+}
+
+__global__ void k3_cells_pack(const int64_t *__restrict__ lstart, const int64_t *__restrict__ cnt, int64_t ncells,
+                              uint2 *__restrict__ cells, unsigned long long *__restrict__ maxlen) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncells) return;
+    cells[c] = make_uint2((uint32_t)lstart[c], (uint32_t)cnt[c]);
+    atomicMax(maxlen, (unsigned long long)cnt[c]);
+}
+
+// ---- query -----------------------------------------------------------------
+__device__ __forceinline__ void nearest3(const Dev3Layout &L, double px, double py, double pz, double &best,
+                                         int &bid) {
+    const int ix = cell_axis(px, L.g0x, L.ginv, L.nx);
+    const int iy = cell_axis(py, L.g0y, L.ginv, L.ny);
+    const int iz = cell_axis(pz, L.g0z, L.ginv, L.nz);
+    const uint2 cr = __ldg(L.cells + ((int64_t)iz * L.ny + iy) * L.nx + ix);
+    best = INFINITY;
+    bid = 0x7FFFFFFF;
+    const float4 *e = L.lists + 2 * (size_t)cr.x;
+    for (uint32_t k = 0; k < cr.y; k++) {
+        const float4 lo = __ldg(e + 2 * k), hi = __ldg(e + 2 * k + 1);
+        const double d = box_dist(px, py, pz, lo, hi);
+        const int id = __float_as_int(lo.w);
+        if (d < best || (d == best && id < bid)) {
+            best = d;
+            bid = id;
+        }
+    }
+}
+
+__global__ void k3_query(const Dev3Layout L, const double *__restrict__ pts, int64_t n, double *__restrict__ clear,
+                         int64_t *__restrict__ nearest) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double d;
+    int id;
+    nearest3(L, pts[3 * i], pts[3 * i + 1], pts[3 * i + 2], d, id);
+    if (clear) clear[i] = d;
+    if (nearest) nearest[i] = id;
+}
+
+// ---- walk ------------------------------------------------------------------
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        if (r) {
+            k.x += 0x9E3779B9u;
+            k.y += 0xBB67AE85u;
+        }
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+    }
+    return c;
+}
+
+__device__ __forceinline__ uint4 block3(const Walk3Params &P, uint64_t walk, uint32_t blk) {
+    return philox4x32_10(make_uint4(blk, (uint32_t)walk, (uint32_t)(walk >> 32), P.stream),
+                         make_uint2((uint32_t)P.seed, (uint32_t)(P.seed >> 32)));
+}
+
+__device__ __forceinline__ uint32_t word_of(const uint4 &b, uint32_t t) {
+    const uint32_t k = t & 3;
+    return k == 0 ? b.x : (k == 1 ? b.y : (k == 2 ? b.z : b.w));
+}
+
+struct Walker {
+    double px, py, pz;
+    double a0, sgn;
+    uint4 rnd;
+    uint64_t idx;  // walk index relative to P.first
+    uint32_t rblk;
+    int hops, b1, axis;
+};
+
+// Start point on the Gaussian box: faces z0, z1, y0, y1, x0, x1 by area from
+// u0 (its remainder places the first coordinate), u1 the second.
+__device__ __forceinline__ void start_walk(const Walk3Params &P, Walker &W, uint64_t j) {
+    W.idx = j;
+    W.rnd = block3(P, P.first + j, 0);
+    W.rblk = 0;
+    const double u0 = (double)W.rnd.x * 0x1p-32, u1 = (double)W.rnd.y * 0x1p-32;
+    const double *G = P.G;
+    const double w = __dsub_rn(G[3], G[0]), h = __dsub_rn(G[4], G[1]), d = __dsub_rn(G[5], G[2]);
+    const double axy = __dmul_rn(w, h), axz = __dmul_rn(w, d), ayz = __dmul_rn(h, d);
+    double s = __dmul_rn(u0, P.S);
+    int f = 0;
+    double a = axy;
+    for (; f < 5; f++) {
+        a = f < 2 ? axy : (f < 4 ? axz : ayz);
+        if (s < a) break;
+        s = __dsub_rn(s, a);
+    }
+    if (f == 5) a = ayz;
+    double t = __ddiv_rn(s, a);
+    if (t > 1.0) t = 1.0;
+    const int hi = f & 1;
+    if ((f >> 1) == 0) {
+        W.px = __dadd_rn(G[0], __dmul_rn(t, w));
+        W.py = __dadd_rn(G[1], __dmul_rn(u1, h));
+        W.pz = hi ? G[5] : G[2];
+        W.axis = 2;
+    } else if ((f >> 1) == 1) {
+        W.px = __dadd_rn(G[0], __dmul_rn(t, w));
+        W.py = hi ? G[4] : G[1];
+        W.pz = __dadd_rn(G[2], __dmul_rn(u1, d));
+        W.axis = 1;
+    } else {
+        W.px = hi ? G[3] : G[0];
+        W.py = __dadd_rn(G[1], __dmul_rn(t, h));
+        W.pz = __dadd_rn(G[2], __dmul_rn(u1, d));
+        W.axis = 0;
+    }
+    W.sgn = hi ? 1.0 : -1.0;
+    W.hops = 0;
+    W.b1 = -1;
+    W.a0 = 0.0;
+}
+
+// Landing on the cube of half-side h at the centre of bin b (face k, row i,
+// column j): offsets o_i = (2 i + 1 - n) / n half-sides from the face centre.
+__device__ __forceinline__ void land(const Walk3Params &P, const double *s_offs, Walker &W, int b, double h) {
+    const int nn = P.n * P.n, k = b / nn, r = b - k * nn, i = r / P.n, j = r - i * P.n;
+    const double hi_ = __dmul_rn(h, s_offs[i]), hj = __dmul_rn(h, s_offs[j]);
+    const double x = W.px, y = W.py, z = W.pz;
+    switch (k) {
+    case 0: W.px = __dadd_rn(x, hi_); W.py = __dadd_rn(y, hj); W.pz = __dsub_rn(z, h); break;
+    case 1: W.px = __dadd_rn(x, h); W.py = __dadd_rn(y, hi_); W.pz = __dadd_rn(z, hj); break;
+    case 2: W.px = __dsub_rn(x, hj); W.py = __dadd_rn(y, h); W.pz = __dadd_rn(z, hi_); break;
+    case 3: W.px = __dsub_rn(x, hi_); W.py = __dsub_rn(y, hj); W.pz = __dadd_rn(z, h); break;
+    case 4: W.px = __dsub_rn(x, h); W.py = __dsub_rn(y, hi_); W.pz = __dsub_rn(z, hj); break;
+    default: W.px = __dadd_rn(x, hj); W.py = __dsub_rn(y, h); W.pz = __dsub_rn(z, hi_); break;
+    }
+}
+
+__global__ void __launch_bounds__(kW3Threads, kW3MinBlocks) k_walk3(const Walk3Params P) {
+    __shared__ uint16_t s_guide[1 << kGuide3Bits];
+    __shared__ double s_offs[FRW3_NSAMPLE_MAX];
+    for (int k = threadIdx.x; k < (1 << kGuide3Bits); k += blockDim.x) s_guide[k] = P.guide[k];
+    for (int k = threadIdx.x; k < P.n; k += blockDim.x) s_offs[k] = P.offs[k];
+    __syncthreads();
+
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const bool trace = P.rec_end || P.rec_hops || P.rec_bin || P.rec_w;
+    Walker W;
+    bool active = false;
+    unsigned long long tn = 0, n_esc = 0, n_ab = 0, n_hops = 0, n_done = 0;
+    double ts = 0.0, ts2 = 0.0;
+    uint64_t next = 0, cend = 0;
+    bool exhausted = false;
+
+    for (;;) {
+        // refill idle lanes from the warp's chunk, claiming chunks as needed
+        unsigned idle = __ballot_sync(kFull, !active);
+        while (idle && !exhausted) {
+            if (next >= cend) {
+                unsigned long long base = 0;
+                if (lane == 0) base = atomicAdd(P.counter, (unsigned long long)kW3Chunk);
+                base = __shfl_sync(kFull, base, 0);
+                if (base >= P.walks) {
+                    exhausted = true;
+                    break;
+                }
+                next = (uint64_t)base;
+                cend = next + kW3Chunk < P.walks ? next + kW3Chunk : P.walks;
+            }
+            const uint64_t avail = cend - next;
+            const unsigned rank = __popc(idle & lt);
+            if (!active && rank < avail) {
+                start_walk(P, W, next + rank);
+                active = true;
+            }
+            next += (uint64_t)__popc(idle) < avail ? (uint64_t)__popc(idle) : avail;
+            idle = __ballot_sync(kFull, !active);
+        }
+        if (__ballot_sync(kFull, active) == 0) break;
+        if (!active) continue;
+
+        // one hop
+        int64_t end = -3;  // still walking
+        double d = 0.0;
+        if (!(W.px > P.L.b[0] && W.py > P.L.b[1] && W.pz > P.L.b[2] && W.px < P.L.b[3] && W.py < P.L.b[4] &&
+              W.pz < P.L.b[5])) {
+            end = -1;
+        } else {
+            int id;
+            nearest3(P.L, W.px, W.py, W.pz, d, id);
+            W.hops++;
+            if (d <= P.shell) end = id;
+            else if (W.hops >= P.hop_cap) end = -2;
+        }
+        if (end == -3) {
+            const uint32_t t = (uint32_t)W.hops + 1;
+            if ((t >> 2) != W.rblk) {
+                W.rblk = t >> 2;
+                W.rnd = block3(P, P.first + W.idx, W.rblk);
+            }
+            const uint32_t x = word_of(W.rnd, t);
+            int b = s_guide[x >> (32 - kGuide3Bits)];
+            while (b + 1 < P.nb && __ldg(P.thr + b + 1) <= x) b++;
+            land(P, s_offs, W, b, d);
+            if (W.hops == 1) {
+                W.b1 = b;
+                W.a0 = __dmul_rn(2.0, d);
+            }
+            continue;
+        }
+        // the walk ended
+        double c = 0.0;
+        if (W.b1 >= 0) {
+            const double wv = __ldg(P.w + 3 * W.b1 + W.axis);
+            c = __ddiv_rn(__dmul_rn(__dmul_rn(P.perm, P.S), __dmul_rn(W.sgn, wv)), W.a0);
+        }
+        if (trace) {
+            if (P.rec_end) P.rec_end[W.idx] = end;
+            if (P.rec_hops) P.rec_hops[W.idx] = W.hops;
+            if (P.rec_bin) P.rec_bin[W.idx] = W.b1;
+            if (P.rec_w) P.rec_w[W.idx] = c;
+        } else if (end == P.target) {
+            tn++;
+            ts = __dadd_rn(ts, c);
+            ts2 = __dadd_rn(ts2, __dmul_rn(c, c));
+        } else if (end >= 0) {
+            atomicAdd(P.hits + end, 1ull);
+            atomicAdd(P.sum_w + end, c);
+            atomicAdd(P.sum_w2 + end, __dmul_rn(c, c));
+        }
+        if (end == -1) n_esc++;
+        else if (end == -2) n_ab++;
+        n_hops += (unsigned long long)W.hops;
+        n_done++;
+        active = false;
+    }
+
+    // warp totals -> global rows
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        tn += __shfl_xor_sync(kFull, tn, o);
+        ts += __shfl_xor_sync(kFull, ts, o);
+        ts2 += __shfl_xor_sync(kFull, ts2, o);
+        n_esc += __shfl_xor_sync(kFull, n_esc, o);
+        n_ab += __shfl_xor_sync(kFull, n_ab, o);
+        n_hops += __shfl_xor_sync(kFull, n_hops, o);
+        n_done += __shfl_xor_sync(kFull, n_done, o);
+    }
+    if (lane == 0) {
+        if (!trace && tn) {
+            atomicAdd(P.hits + P.target, tn);
+            atomicAdd(P.sum_w + P.target, ts);
+            atomicAdd(P.sum_w2 + P.target, ts2);
+        }
+        if (P.stats) {
+            atomicAdd(P.stats + 0, n_esc);
+            atomicAdd(P.stats + 1, n_ab);
+            atomicAdd(P.stats + 2, n_hops);
+            atomicAdd(P.stats + 3, n_done);
+        }
+    }
+}
+
+}  // namespace
+
+void free_grid3(Grid3Buffers *g, cudaStream_t st) {
+    if (g->cells) cudaFreeAsync(g->cells, st);
+    if (g->lists) cudaFreeAsync(g->lists, st);
+    *g = Grid3Buffers();
+}
+
+void attach_grid3(Dev3Layout &L, const Grid3Buffers &g, const double bounds[6]) {
+    L.cells = g.cells;
+    L.lists = g.lists;
+    L.g0x = g.g0[0];
+    L.g0y = g.g0[1];
+    L.g0z = g.g0[2];
+    L.ginv = 1.0 / g.side;
+    L.nx = g.nx;
+    L.ny = g.ny;
+    L.nz = g.nz;
+    for (int c = 0; c < 6; c++) L.b[c] = bounds[c];
+}
+
+frw_status build_grid3(const float *d_boxes, int64_t n, const double bounds[6], double cells_per_box,
+                       cudaStream_t st, Grid3Buffers *out) {
+    *out = Grid3Buffers();
+    if (!(cells_per_box > 0) || n < 1 || n > INT32_MAX) {
+        set_error("build_grid3: cells_per_box must be > 0 and 1 <= n < 2^31");
+        return FRW_E_ARG;
+    }
+    double ext[3], vol = 1.0, M = 16.0;
+    for (int c = 0; c < 3; c++) {
+        ext[c] = bounds[3 + c] - bounds[c];
+        vol *= ext[c];
+        M = std::max(M, 4.0 * std::max(std::max(std::fabs(bounds[c]), std::fabs(bounds[3 + c])), ext[c]));
+    }
+    const double target = std::min((double)kMaxCells3, std::max(1.0, cells_per_box * (double)n));
+    double side = std::cbrt(vol / target);
+    if (!(side > 0) || !std::isfinite(side)) side = std::max(ext[0], std::max(ext[1], ext[2]));
+    for (int c = 0; c < 3; c++) side = std::max(side, ext[c] / kMaxAxisCells3);
+    int64_t nc[3];
+    for (;;) {
+        int64_t tot = 1;
+        for (int c = 0; c < 3; c++) {
+            nc[c] = std::max<int64_t>(1, (int64_t)std::ceil(ext[c] / side));
+            tot *= nc[c];
+        }
+        if (tot <= kMaxCells3 && nc[0] <= kMaxAxisCells3 && nc[1] <= kMaxAxisCells3 && nc[2] <= kMaxAxisCells3)
+            break;
+        side *= 1.25;
+    }
+    const int64_t ncells = nc[0] * nc[1] * nc[2];
+    Grid3 G;
+    for (int c = 0; c < 3; c++) {
+        G.o[c] = bounds[c];
+        G.n[c] = (int)nc[c];
+    }
+    G.side = side;
+    G.inv = 1.0 / side;
+    G.h = 0.5 * side;
+    G.margin = std::ldexp(M, -30);
+
+    Events ev(2);
+    if (!ev.ok(2)) return cuda_fail(cudaErrorUnknown, "event create");
+    Grid3Buffers B;
+    B.ncells = ncells;
+    B.nx = G.n[0];
+    B.ny = G.n[1];
+    B.nz = G.n[2];
+    for (int c = 0; c < 3; c++) B.g0[c] = G.o[c];
+    B.side = side;
+    int64_t *bcnt = nullptr, *bstart = nullptr, *lcnt = nullptr, *lstart = nullptr, *sums = nullptr,
+            *grand = nullptr;
+    int32_t *items = nullptr;
+    unsigned long long *maxlen = nullptr;
+    const int64_t tiles = scan_i64_tiles(ncells + 1);
+    frw_status rc = FRW_OK;
+    auto ck = [&](cudaError_t e, const char *what) {
+        if (e != cudaSuccess && rc == FRW_OK) rc = cuda_fail(e, what);
+        return rc == FRW_OK;
+    };
+    do {
+        if (!ck(cudaEventRecord(ev[0], st), "event")) break;
+        const size_t cb = (size_t)(ncells + 1) * 8;
+        if (!ck(cudaMallocAsync(&bcnt, cb, st), "malloc bin counts")) break;
+        if (!ck(cudaMallocAsync(&bstart, cb, st), "malloc bin starts")) break;
+        if (!ck(cudaMallocAsync(&lcnt, cb, st), "malloc list counts")) break;
+        if (!ck(cudaMallocAsync(&lstart, cb, st), "malloc list starts")) break;
+        if (!ck(cudaMallocAsync(&sums, (size_t)tiles * 8, st), "malloc tile sums")) break;
+        if (!ck(cudaMallocAsync(&grand, 16, st), "malloc totals")) break;
+        if (!ck(cudaMallocAsync(&maxlen, 8, st), "malloc max")) break;
+        if (!ck(cudaMallocAsync(&B.cells, (size_t)ncells * sizeof(uint2), st), "malloc cells")) break;
+        if (!ck(cudaMemsetAsync(bcnt, 0, cb, st), "memset")) break;
+        if (!ck(cudaMemsetAsync(lcnt, 0, cb, st), "memset")) break;
+        if (!ck(cudaMemsetAsync(maxlen, 0, 8, st), "memset")) break;
+        const unsigned nb = (unsigned)((n + 255) / 256);
+        k3_bin_count<<<nb, 256, 0, st>>>(d_boxes, n, G, (unsigned long long *)bcnt);
+        launch_scan_i64(bcnt, ncells + 1, bstart, sums, grand, st);
+        if (!ck(cudaGetLastError(), "bin count")) break;
+        int64_t nitems = 0;
+        if (!ck(cudaMemcpyAsync(&nitems, grand, 8, cudaMemcpyDeviceToHost, st), "bin total")) break;
+        if (!ck(cudaStreamSynchronize(st), "bin total")) break;
+        if (nitems > INT32_MAX) {
+            set_error("build_grid3: more than 2^31 bin entries; use fewer cells per box");
+            rc = FRW_E_ARG;
+            break;
+        }
+        if (!ck(cudaMallocAsync(&items, (size_t)std::max<int64_t>(nitems, 1) * 4, st), "malloc bins")) break;
+        // the fill uses bcnt as its cursor: start it at the bin starts
+        if (!ck(cudaMemcpyAsync(bcnt, bstart, cb, cudaMemcpyDeviceToDevice, st), "cursor")) break;
+        k3_bin_fill<<<nb, 256, 0, st>>>(d_boxes, n, G, (unsigned long long *)bcnt, items);
+        const unsigned cbk = (unsigned)((ncells + 127) / 128);
+        k3_cell_lists<false><<<cbk, 128, 0, st>>>(d_boxes, G, bstart, items, ncells, lcnt, nullptr, nullptr);
+        launch_scan_i64(lcnt, ncells + 1, lstart, sums, grand + 1, st);
+        if (!ck(cudaGetLastError(), "cell count")) break;
+        int64_t total = 0;
+        if (!ck(cudaMemcpyAsync(&total, grand + 1, 8, cudaMemcpyDeviceToHost, st), "list total")) break;
+        if (!ck(cudaStreamSynchronize(st), "list total")) break;
+        if (total > (int64_t)UINT32_MAX / 2) {
+            set_error("build_grid3: more than 2^31 list entries; use fewer cells per box");
+            rc = FRW_E_ARG;
+            break;
+        }
+        B.entries = total;
+        if (!ck(cudaMallocAsync(&B.lists, (size_t)std::max<int64_t>(total, 1) * 32, st), "malloc lists")) break;
+        k3_cell_lists<true><<<cbk, 128, 0, st>>>(d_boxes, G, bstart, items, ncells, nullptr, lstart, B.lists);
+        k3_cells_pack<<<cbk, 128, 0, st>>>(lstart, lcnt, ncells, B.cells, maxlen);
+        if (!ck(cudaGetLastError(), "cell fill")) break;
+        unsigned long long ml = 0;
+        if (!ck(cudaMemcpyAsync(&ml, maxlen, 8, cudaMemcpyDeviceToHost, st), "max list")) break;
+        if (!ck(cudaEventRecord(ev[1], st), "event")) break;
+        if (!ck(cudaEventSynchronize(ev[1]), "grid sync")) break;
+        B.max_list = (int32_t)ml;
+        cudaEventElapsedTime(&B.build_ms, ev[0], ev[1]);
+    } while (0);
+    for (void *p : {(void *)bcnt, (void *)bstart, (void *)lcnt, (void *)lstart, (void *)sums, (void *)grand,
+                    (void *)items, (void *)maxlen})
+        if (p) cudaFreeAsync(p, st);
+    if (rc != FRW_OK) {
+        free_grid3(&B, st);
+        return rc;
+    }
+    *out = B;
+    return FRW_OK;
+}
+
+frw_status launch_query3(const Dev3Layout &L, const double *d_pts, int64_t n, double *d_clear, int64_t *d_nearest,
+                         cudaStream_t st) {
+    if (n <= 0) return FRW_OK;
+    k3_query<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(L, d_pts, n, d_clear, d_nearest);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? FRW_OK : cuda_fail(e, "k3_query");
+}
+
+frw_status launch_walk3(const Walk3Params &P, int blocks, cudaStream_t st) {
+    k_walk3<<<blocks, kW3Threads, 0, st>>>(P);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? FRW_OK : cuda_fail(e, "k_walk3");
+}
+
+int walk3_max_blocks_per_sm() {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk3, kW3Threads, 0) != cudaSuccess) return 1;
+    return std::max(b, 1);
+}
+
+int walk3_threads() { return kW3Threads; }
+
+}  // namespace frw

@@ -16,6 +16,10 @@ Names follow the reference (piogrzej/engineer-thesis, randomWalk/):
 * :meth:`Layout.walk` -- the estimator of ``getAvgPathLen(CUDA)``.
 * :meth:`Layout.walk_trace` -- ``randomWalkCudaWrapper``'s per-walk outputs.
 * :func:`get_avg_path_len_cuda` -- ``getAvgPathLenCUDA``.
+* :func:`cube_green_table`, :func:`green_cube`, :func:`deriv_green_cube` --
+  ``precompute_unit_cube_green``, ``green_cube``, ``deriv_green_cube``
+  (green/green.h:71-80), and :class:`Layout3`, the 3-D walk over box
+  conductors that the reference's cube table was written for (include/frw3d.h).
 """
 from __future__ import annotations
 
@@ -28,6 +32,7 @@ import numpy as np
 PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB_PATH = os.path.join(PKG, "lib", "libfrw.so")
 HEADER = os.path.join(os.path.dirname(PKG), "include", "frw.h")
+HEADER3 = os.path.join(os.path.dirname(PKG), "include", "frw3d.h")
 
 OK, E_ARG, E_IO, E_CUDA, E_OOM, E_HOPCAP, E_TIMEOUT, E_DEVICE, E_KERNEL = 0, -1, -2, -3, -4, -5, -6, -7, -8
 NSAMPLE = 200
@@ -157,6 +162,56 @@ class CellsInfo(C.Structure):
     ]
 
 
+class Opts3(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_uint32),
+        ("gauss_offset", C.c_double),
+        ("shell", C.c_double),
+        ("hop_cap", C.c_int64),
+        ("permittivity", C.c_double),
+        ("stream_id", C.c_uint32),
+        ("nsample", C.c_int32),
+        ("first_walk", C.c_uint64),
+        ("blocks_per_sm", C.c_int32),
+    ]
+
+
+class Result3(C.Structure):
+    _fields_ = [
+        ("walks", C.c_uint64),
+        ("escaped", C.c_uint64),
+        ("aborted", C.c_uint64),
+        ("hops_total", C.c_uint64),
+        ("gauss", C.c_double * 6),
+        ("shell", C.c_double),
+        ("fraction_other", C.c_double),
+        ("kernel_ms", C.c_double),
+        ("capacity", C.c_int64),
+        ("n_entries", C.c_int64),
+        ("conductor", C.POINTER(C.c_int64)),
+        ("hits", C.POINTER(C.c_uint64)),
+        ("cap", C.POINTER(C.c_double)),
+        ("cap_se", C.POINTER(C.c_double)),
+        ("sum_w", C.POINTER(C.c_double)),
+        ("sum_w2", C.POINTER(C.c_double)),
+    ]
+
+
+class Layout3Info(C.Structure):
+    _fields_ = [
+        ("n", C.c_int64),
+        ("device", C.c_int),
+        ("grid", C.c_int32 * 3),
+        ("bounds", C.c_double * 6),
+        ("cell_side", C.c_double),
+        ("min_edge", C.c_double),
+        ("list_entries", C.c_int64),
+        ("max_list", C.c_int32),
+        ("mean_list", C.c_double),
+        ("build_ms", C.c_float),
+    ]
+
+
 _D = C.POINTER(C.c_double)
 _F = C.POINTER(C.c_float)
 _I64 = C.POINTER(C.c_int64)
@@ -205,6 +260,21 @@ _SIGS = {
     "frw_mlp_forward": ([_F, _F, C.c_int64, _F, C.c_int], C.c_int),
     "frw_mlp_grad": ([_F, _F, _F, _F, C.c_int64, C.c_double, _F, _D, C.c_int], C.c_int),
     "frw_cv_features": ([_VP, C.c_int64, _D, C.c_int64, _F], C.c_int),
+    "frw3_cube_green_table": ([C.c_int, _D, _D, _D, _D, _D], C.c_int),
+    "frw3_green_cube": ([C.c_double, C.c_double, C.c_double, _D], C.c_int),
+    "frw3_deriv_green_cube": ([C.c_double, C.c_double, C.c_double, _D], C.c_int),
+    "frw3_layout_create": ([_F, C.c_int64, _D, C.c_double, C.c_int, C.POINTER(_VP)], C.c_int),
+    "frw3_layout_from_file": ([C.c_char_p, _D, _D, C.c_int, _D, C.c_double, C.c_int, C.POINTER(_VP)], C.c_int),
+    "frw3_layout_destroy": ([_VP], C.c_int),
+    "frw3_layout_info_get": ([_VP, C.POINTER(Layout3Info)], C.c_int),
+    "frw3_layout_boxes": ([_VP, _F], C.c_int),
+    "frw3_query_batch": ([_VP, _VP, C.c_int64, _VP, _VP, C.c_int, _VP], C.c_int),
+    "frw3_opts_default": ([C.POINTER(Opts3)], None),
+    "frw3_walk": ([_VP, C.c_int64, C.c_uint64, C.c_uint64, C.POINTER(Opts3), C.POINTER(Result3), _VP], C.c_int),
+    "frw3_walk_trace": ([_VP, C.c_int64, C.c_uint64, C.c_uint64, C.c_uint64, C.POINTER(Opts3), _VP, _VP, _VP,
+                         _VP, C.c_int, _VP], C.c_int),
+    "frw3_generate_layout": ([C.c_uint64, C.c_int64, C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_int32,
+                              C.c_int32, C.c_int32, _F], C.c_int),
 }
 CV_PARAMS = 5313
 
@@ -607,9 +677,168 @@ def get_avg_path_len_cuda(path: str, iter_num: int, rect_id: int, layer: int = 0
     return out.value
 
 
-def header_symbols(header: str = HEADER):
-    """Function names declared in include/frw.h."""
+def header_symbols(headers=(HEADER, HEADER3)):
+    """Function names declared in include/frw.h and include/frw3d.h."""
     import re
 
-    txt = open(header).read()
-    return sorted(set(re.findall(r"^\s*(?:const\s+)?[a-z_0-9]+\s*\*?\s*(frw_[a-z_0-9]+)\s*\(", txt, re.M)))
+    if isinstance(headers, str):
+        headers = (headers,)
+    names = set()
+    for h in headers:
+        txt = open(h).read()
+        names |= set(re.findall(r"^\s*(?:const\s+)?[a-z_0-9]+\s*\*?\s*(frw3?_[a-z_0-9]+)\s*\(", txt, re.M))
+    return sorted(names)
+
+
+# ---- 3-D path (include/frw3d.h) ------------------------------------------------
+NSAMPLE3 = 50
+
+
+def cube_green_table(n: int = NSAMPLE3):
+    """precompute_unit_cube_green(g, dgdx, dgdy, dgdz, intg, n) (host, FP64)."""
+    nb = 6 * n * n
+    out = [np.zeros(nb) for _ in range(4)] + [np.zeros(nb + 1)]
+    _check(lib().frw3_cube_green_table(n, *[_ptr(a, _D) for a in out]))
+    return tuple(out)
+
+
+def green_cube(a: float, eta: float, dzeta: float) -> float:
+    g = C.c_double()
+    _check(lib().frw3_green_cube(a, eta, dzeta, C.byref(g)))
+    return g.value
+
+
+def deriv_green_cube(a: float, eta: float, dzeta: float) -> np.ndarray:
+    dg = np.zeros(3)
+    _check(lib().frw3_deriv_green_cube(a, eta, dzeta, _ptr(dg, _D)))
+    return dg
+
+
+def opts3(gauss_offset=1.0, shell=0.0, hop_cap=100000, permittivity=PERMITTIVITY, stream_id=0, nsample=NSAMPLE3,
+          first_walk=0, blocks_per_sm=0) -> Opts3:
+    o = Opts3()
+    lib().frw3_opts_default(C.byref(o))
+    o.gauss_offset = gauss_offset
+    o.shell = shell
+    o.hop_cap = hop_cap
+    o.permittivity = permittivity
+    o.stream_id = stream_id
+    o.nsample = nsample
+    o.first_walk = first_walk
+    o.blocks_per_sm = blocks_per_sm
+    return o
+
+
+def generate_layout3(seed: int, n: int, domain: float, zdomain: float, wmin: int = 5, wmax: int = 50,
+                     zmin: int = 5, zmax: int = 50, gap: int = 2) -> np.ndarray:
+    out = np.zeros((n, 6), dtype=np.float32)
+    _check(lib().frw3_generate_layout(seed, n, domain, zdomain, wmin, wmax, zmin, zmax, gap, _ptr(out, _F)))
+    return out
+
+
+class Layout3:
+    """A device-resident 3-D layout (boxes) with its cell grid."""
+
+    def __init__(self, handle, n: int):
+        self._h = handle
+        self.n = n
+
+    @classmethod
+    def from_boxes(cls, boxes, bounds=None, cells_per_box: float = 0.0, device: int = 0) -> "Layout3":
+        b = np.ascontiguousarray(boxes, dtype=np.float32)
+        if b.ndim != 2 or b.shape[1] != 6:
+            raise ValueError("boxes must be (n, 6)")
+        bd = None if bounds is None else np.ascontiguousarray(bounds, dtype=np.float64)
+        h = _VP()
+        _check(lib().frw3_layout_create(_ptr(b, _F), len(b), _ptr(bd, _D), cells_per_box, device, C.byref(h)))
+        return cls(h, len(b))
+
+    @classmethod
+    def from_file(cls, path: str, z0, z1, bounds=None, cells_per_box: float = 0.0, device: int = 0) -> "Layout3":
+        a = np.ascontiguousarray(z0, dtype=np.float64)
+        b = np.ascontiguousarray(z1, dtype=np.float64)
+        bd = None if bounds is None else np.ascontiguousarray(bounds, dtype=np.float64)
+        h = _VP()
+        _check(lib().frw3_layout_from_file(path.encode(), _ptr(a, _D), _ptr(b, _D), len(a), _ptr(bd, _D),
+                                           cells_per_box, device, C.byref(h)))
+        info = Layout3Info()
+        _check(lib().frw3_layout_info_get(h, C.byref(info)))
+        return cls(h, info.n)
+
+    def close(self):
+        if self._h:
+            lib().frw3_layout_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def info(self) -> Layout3Info:
+        i = Layout3Info()
+        _check(lib().frw3_layout_info_get(self._h, C.byref(i)))
+        return i
+
+    @property
+    def bounds(self) -> np.ndarray:
+        return np.array(self.info.bounds[:])
+
+    def boxes(self) -> np.ndarray:
+        out = np.zeros((self.n, 6), dtype=np.float32)
+        _check(lib().frw3_layout_boxes(self._h, _ptr(out, _F)))
+        return out
+
+    def query(self, pts):
+        """Clearance (L-infinity distance to the nearest box) and that box for (n,3) points."""
+        p = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+        d = np.zeros(len(p))
+        k = np.zeros(len(p), dtype=np.int64)
+        _check(lib().frw3_query_batch(self._h, _ptr(p), len(p), _ptr(d), _ptr(k), MEM_HOST, None))
+        return d, k
+
+    def query_device(self, pts_t, clear_t, nearest_t, stream: int = 0):
+        _check(lib().frw3_query_batch(self._h, C.c_void_p(pts_t.data_ptr()), pts_t.shape[0],
+                                      C.c_void_p(clear_t.data_ptr()), C.c_void_p(nearest_t.data_ptr()), MEM_DEVICE,
+                                      stream or None))
+
+    def walk(self, target: int, walks: int, seed: int, o: Opts3 | None = None, capacity: int | None = None,
+             stream: int = 0) -> WalkResult:
+        o = o or opts3()
+        cap = self.n if capacity is None else capacity
+        cond = np.zeros(cap, dtype=np.int64)
+        hits = np.zeros(cap, dtype=np.uint64)
+        c = np.zeros(cap)
+        se = np.zeros(cap)
+        s1 = np.zeros(cap)
+        s2 = np.zeros(cap)
+        r = Result3()
+        r.capacity = cap
+        r.conductor = _ptr(cond, _I64)
+        r.hits = _ptr(hits, C.POINTER(C.c_uint64))
+        r.cap = _ptr(c, _D)
+        r.cap_se = _ptr(se, _D)
+        r.sum_w = _ptr(s1, _D)
+        r.sum_w2 = _ptr(s2, _D)
+        _check(lib().frw3_walk(self._h, target, walks, seed, C.byref(o), C.byref(r), stream or None))
+        m = min(r.n_entries, cap)
+        return WalkResult(r.walks, r.escaped, r.aborted, r.hops_total, np.array(r.gauss[:]), r.fraction_other,
+                          r.kernel_ms, cond[:m], hits[:m], c[:m], se[:m], s1[:m], s2[:m], {"shell": r.shell})
+
+    def walk_trace(self, target: int, first: int, walks: int, seed: int, o: Opts3 | None = None):
+        o = o or opts3()
+        end = np.zeros(walks, dtype=np.int64)
+        hops = np.zeros(walks, dtype=np.int32)
+        b1 = np.zeros(walks, dtype=np.int32)
+        w = np.zeros(walks)
+        _check(lib().frw3_walk_trace(self._h, target, first, walks, seed, C.byref(o), _ptr(end), _ptr(hops),
+                                     _ptr(b1), _ptr(w), MEM_HOST, None))
+        return end, hops, b1, w

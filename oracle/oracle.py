@@ -4,7 +4,8 @@ Only tests/, ``__graft_entry__.smoke()`` and the cpu_baseline / reference legs
 of ``bench.py`` import this module.  It wraps
 
 * ``liboracle.so``      -- the C restatement of the reference CPU path
-                           (``frwcpu.c``), and
+                           (``frwcpu.c``) and of the 3-D walk with the cube
+                           table (``frwcpu3d.c``), and
 * ``_ref/librefcpu.so`` -- the unmodified reference CPU sources compiled in
                            place (``ref_driver.cpp``), when present.
 """
@@ -59,6 +60,20 @@ class WalkCfg(C.Structure):
     ]
 
 
+class Cfg3(C.Structure):
+    """oc3_cfg of frwcpu3d.h."""
+    _fields_ = [
+        ("target", C.c_int64),
+        ("offset", C.c_double),
+        ("shell", C.c_double),
+        ("hop_cap", C.c_int64),
+        ("permittivity", C.c_double),
+        ("seed", C.c_uint64),
+        ("stream", C.c_uint32),
+        ("nsample", C.c_int),
+    ]
+
+
 _lib = None
 
 
@@ -105,6 +120,22 @@ def lib():
                                      _I64, _I32]
         L.oc_walk_stream.restype = C.c_int64
         L.oc_cv_features.argtypes = [_D, C.c_int64, C.c_int64, _D, C.c_int64, C.POINTER(C.c_float)]
+        L.oc3_cube_green_table.argtypes = [C.c_int, _D, _D, _D, _D, _D]
+        L.oc3_green_cube.argtypes = [C.c_double, C.c_double, C.c_double]
+        L.oc3_green_cube.restype = C.c_double
+        L.oc3_deriv_green_cube.argtypes = [_D, C.c_double, C.c_double, C.c_double]
+        L.oc3_weight_table.argtypes = [C.c_int, _D, _D, _D, _D, _D]
+        L.oc3_layout_bounds.argtypes = [_D, C.c_int64, _D]
+        L.oc3_default_shell.argtypes = [_D, C.c_int64]
+        L.oc3_default_shell.restype = C.c_double
+        L.oc3_nearest.argtypes = [_D, C.c_int64, _D, _D, _I64]
+        L.oc3_grid_create.argtypes = [_D, C.c_int64, _D, C.c_double]
+        L.oc3_grid_create.restype = C.c_void_p
+        L.oc3_grid_destroy.argtypes = [C.c_void_p]
+        L.oc3_grid_nearest.argtypes = [C.c_void_p, _D, _D, _I64]
+        L.oc3_query_batch.argtypes = [_D, C.c_int64, C.c_void_p, _D, C.c_int64, _D, _I64]
+        L.oc3_walk_run.argtypes = [_D, C.c_int64, _D, C.c_void_p, C.POINTER(Cfg3), C.c_uint64, C.c_uint64,
+                                   _I64, _I32, _I32, _D]
         _lib = L
     return _lib
 
@@ -317,6 +348,10 @@ def ref():
         L.ref_walks_seeded.argtypes = [C.c_int64, C.c_int64, C.c_uint32, C.c_uint32, C.c_uint32,
                                        C.c_uint32, _I64, _I32, _D, C.c_int64, _I64]
         L.ref_walks_as_shipped.argtypes = [C.c_int64, C.c_int64, _I64, _I32]
+        L.ref_unit_cube_green.argtypes = [C.c_int, _D, _D, _D, _D, _D]
+        L.ref_green_cube.argtypes = [C.c_double, C.c_double, C.c_double]
+        L.ref_green_cube.restype = C.c_double
+        L.ref_deriv_green_cube.argtypes = [_D, C.c_double, C.c_double, C.c_double]
         _ref = L
     return _ref
 
@@ -394,3 +429,77 @@ class Ref:
         hops = np.zeros(n, dtype=np.int32)
         ref().ref_walks_as_shipped(int(target), int(n), _p(end, _I64), _p(hops, _I32))
         return end, hops
+
+
+# ---------------------------------------------------------------- 3-D path
+NSAMPLE3 = 50
+
+
+def cube_green_table(n: int = NSAMPLE3):
+    """The restated precompute_unit_cube_green: (g, dgdx, dgdy, dgdz, intg)."""
+    nb = 6 * n * n
+    out = [np.zeros(nb) for _ in range(4)] + [np.zeros(nb + 1)]
+    lib().oc3_cube_green_table(n, *[_p(a) for a in out])
+    return tuple(out)
+
+
+def ref_cube_green_table(n: int = NSAMPLE3):
+    """The reference's own precompute_unit_cube_green (oracle/_ref)."""
+    nb = 6 * n * n
+    out = [np.zeros(nb) for _ in range(4)] + [np.zeros(nb + 1)]
+    ref().ref_unit_cube_green(n, *[_p(a) for a in out])
+    return tuple(out)
+
+
+def cube_weight_table(n: int = NSAMPLE3) -> np.ndarray:
+    g, dx, dy, dz, intg = cube_green_table(n)
+    w = np.zeros((6 * n * n, 3))
+    lib().oc3_weight_table(n, _p(intg), _p(dx), _p(dy), _p(dz), _p(w))
+    return w
+
+
+def layout_bounds3(boxes) -> np.ndarray:
+    b = np.ascontiguousarray(boxes, dtype=np.float64)
+    out = np.zeros(6)
+    lib().oc3_layout_bounds(_p(b), len(b), _p(out))
+    return out
+
+
+class Boxes3:
+    """A 3-D layout for the oracle: brute-force or cell-grid nearest box and walks."""
+
+    def __init__(self, boxes, bounds=None, grid: bool = False, boxes_per_cell: float = 2.0):
+        self.boxes = np.ascontiguousarray(boxes, dtype=np.float64)
+        self.n = len(self.boxes)
+        self.bounds = layout_bounds3(self.boxes) if bounds is None else np.ascontiguousarray(bounds, np.float64)
+        self.shell = float(lib().oc3_default_shell(_p(self.boxes), self.n))
+        self._g = lib().oc3_grid_create(_p(self.boxes), self.n, _p(self.bounds), boxes_per_cell) if grid else None
+
+    def __del__(self):
+        g, self._g = getattr(self, "_g", None), None
+        if g:
+            lib().oc3_grid_destroy(g)
+
+    def nearest(self, pts, use_grid: bool | None = None):
+        """(clearance, nearest box) per point; the grid when built unless use_grid is False."""
+        p = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+        d = np.zeros(len(p))
+        k = np.zeros(len(p), dtype=np.int64)
+        g = self._g if use_grid is None or use_grid else None
+        lib().oc3_query_batch(_p(self.boxes), self.n, g, _p(p), len(p), _p(d), _p(k, _I64))
+        return d, k
+
+    def cfg(self, target=0, offset=1.0, shell=None, hop_cap=100000, seed=0, stream=0, nsample=NSAMPLE3):
+        return Cfg3(target, offset, self.shell if shell is None else shell, hop_cap, PERMITTIVITY, seed, stream,
+                    nsample)
+
+    def walks(self, cfg: Cfg3, first: int, count: int):
+        end = np.zeros(count, dtype=np.int64)
+        hops = np.zeros(count, dtype=np.int32)
+        b1 = np.zeros(count, dtype=np.int32)
+        w = np.zeros(count)
+        rc = lib().oc3_walk_run(_p(self.boxes), self.n, _p(self.bounds), self._g, C.byref(cfg), first, count,
+                                _p(end, _I64), _p(hops, _I32), _p(b1, _I32), _p(w))
+        if rc != 0:
+            raise ValueError(f"oc3_walk_run failed: {rc}")
+        return end, hops, b1, w

@@ -102,6 +102,19 @@ void ref_green(double *g, double *dgdx, double *dgdy, double *intg) {
     memcpy(intg, g_intg, sizeof(g_intg));
 }
 
+// The reference's unit-cube table, precompute_unit_cube_green
+// (green/green.h:79-80, green/green.cpp:392-431; never called by the
+// reference itself): 6 n^2 samples per array, intg of 6 n^2 + 1.
+void ref_unit_cube_green(int n, double *g, double *dgdx, double *dgdy, double *dgdz, double *intg) {
+    precompute_unit_cube_green(g, dgdx, dgdy, dgdz, intg, (UINTpt_t)n);
+}
+
+// green_cube / deriv_green_cube (green/green.cpp:232-267,311-388) at one point.
+double ref_green_cube(double a, double eta, double dzeta) { return green_cube(a, eta, dzeta); }
+void ref_deriv_green_cube(double *dg, double a, double eta, double dzeta) {
+    deriv_green_cube(dg, a, eta, dzeta);
+}
+
 int ref_get_index(double r) { return getIndex(g_intg, r); }
 
 void ref_point_from_index(const double *sq, int index, double *out) {
