@@ -224,9 +224,8 @@ def test_walk3_argument_errors():
 
 def test_walk3_full_size_workload():
     """The benchmark's 3-D workload: 10,000 boxes in [0,2000)^2 x [0,400),
-    1e7 walks from box 0: every walk ends, none aborted, the target's charge
-    is positive and its neighbours' negative, and two disjoint halves of the
-    walks add up to the full run's hits."""
+    1e7 walks from box 0: every walk ends, none aborted, the row balances,
+    and two disjoint halves of the walks add up to the full run's hits."""
     b = frw.generate_layout3(0xF4A7 + 6, 10_000, 2000.0, 400.0, 5, 50, 5, 20, 2)
     with frw.Layout3.from_boxes(b) as L:
         r = L.walk(0, 10_000_000, 0x3D)
@@ -235,7 +234,10 @@ def test_walk3_full_size_workload():
     assert r.aborted == 0 and r.hits.sum() + r.escaped == 10_000_000
     c0, se0 = r.row(0)[1:]
     assert c0 > 0 and se0 < 0.01 * c0
-    assert r.sum_w.sum() > 0 and r.sum_w.sum() < c0  # neighbours and the bounds take negative charge
+    # the row sums to minus the charge at the bounds, which few walks reach
+    # here: the conductors' charges cancel to within a per cent of the target's
+    assert r.escaped < 1e-4 * r.walks
+    assert abs(r.cap.sum()) < 0.01 * c0
     a = dict(zip(h1.conductor, h1.hits))
     for k, n in zip(h2.conductor, h2.hits):
         a[k] = a.get(k, 0) + n
