@@ -83,8 +83,9 @@ frw_status device_cube_tables(int dev, int n, const Cube3Tables **out) {
 
 bool fp32_exact3(double v) { return std::isfinite(v) && (double)(float)v == v && fabs(v) < 16777216.0; }
 
-// Interiors pairwise disjoint (touching faces allowed): each box is checked
-// against the earlier boxes registered in the hash cells it overlaps.
+// Interiors pairwise disjoint (touching faces allowed): boxes are binned
+// into a hash grid of cells about one box across (count -> prefix -> fill),
+// and the boxes sharing a cell are compared pairwise.
 frw_status check_disjoint(const float *b, int64_t n) {
     double emax = 0, lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
     for (int64_t i = 0; i < n; i++)
@@ -93,34 +94,60 @@ frw_status check_disjoint(const float *b, int64_t n) {
             lo[c] = std::min(lo[c], (double)b[6 * i + c]);
             hi[c] = std::max(hi[c], (double)b[6 * i + 3 + c]);
         }
-    double cs = std::max(emax, 1e-30);
-    for (int c = 0; c < 3; c++) cs = std::max(cs, (hi[c] - lo[c]) / 1024.0);
-    int64_t nc[3];
-    for (int c = 0; c < 3; c++) nc[c] = std::max<int64_t>(1, (int64_t)floor((hi[c] - lo[c]) / cs) + 1);
-    std::map<int64_t, std::vector<int32_t>> cells;
-    for (int64_t i = 0; i < n; i++) {
-        const float *p = b + 6 * i;
-        int64_t c0[3], c1[3];
+    double vol = 1.0;
+    for (int c = 0; c < 3; c++) vol *= std::max(hi[c] - lo[c], 1e-30);
+    double cs = std::max(emax, std::cbrt(vol / (double)n));
+    int64_t nc[3], total;
+    for (;;) {
+        total = 1;
+        for (int c = 0; c < 3; c++) {
+            nc[c] = std::max<int64_t>(1, (int64_t)floor((hi[c] - lo[c]) / cs) + 1);
+            total *= nc[c];
+        }
+        if (total <= 8 * n + 64) break;
+        cs *= 1.25;
+    }
+    auto range = [&](const float *p, int64_t c0[3], int64_t c1[3]) {
         for (int c = 0; c < 3; c++) {
             c0[c] = std::min(nc[c] - 1, (int64_t)floor((p[c] - lo[c]) / cs));
             c1[c] = std::min(nc[c] - 1, (int64_t)floor((p[3 + c] - lo[c]) / cs));
         }
-        for (int64_t z = c0[2]; z <= c1[2]; z++)
-            for (int64_t y = c0[1]; y <= c1[1]; y++)
-                for (int64_t x = c0[0]; x <= c1[0]; x++) {
-                    auto &v = cells[(z * nc[1] + y) * nc[0] + x];
-                    for (int32_t j : v) {
-                        const float *q = b + 6 * (int64_t)j;
-                        bool ov = true;
-                        for (int c = 0; c < 3 && ov; c++) ov = p[c] < q[3 + c] && q[c] < p[3 + c];
-                        if (ov) {
-                            set_error("boxes " + std::to_string(j) + " and " + std::to_string(i) + " overlap");
-                            return FRW_E_ARG;
-                        }
+    };
+    std::vector<int64_t> start((size_t)total + 1, 0);
+    std::vector<int32_t> items;
+    for (int pass = 0; pass < 2; pass++) {
+        for (int64_t i = 0; i < n; i++) {
+            int64_t c0[3], c1[3];
+            range(b + 6 * i, c0, c1);
+            for (int64_t z = c0[2]; z <= c1[2]; z++)
+                for (int64_t y = c0[1]; y <= c1[1]; y++)
+                    for (int64_t x = c0[0]; x <= c1[0]; x++) {
+                        const int64_t cell = (z * nc[1] + y) * nc[0] + x;
+                        if (pass == 0) start[(size_t)cell + 1]++;
+                        else items[(size_t)start[(size_t)cell]++] = (int32_t)i;
                     }
-                    v.push_back((int32_t)i);
-                }
+        }
+        if (pass == 0) {
+            for (int64_t c = 0; c < total; c++) start[(size_t)c + 1] += start[(size_t)c];
+            items.resize((size_t)start[(size_t)total]);
+        } else {
+            for (int64_t c = total; c > 0; c--) start[(size_t)c] = start[(size_t)c - 1];
+            start[0] = 0;
+        }
     }
+    for (int64_t cell = 0; cell < total; cell++)
+        for (int64_t u = start[(size_t)cell]; u < start[(size_t)cell + 1]; u++)
+            for (int64_t v = u + 1; v < start[(size_t)cell + 1]; v++) {
+                const int32_t i = items[(size_t)u], j = items[(size_t)v];
+                const float *p = b + 6 * (int64_t)i, *q = b + 6 * (int64_t)j;
+                bool ov = true;
+                for (int c = 0; c < 3 && ov; c++) ov = p[c] < q[3 + c] && q[c] < p[3 + c];
+                if (ov) {
+                    set_error("boxes " + std::to_string(std::min(i, j)) + " and " + std::to_string(std::max(i, j)) +
+                              " overlap");
+                    return FRW_E_ARG;
+                }
+            }
     return FRW_OK;
 }
 

@@ -14,13 +14,16 @@ namespace frw {
 // L-infinity distance from the cell centre is at most D_c + 2 h + margin
 // (D_c = distance from the centre to its nearest box, h = s/2): the nearest
 // box of any point of the cell is among them.  Entries are copies of the
-// boxes, two float4 each: (x0, y0, z0, id bits) and (x1, y1, z1, 0), so a
-// query reads one 8-byte cell record and 32 bytes per candidate.
+// boxes, two float4 each: (x0, y0, z0, id bits) and (x1, y1, z1, d_c) with
+// d_c <= the box's distance from the cell centre, sorted by d_c: a query
+// reads one 8-byte cell record and 32 bytes per candidate, and stops once
+// d_c - (h + margin) exceeds its best distance.
 struct Dev3Layout {
     const uint2 *cells;    // [ncells] (first entry, entry count)
     const float4 *lists;   // [2 * entries]
     double g0x, g0y, g0z;  // grid origin
     double ginv;           // 1 / cell side
+    double hq;             // half a cell side + rounding margin
     int nx, ny, nz;
     double b[6];           // bounds (x0,y0,z0,x1,y1,z1), open
 };
@@ -32,6 +35,7 @@ struct Grid3Buffers {
     int nx = 0, ny = 0, nz = 0;
     double g0[3] = {0, 0, 0};
     double side = 0;
+    double margin = 0;
     int32_t max_list = 0;
     float build_ms = 0;
 };

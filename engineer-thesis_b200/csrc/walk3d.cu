@@ -5,7 +5,9 @@
 // 232-431, is never called); this is its 2-D walk (CPU/mainFunctions.cpp:
 // 48-90) lifted to cubes, written for B200 the way the 2-D kernels are:
 //   * the clearance query reads one cell record and a short list of box
-//     copies (32 bytes each) -- no tree descent and no stack;
+//     copies (32 bytes each), sorted by distance from the cell centre so
+//     the scan stops at the first entry that cannot be nearer -- no tree
+//     descent and no stack;
 //   * the cell lists are built on the device: boxes binned by overlap
 //     (count -> scan -> fill), then for every cell a ring search for the
 //     nearest box to its centre and a count -> scan -> fill of the boxes
@@ -170,8 +172,20 @@ __global__ void k3_cell_lists(const float *__restrict__ boxes, Grid3 G, const in
                     if (fx != x || fy != y || fz != z) continue;
                     if (box_dist(px, py, pz, lo, hi) > R) continue;
                     if (kFill) {
-                        lists[2 * (out + m)] = lo;
-                        lists[2 * (out + m) + 1] = hi;
+                        // insertion by (distance from the centre, index): a
+                        // query stops at the first entry that cannot win
+                        const double dc = box_dist(px, py, pz, lo, hi);
+                        hi.w = __double2float_rd(dc);
+                        int64_t at = out + m;
+                        while (at > out) {
+                            const float4 plo = lists[2 * (at - 1)], phi = lists[2 * (at - 1) + 1];
+                            if (phi.w < hi.w || (phi.w == hi.w && __float_as_int(plo.w) < i)) break;
+                            lists[2 * at] = plo;
+                            lists[2 * at + 1] = phi;
+                            at--;
+                        }
+                        lists[2 * at] = lo;
+                        lists[2 * at + 1] = hi;
                     }
                     m++;
                 }
@@ -199,6 +213,10 @@ __device__ __forceinline__ void nearest3(const Dev3Layout &L, double px, double 
     const float4 *e = L.lists + 2 * (size_t)cr.x;
     for (uint32_t k = 0; k < cr.y; k++) {
         const float4 lo = __ldg(e + 2 * k), hi = __ldg(e + 2 * k + 1);
+        // hi.w <= the entry's distance from the cell centre and the point is
+        // within L.hq of that centre: this entry and every later one are
+        // farther than the best so far
+        if (__dsub_rn((double)hi.w, L.hq) > best) break;
         const double d = box_dist(px, py, pz, lo, hi);
         const int id = __float_as_int(lo.w);
         if (d < best || (d == best && id < bid)) {
@@ -454,6 +472,7 @@ void attach_grid3(Dev3Layout &L, const Grid3Buffers &g, const double bounds[6]) 
     L.g0y = g.g0[1];
     L.g0z = g.g0[2];
     L.ginv = 1.0 / g.side;
+    L.hq = 0.5 * g.side + 2.0 * g.margin;
     L.nx = g.nx;
     L.ny = g.ny;
     L.nz = g.nz;
@@ -508,6 +527,7 @@ frw_status build_grid3(const float *d_boxes, int64_t n, const double bounds[6], 
     B.nz = G.n[2];
     for (int c = 0; c < 3; c++) B.g0[c] = G.o[c];
     B.side = side;
+    B.margin = G.margin;
     int64_t *bcnt = nullptr, *bstart = nullptr, *lcnt = nullptr, *lstart = nullptr, *sums = nullptr,
             *grand = nullptr;
     int32_t *items = nullptr;

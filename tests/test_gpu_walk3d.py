@@ -209,6 +209,18 @@ def test_walk3_argument_errors():
         with pytest.raises(frw.FrwError) as e:
             frw.Layout3.from_boxes(x)
         assert e.value.status == frw.E_ARG
+    # one overlapping pair among thousands of disjoint boxes; touching faces are fine
+    many = _layout(0xF4A7 + 55, 3000, 1500.0, 400.0)
+    extra = many[1234].copy()
+    extra[:3] += 1
+    extra[3:] += 1
+    with pytest.raises(frw.FrwError) as e:
+        frw.Layout3.from_boxes(np.vstack([many, extra]))
+    assert e.value.status == frw.E_ARG and "1234" in str(e.value)
+    touch = many[77].copy()
+    touch[0], touch[3] = many[77, 3], many[77, 3] + 1  # shares box 77's x1 face
+    if not (np.maximum(many[:, :3], touch[:3]) < np.minimum(many[:, 3:], touch[3:])).all(1).any():
+        frw.Layout3.from_boxes(np.vstack([many, touch])).close()
     with pytest.raises(frw.FrwError):
         frw.Layout3.from_boxes(ok, bounds=[1, 1, 1, 50, 50, 50])  # does not contain box 0
     with frw.Layout3.from_boxes(ok) as L:
