@@ -408,6 +408,17 @@ def walk3d_run(frw, device, stream, steps, cpu_seconds, cores):
             Le.walk(W3D["target"], W3D["walks"], 500 + i, o, stream=stream.cuda_stream)
     torch.cuda.synchronize()
     e2e_s = (time.perf_counter() - t0) / steps
+    # algorithmic bytes per hop: the cell record, the cell's candidate list
+    # (32 B per entry, mean over cells) and one CDF threshold
+    bh = 8 + 32 * info.mean_list + 4
+    hops = r.hops_total
+    peak, peak_kind = measured_peak_hbm()
+    ach = hops * bh / (kms * 1e-3) / 1e9
+    roof3 = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+             "traffic": 1045248,
+             "note": f"k_walk3; algorithmic {bh:.0f} B/hop x {hops / W3D['walks']:.2f} hops/walk; peak {peak_kind}; "
+                     "traffic = DRAM bytes of one 1e6-walk launch under ncu (cold reads; the lists and tables "
+                     "are L2-resident, so HBM is an upper-bound denominator)"}
     out = {"workload": W3D["workload"], "config": W3D, "ms_per_step": ms, "walks_per_s": W3D["walks"] / (ms * 1e-3),
            "kernel_ms": kms, "kernel_walks_per_s": W3D["walks"] / (kms * 1e-3),
            "hops_per_s": r.hops_total / (kms * 1e-3), "mean_hops": r.hops_total / W3D["walks"],
@@ -415,6 +426,7 @@ def walk3d_run(frw, device, stream, steps, cpu_seconds, cores):
            "grid": list(info.grid), "grid_build_ms": info.build_ms, "mean_list": info.mean_list,
            "max_list": info.max_list,
            "queries_1e7": {"ms": qms, "queries_per_s": 1e7 / (qms * 1e-3)},
+           "roofline": roof3,
            "e2e": {"value": W3D["walks"] / e2e_s, "unit": "walks/s", "h2d_bytes_per_step": W3D["boxes"] * 24,
                    "d2h_bytes_per_step": (5 + 3 * W3D["boxes"]) * 8}}
     if cpu_seconds > 0 and cores > 0:
