@@ -254,3 +254,37 @@ def test_walk3_full_size_workload():
     for k, n in zip(h2.conductor, h2.hits):
         a[k] = a.get(k, 0) + n
     assert a == dict(zip(r.conductor, r.hits))
+
+
+def test_cli_3d_mode(tmp_path):
+    """lib/frw --3d: the layers of a reference layout file extruded to z
+    ranges, the reference's two lines, the histogram and the JSON record of
+    the 3-D run."""
+    import json
+    import os
+    import subprocess
+
+    a = frw.generate_layout(21, 40, 400.0)
+    c = frw.generate_layout(22, 40, 400.0)
+    p = str(tmp_path / "two.txt")
+    with open(p, "w") as f:
+        f.write("<< m1 >>\n")
+        for r in a:
+            f.write("rect %g %g %g %g\n" % tuple(r))
+        f.write("<< m2 >>\n")
+        for r in c:
+            f.write("rect %g %g %g %g\n" % tuple(r))
+        f.write("<< end >>\n")
+    exe = os.path.join(frw.PKG, "lib", "frw")
+    h = str(tmp_path / "hist3.txt")
+    out = subprocess.run([exe, "-S", p, "-I", "50000", "-O", "3", "--3d", "0:8,12:20", "--seed", "5", "--hist", h,
+                          "--json", "--cap"], capture_output=True, text=True, check=True).stdout.splitlines()
+    assert out[1].startswith("[GPU] Ile sciezek trafi") and out[2].startswith("Czas wykonania:")
+    rec = json.loads(out[-1])
+    with frw.Layout3.from_file(p, [0.0, 12.0], [8.0, 20.0]) as L:
+        r = L.walk(3, 50_000, 5)
+    assert rec["dims"] == 3 and rec["boxes"] == 80 and rec["fraction_other"] == r.fraction_other
+    assert [x["conductor"] for x in rec["rows"]] == list(r.conductor)
+    assert open(h, encoding="utf-8").readline().strip() == "[GPU 3D]"
+    bad = subprocess.run([exe, "-S", p, "--3d", "0:8"], capture_output=True, text=True)
+    assert bad.returncode != 0 and "layers" in bad.stderr
