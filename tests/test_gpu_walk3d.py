@@ -256,6 +256,25 @@ def test_walk3_full_size_workload():
     assert a == dict(zip(r.conductor, r.hits))
 
 
+def test_walk3_million_boxes():
+    """10^6 boxes in [0,20000)^2 x [0,2000): 2e5 clearance queries and 2e4
+    walks from the middle of the walk index space equal the oracle's."""
+    b = frw.generate_layout3(0xF4A7 + 8, 1_000_000, 20000.0, 2000.0, 5, 50, 5, 20, 2)
+    B = O.Boxes3(b, grid=True, boxes_per_cell=2.0)
+    rng = np.random.default_rng(3)
+    pts = B.bounds[:3] + rng.random((200_000, 3)) * (B.bounds[3:] - B.bounds[:3])
+    with frw.Layout3.from_boxes(b) as L:
+        info = L.info
+        d, k = L.query(pts)
+        e, h, bb, w = L.walk_trace(0, 1 << 35, 20_000, 9)
+    assert info.grid[0] * info.grid[1] * info.grid[2] > 8_000_000
+    d_o, k_o = B.nearest(pts)
+    assert np.array_equal(d, d_o) and np.array_equal(k, k_o)
+    e_o, h_o, b_o, w_o = B.walks(B.cfg(target=0, seed=9), 1 << 35, 20_000)
+    assert np.array_equal(e, e_o) and np.array_equal(h, h_o) and np.array_equal(bb, b_o)
+    assert _bits_equal(w, w_o)
+
+
 def test_cli_3d_mode(tmp_path):
     """lib/frw --3d: the layers of a reference layout file extruded to z
     ranges, the reference's two lines, the histogram and the JSON record of
