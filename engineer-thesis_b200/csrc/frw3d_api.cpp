@@ -158,8 +158,8 @@ frw_status check_opts3(const frw3_opts *o) {
     }
     if (!(o->gauss_offset > 0) || !std::isfinite(o->gauss_offset) || !(o->shell >= 0 || o->shell <= 0) ||
         o->hop_cap < 1 || !std::isfinite(o->permittivity) || o->nsample < 1 || o->nsample > FRW3_NSAMPLE_MAX ||
-        o->blocks_per_sm < 0) {
-        set_error("frw3_opts: need gauss_offset > 0, hop_cap >= 1, nsample in [1, 100]");
+        o->blocks_per_sm < 0 || o->refill_min < 0 || o->refill_min > 32) {
+        set_error("frw3_opts: need gauss_offset > 0, hop_cap >= 1, nsample in [1, 100], refill_min in [0, 32]");
         return FRW_E_ARG;
     }
     return FRW_OK;
@@ -198,6 +198,11 @@ frw_status prepare_walk(const frw3_layout *L, int64_t target, uint64_t first, ui
     P->offs = T->offs;
     P->n = T->n;
     P->nb = T->nb;
+    if (T->n > 1) {
+        P->magic_n = (uint32_t)((((uint64_t)1 << 32) + (uint64_t)T->n - 1) / (uint64_t)T->n);
+        P->magic_nn = (uint32_t)((((uint64_t)1 << 32) + (uint64_t)(T->n * T->n) - 1) / (uint64_t)(T->n * T->n));
+    }
+    P->refill_min = o->refill_min < 1 ? 1 : (o->refill_min > 32 ? 32 : o->refill_min);
     const float *tb = L->boxes.data() + 6 * target;
     for (int c = 0; c < 3; c++) {
         P->G[c] = (double)tb[c] - o->gauss_offset;
@@ -461,6 +466,7 @@ void frw3_opts_default(frw3_opts *o) {
     o->nsample = FRW3_NSAMPLE_DEFAULT;
     o->first_walk = 0;
     o->blocks_per_sm = 0;
+    o->refill_min = 4;
 }
 
 frw_status frw3_walk(const frw3_layout *L, int64_t target, uint64_t walks, uint64_t seed, const frw3_opts *o,

@@ -61,6 +61,8 @@ struct Walk3Params {
     const double *w;
     const double *offs;
     int n, nb;
+    uint32_t magic_n, magic_nn;  // ceil(2^32 / n), ceil(2^32 / n^2) (n > 1)
+    int refill_min;              // refill idle lanes once this many are idle (1..32)
     double G[6];  // Gaussian box
     double S;     // its area
     int64_t target;

@@ -318,7 +318,15 @@ __device__ __forceinline__ void start_walk(const Walk3Params &P, Walker &W, uint
 // Landing on the cube of half-side h at the centre of bin b (face k, row i,
 // column j): offsets o_i = (2 i + 1 - n) / n half-sides from the face centre.
 __device__ __forceinline__ void land(const Walk3Params &P, const double *s_offs, Walker &W, int b, double h) {
-    const int nn = P.n * P.n, k = b / nn, r = b - k * nn, i = r / P.n, j = r - i * P.n;
+    // b / n^2 and r / n as multiply-highs by ceil(2^32 / d): exact for every
+    // b < 6 n^2, n <= 100 (checked exhaustively); n = 1 has no division
+    int k = b, r = 0, i = 0, j = 0;
+    if (P.n > 1) {
+        k = (int)__umulhi((unsigned)b, P.magic_nn);
+        r = b - k * P.n * P.n;
+        i = (int)__umulhi((unsigned)r, P.magic_n);
+        j = r - i * P.n;
+    }
     const double hi_ = __dmul_rn(h, s_offs[i]), hj = __dmul_rn(h, s_offs[j]);
     const double x = W.px, y = W.py, z = W.pz;
     switch (k) {
@@ -351,6 +359,9 @@ __global__ void __launch_bounds__(kW3Threads, kW3MinBlocks) k_walk3(const Walk3P
     for (;;) {
         // refill idle lanes from the warp's chunk, claiming chunks as needed
         unsigned idle = __ballot_sync(kFull, !active);
+        // refill only once refill_min lanes are idle (or none is walking):
+        // fewer divergent starts, at the price of lanes idling meanwhile
+        if (__popc(idle) < (unsigned)P.refill_min && idle != kFull) idle = 0;
         while (idle && !exhausted) {
             if (next >= cend) {
                 unsigned long long base = 0;

@@ -173,6 +173,7 @@ class Opts3(C.Structure):
         ("nsample", C.c_int32),
         ("first_walk", C.c_uint64),
         ("blocks_per_sm", C.c_int32),
+        ("refill_min", C.c_int32),
     ]
 
 
@@ -715,7 +716,7 @@ def deriv_green_cube(a: float, eta: float, dzeta: float) -> np.ndarray:
 
 
 def opts3(gauss_offset=1.0, shell=0.0, hop_cap=100000, permittivity=PERMITTIVITY, stream_id=0, nsample=NSAMPLE3,
-          first_walk=0, blocks_per_sm=0) -> Opts3:
+          first_walk=0, blocks_per_sm=0, refill_min=4) -> Opts3:
     o = Opts3()
     lib().frw3_opts_default(C.byref(o))
     o.gauss_offset = gauss_offset
@@ -726,6 +727,7 @@ def opts3(gauss_offset=1.0, shell=0.0, hop_cap=100000, permittivity=PERMITTIVITY
     o.nsample = nsample
     o.first_walk = first_walk
     o.blocks_per_sm = blocks_per_sm
+    o.refill_min = refill_min
     return o
 
 

@@ -105,6 +105,8 @@ typedef struct frw3_opts {
     int32_t nsample;       /* cube table cells per face edge */
     uint64_t first_walk;   /* Philox index of the first walk (runs over disjoint ranges add up) */
     int32_t blocks_per_sm; /* 0: library choice */
+    int32_t refill_min;    /* a warp starts new walks once this many lanes are idle (default 4; 0 or 1: at
+                              once; <= 32).  Results do not depend on it. */
 } frw3_opts;
 void frw3_opts_default(frw3_opts *opts);
 
