@@ -175,6 +175,19 @@ struct Scratch3 {
     }
 };
 
+// The layout's device status word (set only if a lookup ever found no list
+// on the whole chain of grid levels, which the build rules out).
+frw_status check_grid_status(const frw3_layout *L, cudaStream_t st) {
+    uint32_t h = 0;
+    FRW_CK(cudaMemcpyAsync(&h, L->grid.status, 4, cudaMemcpyDeviceToHost, st));
+    FRW_CK(cudaStreamSynchronize(st));
+    if (h) {
+        set_error("3-D grid: a lookup found no candidate list on any level");
+        return FRW_E_KERNEL;
+    }
+    return FRW_OK;
+}
+
 frw_status prepare_walk(const frw3_layout *L, int64_t target, uint64_t first, uint64_t walks, uint64_t seed,
                         const frw3_opts *o, Walk3Params *P, double *shell_used) {
     frw_status rc = check_opts3(o);
@@ -413,6 +426,9 @@ frw_status frw3_layout_info_get(const frw3_layout *L, frw3_layout_info *info) {
     info->max_list = L->grid.max_list;
     info->mean_list = L->grid.ncells ? (double)L->grid.entries / (double)L->grid.ncells : 0.0;
     info->build_ms = L->grid.build_ms;
+    info->levels = 1 + L->grid.nup;
+    info->deferred_cells = L->grid.deferred;
+    info->upper_entries = L->grid.up_entries;
     return FRW_OK;
 }
 
@@ -437,8 +453,7 @@ frw_status frw3_query_batch(const frw3_layout *L, const double *pts, int64_t n, 
     if (mem == FRW_MEM_DEVICE) {
         frw_status rc = launch_query3(L->dl, pts, n, clear, nearest, st);
         if (rc) return rc;
-        FRW_CK(cudaStreamSynchronize(st));
-        return FRW_OK;
+        return check_grid_status(L, st);
     }
     Scratch3 s(st);
     const size_t pb = (size_t)n * 24, cb = clear ? (size_t)n * 8 : 0, nbt = nearest ? (size_t)n * 8 : 0;
@@ -451,8 +466,7 @@ frw_status frw3_query_batch(const frw3_layout *L, const double *pts, int64_t n, 
     if (rc) return rc;
     if (clear) FRW_CK(cudaMemcpyAsync(clear, dc, cb, cudaMemcpyDeviceToHost, st));
     if (nearest) FRW_CK(cudaMemcpyAsync(nearest, dn, nbt, cudaMemcpyDeviceToHost, st));
-    FRW_CK(cudaStreamSynchronize(st));
-    return FRW_OK;
+    return check_grid_status(L, st);
 }
 
 void frw3_opts_default(frw3_opts *o) {
@@ -512,6 +526,8 @@ frw_status frw3_walk(const frw3_layout *L, int64_t target, uint64_t walks, uint6
         set_error("3-D walk kernel finished " + std::to_string(stats[3]) + " of " + std::to_string(walks) + " walks");
         return FRW_E_KERNEL;
     }
+    rc = check_grid_status(L, st);
+    if (rc) return rc;
     res->walks = walks;
     res->escaped = stats[0];
     res->aborted = stats[1];
@@ -592,7 +608,7 @@ frw_status frw3_walk_trace(const frw3_layout *L, int64_t target, uint64_t first_
         set_error("3-D walk kernel finished " + std::to_string(done) + " of " + std::to_string(walks) + " walks");
         return FRW_E_KERNEL;
     }
-    return FRW_OK;
+    return check_grid_status(L, st);
 }
 
 frw_status frw3_generate_layout(uint64_t seed, int64_t n, double domain, double zdomain, int32_t wmin, int32_t wmax,

@@ -18,17 +18,42 @@ namespace frw {
 // d_c <= the box's distance from the cell centre, sorted by d_c: a query
 // reads one 8-byte cell record and 32 bytes per candidate, and stops once
 // d_c - (h + margin) exceeds its best distance.
+//
+// A cell whose search would reach more than kRingCap3 rings of cells (it lies
+// far from every box) has no list of its own: its record holds kDefer3 and
+// its points are looked up in the next level, a grid of cells twice as
+// large with the same origin (cell i of level l lies in cell i >> 1 of level
+// l + 1).  Coarser levels build lists only for the cells that deferred
+// points reach; the top level (at most 2 kRingCap3 + 1 cells per axis) has
+// no cap.  So the build visits at most (2 kRingCap3 + 1)^3 bins per cell
+// however sparse the layout is.
+constexpr int kRingCap3 = 4;
+constexpr uint32_t kDefer3 = 0xFFFFFFFFu;
+constexpr int kMaxLevels3 = 16;
+constexpr uint32_t kSt3LevelChain = 1u;  // a lookup reached the top level without a list (never expected)
+
+struct Level3 {
+    const uint2 *cells;
+    const float4 *lists;
+    double ginv, hq;
+    int nx, ny, nz, pad;
+};
+
 struct Dev3Layout {
-    const uint2 *cells;    // [ncells] (first entry, entry count)
+    const uint2 *cells;    // [ncells] (first entry, entry count) or (0, kDefer3)
     const float4 *lists;   // [2 * entries]
-    double g0x, g0y, g0z;  // grid origin
+    double g0x, g0y, g0z;  // grid origin (every level)
     double ginv;           // 1 / cell side
     double hq;             // half a cell side + rounding margin
     int nx, ny, nz;
+    int nup;               // coarser levels
+    const Level3 *up;      // [nup] device array
+    uint32_t *status;      // kSt3* bits (device word of the layout)
     double b[6];           // bounds (x0,y0,z0,x1,y1,z1), open
 };
 
 struct Grid3Buffers {
+    // level 0
     uint2 *cells = nullptr;
     float4 *lists = nullptr;
     int64_t ncells = 0, entries = 0;
@@ -36,6 +61,14 @@ struct Grid3Buffers {
     double g0[3] = {0, 0, 0};
     double side = 0;
     double margin = 0;
+    // coarser levels (device buffers owned here) and their descriptors
+    int nup = 0;
+    uint2 *up_cells[kMaxLevels3] = {};
+    float4 *up_lists[kMaxLevels3] = {};
+    Level3 *up = nullptr;          // device copy of the descriptors
+    int64_t up_entries = 0;        // list entries of all coarser levels
+    int64_t deferred = 0;          // level-0 cells that defer
+    uint32_t *status = nullptr;
     int32_t max_list = 0;
     float build_ms = 0;
 };

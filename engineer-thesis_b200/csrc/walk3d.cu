@@ -45,6 +45,7 @@ struct Grid3 {
     double o[3];   // origin
     double side, inv, h, margin;
     int n[3];
+    int cap;       // largest search radius in rings (the top level: no cap)
 };
 
 __device__ __forceinline__ int cell_axis(double v, double o, double inv, int n) {
@@ -128,21 +129,37 @@ __device__ __forceinline__ void for_ring(const Grid3 &G, int cx, int cy, int cz,
 // bins: boxes in ring r are at least (2r - 1) h away), then every box within
 // R = D + 2h + margin, each counted once (in the first cell, in index order,
 // where its cell range meets the search cube) -- counted (kFill = false) or
-// written (kFill = true).
+// written (kFill = true).  A cell whose search needs more than G.cap rings
+// defers (flag 1) and marks its parent cell of the next level as needed;
+// cells outside `need` (when given) are unused (flag 2).
 template <bool kFill>
 __global__ void k3_cell_lists(const float *__restrict__ boxes, Grid3 G, const int64_t *__restrict__ bstart,
-                              const int32_t *__restrict__ items, int64_t ncells, int64_t *__restrict__ cnt,
+                              const int32_t *__restrict__ items, int64_t ncells, const uint8_t *__restrict__ need,
+                              uint8_t *__restrict__ flag, uint8_t *__restrict__ need_up, int upnx, int upny,
+                              unsigned long long *__restrict__ ndefer, int64_t *__restrict__ cnt,
                               const int64_t *__restrict__ lstart, float4 *__restrict__ lists) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncells) return;
+    if (kFill) {
+        if (flag[c]) return;
+    } else if (need && !need[c]) {
+        cnt[c] = 0;
+        flag[c] = 2;
+        return;
+    }
     const int cx = (int)(c % G.n[0]), cy = (int)((c / G.n[0]) % G.n[1]), cz = (int)(c / ((int64_t)G.n[0] * G.n[1]));
     const double px = __dadd_rn(G.o[0], __dmul_rn((double)cx + 0.5, G.side));
     const double py = __dadd_rn(G.o[1], __dmul_rn((double)cy + 0.5, G.side));
     const double pz = __dadd_rn(G.o[2], __dmul_rn((double)cz + 0.5, G.side));
     const int rlim = max(G.n[0], max(G.n[1], G.n[2]));
     double best = INFINITY;
+    bool defer = false;
     for (int r = 0; r <= rlim; r++) {
         if (r > 0 && __dmul_rn((double)(2 * r - 1), G.h) > __dadd_rn(best, G.margin)) break;
+        if (r > G.cap) {
+            defer = true;
+            break;
+        }
         for_ring(G, cx, cy, cz, r, [&](int64_t q) {
             for (int64_t k = bstart[q]; k < bstart[q + 1]; k++) {
                 float4 lo, hi;
@@ -153,7 +170,19 @@ __global__ void k3_cell_lists(const float *__restrict__ boxes, Grid3 G, const in
     }
     const double R = __dadd_rn(__dadd_rn(best, __dmul_rn(2.0, G.h)), G.margin);
     int rmax = 0;
-    while (rmax < rlim && __dmul_rn((double)(2 * rmax + 1), G.h) <= R) rmax++;
+    if (!defer) {
+        while (rmax < rlim && __dmul_rn((double)(2 * rmax + 1), G.h) <= R) rmax++;
+        defer = rmax > G.cap;
+    }
+    if (defer) {  // only the counting pass gets here: the fill skips flagged cells
+        if (!kFill) {
+            cnt[c] = 0;
+            flag[c] = 1;
+            atomicAdd(ndefer, 1ull);
+            if (need_up) need_up[((int64_t)(cz >> 1) * upny + (cy >> 1)) * upnx + (cx >> 1)] = 1;
+        }
+        return;
+    }
     const int s0[3] = {max(cx - rmax, 0), max(cy - rmax, 0), max(cz - rmax, 0)};
     const int s1[3] = {min(cx + rmax, G.n[0] - 1), min(cy + rmax, G.n[1] - 1), min(cz + rmax, G.n[2] - 1)};
     int64_t m = 0, out = kFill ? lstart[c] : 0;
@@ -190,13 +219,21 @@ __global__ void k3_cell_lists(const float *__restrict__ boxes, Grid3 G, const in
                     m++;
                 }
             }
-    if (!kFill) cnt[c] = m;
+    if (!kFill) {
+        cnt[c] = m;
+        flag[c] = 0;
+    }
 }
 
-__global__ void k3_cells_pack(const int64_t *__restrict__ lstart, const int64_t *__restrict__ cnt, int64_t ncells,
-                              uint2 *__restrict__ cells, unsigned long long *__restrict__ maxlen) {
+__global__ void k3_cells_pack(const int64_t *__restrict__ lstart, const int64_t *__restrict__ cnt,
+                              const uint8_t *__restrict__ flag, int64_t ncells, uint2 *__restrict__ cells,
+                              unsigned long long *__restrict__ maxlen) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncells) return;
+    if (flag[c]) {
+        cells[c] = make_uint2(0u, kDefer3);
+        return;
+    }
     cells[c] = make_uint2((uint32_t)lstart[c], (uint32_t)cnt[c]);
     atomicMax(maxlen, (unsigned long long)cnt[c]);
 }
@@ -207,16 +244,35 @@ __device__ __forceinline__ void nearest3(const Dev3Layout &L, double px, double 
     const int ix = cell_axis(px, L.g0x, L.ginv, L.nx);
     const int iy = cell_axis(py, L.g0y, L.ginv, L.ny);
     const int iz = cell_axis(pz, L.g0z, L.ginv, L.nz);
-    const uint2 cr = __ldg(L.cells + ((int64_t)iz * L.ny + iy) * L.nx + ix);
+    uint2 cr = __ldg(L.cells + ((int64_t)iz * L.ny + iy) * L.nx + ix);
+    const float4 *e = L.lists;
+    double hq = L.hq;
+    if (cr.y == kDefer3) {  // far from every box: the coarser levels
+        for (int l = 0; l < L.nup && cr.y == kDefer3; l++) {
+            const Level3 *V = L.up + l;
+            const double gi = __ldg(&V->ginv);
+            const int nx = __ldg(&V->nx), ny = __ldg(&V->ny), nz = __ldg(&V->nz);
+            const int jx = cell_axis(px, L.g0x, gi, nx), jy = cell_axis(py, L.g0y, gi, ny),
+                      jz = cell_axis(pz, L.g0z, gi, nz);
+            const uint2 *cells = (const uint2 *)__ldg((const unsigned long long *)&V->cells);
+            cr = __ldg(cells + ((int64_t)jz * ny + jy) * nx + jx);
+            e = (const float4 *)__ldg((const unsigned long long *)&V->lists);
+            hq = __ldg(&V->hq);
+        }
+        if (cr.y == kDefer3) {  // cannot happen by construction; reported, never looped on
+            atomicOr(L.status, kSt3LevelChain);
+            cr.y = 0;
+        }
+    }
     best = INFINITY;
     bid = 0x7FFFFFFF;
-    const float4 *e = L.lists + 2 * (size_t)cr.x;
+    e += 2 * (size_t)cr.x;
     for (uint32_t k = 0; k < cr.y; k++) {
         const float4 lo = __ldg(e + 2 * k), hi = __ldg(e + 2 * k + 1);
         // hi.w <= the entry's distance from the cell centre and the point is
-        // within L.hq of that centre: this entry and every later one are
+        // within hq of that centre: this entry and every later one are
         // farther than the best so far
-        if (__dsub_rn((double)hi.w, L.hq) > best) break;
+        if (__dsub_rn((double)hi.w, hq) > best) break;
         const double d = box_dist(px, py, pz, lo, hi);
         const int id = __float_as_int(lo.w);
         if (d < best || (d == best && id < bid)) {
@@ -473,6 +529,12 @@ __global__ void __launch_bounds__(kW3Threads, kW3MinBlocks) k_walk3(const Walk3P
 void free_grid3(Grid3Buffers *g, cudaStream_t st) {
     if (g->cells) cudaFreeAsync(g->cells, st);
     if (g->lists) cudaFreeAsync(g->lists, st);
+    for (int l = 0; l < kMaxLevels3; l++) {
+        if (g->up_cells[l]) cudaFreeAsync(g->up_cells[l], st);
+        if (g->up_lists[l]) cudaFreeAsync(g->up_lists[l], st);
+    }
+    if (g->up) cudaFreeAsync(g->up, st);
+    if (g->status) cudaFreeAsync(g->status, st);
     *g = Grid3Buffers();
 }
 
@@ -487,8 +549,104 @@ void attach_grid3(Dev3Layout &L, const Grid3Buffers &g, const double bounds[6]) 
     L.nx = g.nx;
     L.ny = g.ny;
     L.nz = g.nz;
+    L.nup = g.nup;
+    L.up = g.up;
+    L.status = g.status;
     for (int c = 0; c < 6; c++) L.b[c] = bounds[c];
 }
+
+namespace {
+
+// One level: bins, the count pass (lists, deferrals, the parents' needs),
+// the scan, the fill pass and the cell records.  need == nullptr: every cell.
+struct LevelOut {
+    uint2 *cells = nullptr;
+    float4 *lists = nullptr;
+    int64_t entries = 0, deferred = 0;
+    unsigned long long max_list = 0;
+};
+
+frw_status build_level(const float *d_boxes, int64_t n, const Grid3 &G, const uint8_t *need, uint8_t *need_up,
+                       int upnx, int upny, cudaStream_t st, LevelOut *out) {
+    const int64_t ncells = (int64_t)G.n[0] * G.n[1] * G.n[2];
+    int64_t *bcnt = nullptr, *bstart = nullptr, *lcnt = nullptr, *lstart = nullptr, *sums = nullptr,
+            *grand = nullptr;
+    int32_t *items = nullptr;
+    uint8_t *flag = nullptr;
+    unsigned long long *dev_stats = nullptr;  // [0] deferred cells, [1] longest list
+    const int64_t tiles = scan_i64_tiles(ncells + 1);
+    frw_status rc = FRW_OK;
+    auto ck = [&](cudaError_t e, const char *what) {
+        if (e != cudaSuccess && rc == FRW_OK) rc = cuda_fail(e, what);
+        return rc == FRW_OK;
+    };
+    do {
+        const size_t cb = (size_t)(ncells + 1) * 8;
+        if (!ck(cudaMallocAsync(&bcnt, cb, st), "malloc bin counts")) break;
+        if (!ck(cudaMallocAsync(&bstart, cb, st), "malloc bin starts")) break;
+        if (!ck(cudaMallocAsync(&lcnt, cb, st), "malloc list counts")) break;
+        if (!ck(cudaMallocAsync(&lstart, cb, st), "malloc list starts")) break;
+        if (!ck(cudaMallocAsync(&sums, (size_t)tiles * 8, st), "malloc tile sums")) break;
+        if (!ck(cudaMallocAsync(&grand, 16, st), "malloc totals")) break;
+        if (!ck(cudaMallocAsync(&flag, (size_t)ncells, st), "malloc flags")) break;
+        if (!ck(cudaMallocAsync(&dev_stats, 16, st), "malloc stats")) break;
+        if (!ck(cudaMallocAsync(&out->cells, (size_t)ncells * sizeof(uint2), st), "malloc cells")) break;
+        if (!ck(cudaMemsetAsync(bcnt, 0, cb, st), "memset")) break;
+        if (!ck(cudaMemsetAsync(lcnt, 0, cb, st), "memset")) break;
+        if (!ck(cudaMemsetAsync(dev_stats, 0, 16, st), "memset")) break;
+        const unsigned nb = (unsigned)((n + 255) / 256);
+        k3_bin_count<<<nb, 256, 0, st>>>(d_boxes, n, G, (unsigned long long *)bcnt);
+        launch_scan_i64(bcnt, ncells + 1, bstart, sums, grand, st);
+        if (!ck(cudaGetLastError(), "bin count")) break;
+        int64_t nitems = 0;
+        if (!ck(cudaMemcpyAsync(&nitems, grand, 8, cudaMemcpyDeviceToHost, st), "bin total")) break;
+        if (!ck(cudaStreamSynchronize(st), "bin total")) break;
+        if (nitems > INT32_MAX) {
+            set_error("build_grid3: more than 2^31 bin entries; use fewer cells per box");
+            rc = FRW_E_ARG;
+            break;
+        }
+        if (!ck(cudaMallocAsync(&items, (size_t)std::max<int64_t>(nitems, 1) * 4, st), "malloc bins")) break;
+        // the fill uses bcnt as its cursor: start it at the bin starts
+        if (!ck(cudaMemcpyAsync(bcnt, bstart, cb, cudaMemcpyDeviceToDevice, st), "cursor")) break;
+        k3_bin_fill<<<nb, 256, 0, st>>>(d_boxes, n, G, (unsigned long long *)bcnt, items);
+        const unsigned cbk = (unsigned)((ncells + 127) / 128);
+        k3_cell_lists<false><<<cbk, 128, 0, st>>>(d_boxes, G, bstart, items, ncells, need, flag, need_up, upnx, upny,
+                                                  dev_stats, lcnt, nullptr, nullptr);
+        launch_scan_i64(lcnt, ncells + 1, lstart, sums, grand + 1, st);
+        if (!ck(cudaGetLastError(), "cell count")) break;
+        int64_t total = 0;
+        unsigned long long ndef = 0;
+        if (!ck(cudaMemcpyAsync(&total, grand + 1, 8, cudaMemcpyDeviceToHost, st), "list total")) break;
+        if (!ck(cudaMemcpyAsync(&ndef, dev_stats, 8, cudaMemcpyDeviceToHost, st), "deferred")) break;
+        if (!ck(cudaStreamSynchronize(st), "list total")) break;
+        if (total > (int64_t)INT32_MAX) {
+            set_error("build_grid3: more than 2^31 list entries; use fewer cells per box");
+            rc = FRW_E_ARG;
+            break;
+        }
+        out->entries = total;
+        out->deferred = (int64_t)ndef;
+        if (!ck(cudaMallocAsync(&out->lists, (size_t)std::max<int64_t>(total, 1) * 32, st), "malloc lists")) break;
+        k3_cell_lists<true><<<cbk, 128, 0, st>>>(d_boxes, G, bstart, items, ncells, need, flag, nullptr, upnx, upny,
+                                                 nullptr, nullptr, lstart, out->lists);
+        k3_cells_pack<<<cbk, 128, 0, st>>>(lstart, lcnt, flag, ncells, out->cells, dev_stats + 1);
+        if (!ck(cudaGetLastError(), "cell fill")) break;
+        if (!ck(cudaMemcpyAsync(&out->max_list, dev_stats + 1, 8, cudaMemcpyDeviceToHost, st), "max list")) break;
+        if (!ck(cudaStreamSynchronize(st), "grid level")) break;
+    } while (0);
+    for (void *p : {(void *)bcnt, (void *)bstart, (void *)lcnt, (void *)lstart, (void *)sums, (void *)grand,
+                    (void *)items, (void *)flag, (void *)dev_stats})
+        if (p) cudaFreeAsync(p, st);
+    if (rc != FRW_OK) {
+        if (out->cells) cudaFreeAsync(out->cells, st);
+        if (out->lists) cudaFreeAsync(out->lists, st);
+        *out = LevelOut();
+    }
+    return rc;
+}
+
+}  // namespace
 
 frw_status build_grid3(const float *d_boxes, int64_t n, const double bounds[6], double cells_per_box,
                        cudaStream_t st, Grid3Buffers *out) {
@@ -518,7 +676,6 @@ frw_status build_grid3(const float *d_boxes, int64_t n, const double bounds[6], 
             break;
         side *= 1.25;
     }
-    const int64_t ncells = nc[0] * nc[1] * nc[2];
     Grid3 G;
     for (int c = 0; c < 3; c++) {
         G.o[c] = bounds[c];
@@ -532,80 +689,85 @@ frw_status build_grid3(const float *d_boxes, int64_t n, const double bounds[6], 
     Events ev(2);
     if (!ev.ok(2)) return cuda_fail(cudaErrorUnknown, "event create");
     Grid3Buffers B;
-    B.ncells = ncells;
+    B.ncells = nc[0] * nc[1] * nc[2];
     B.nx = G.n[0];
     B.ny = G.n[1];
     B.nz = G.n[2];
     for (int c = 0; c < 3; c++) B.g0[c] = G.o[c];
     B.side = side;
     B.margin = G.margin;
-    int64_t *bcnt = nullptr, *bstart = nullptr, *lcnt = nullptr, *lstart = nullptr, *sums = nullptr,
-            *grand = nullptr;
-    int32_t *items = nullptr;
-    unsigned long long *maxlen = nullptr;
-    const int64_t tiles = scan_i64_tiles(ncells + 1);
     frw_status rc = FRW_OK;
+    uint8_t *need = nullptr, *need_up = nullptr;
+    std::vector<Level3> up;
+    unsigned long long max_list = 0;
     auto ck = [&](cudaError_t e, const char *what) {
         if (e != cudaSuccess && rc == FRW_OK) rc = cuda_fail(e, what);
         return rc == FRW_OK;
     };
     do {
         if (!ck(cudaEventRecord(ev[0], st), "event")) break;
-        const size_t cb = (size_t)(ncells + 1) * 8;
-        if (!ck(cudaMallocAsync(&bcnt, cb, st), "malloc bin counts")) break;
-        if (!ck(cudaMallocAsync(&bstart, cb, st), "malloc bin starts")) break;
-        if (!ck(cudaMallocAsync(&lcnt, cb, st), "malloc list counts")) break;
-        if (!ck(cudaMallocAsync(&lstart, cb, st), "malloc list starts")) break;
-        if (!ck(cudaMallocAsync(&sums, (size_t)tiles * 8, st), "malloc tile sums")) break;
-        if (!ck(cudaMallocAsync(&grand, 16, st), "malloc totals")) break;
-        if (!ck(cudaMallocAsync(&maxlen, 8, st), "malloc max")) break;
-        if (!ck(cudaMallocAsync(&B.cells, (size_t)ncells * sizeof(uint2), st), "malloc cells")) break;
-        if (!ck(cudaMemsetAsync(bcnt, 0, cb, st), "memset")) break;
-        if (!ck(cudaMemsetAsync(lcnt, 0, cb, st), "memset")) break;
-        if (!ck(cudaMemsetAsync(maxlen, 0, 8, st), "memset")) break;
-        const unsigned nb = (unsigned)((n + 255) / 256);
-        k3_bin_count<<<nb, 256, 0, st>>>(d_boxes, n, G, (unsigned long long *)bcnt);
-        launch_scan_i64(bcnt, ncells + 1, bstart, sums, grand, st);
-        if (!ck(cudaGetLastError(), "bin count")) break;
-        int64_t nitems = 0;
-        if (!ck(cudaMemcpyAsync(&nitems, grand, 8, cudaMemcpyDeviceToHost, st), "bin total")) break;
-        if (!ck(cudaStreamSynchronize(st), "bin total")) break;
-        if (nitems > INT32_MAX) {
-            set_error("build_grid3: more than 2^31 bin entries; use fewer cells per box");
-            rc = FRW_E_ARG;
-            break;
+        if (!ck(cudaMallocAsync(&B.status, 4, st), "malloc status")) break;
+        if (!ck(cudaMemsetAsync(B.status, 0, 4, st), "memset")) break;
+        for (int l = 0; l < kMaxLevels3; l++) {
+            const bool top = std::max(G.n[0], std::max(G.n[1], G.n[2])) <= 2 * kRingCap3 + 1 || l == kMaxLevels3 - 1;
+            G.cap = top ? (1 << 28) : kRingCap3;
+            const int upnx = (G.n[0] + 1) / 2, upny = (G.n[1] + 1) / 2, upnz = (G.n[2] + 1) / 2;
+            const int64_t upcells = (int64_t)upnx * upny * upnz;
+            if (!top) {
+                if (!ck(cudaMallocAsync(&need_up, (size_t)upcells, st), "malloc needs")) break;
+                if (!ck(cudaMemsetAsync(need_up, 0, (size_t)upcells, st), "memset")) break;
+            }
+            LevelOut lo;
+            rc = build_level(d_boxes, n, G, need, top ? nullptr : need_up, upnx, upny, st, &lo);
+            if (rc != FRW_OK) break;
+            max_list = std::max(max_list, lo.max_list);
+            if (l == 0) {
+                B.cells = lo.cells;
+                B.lists = lo.lists;
+                B.entries = lo.entries;
+                B.deferred = lo.deferred;
+            } else {
+                B.up_cells[l - 1] = lo.cells;
+                B.up_lists[l - 1] = lo.lists;
+                B.up_entries += lo.entries;
+                Level3 V;
+                V.cells = lo.cells;
+                V.lists = lo.lists;
+                V.ginv = G.inv;
+                V.hq = G.h + 2.0 * G.margin;
+                V.nx = G.n[0];
+                V.ny = G.n[1];
+                V.nz = G.n[2];
+                V.pad = 0;
+                up.push_back(V);
+                B.nup = l;
+            }
+            if (need) cudaFreeAsync(need, st);
+            need = need_up;
+            need_up = nullptr;
+            if (top || lo.deferred == 0) break;
+            // the next level: cells twice as large, same origin
+            G.n[0] = upnx;
+            G.n[1] = upny;
+            G.n[2] = upnz;
+            G.side = std::ldexp(G.side, 1);
+            G.inv = std::ldexp(G.inv, -1);
+            G.h = std::ldexp(G.h, 1);
         }
-        if (!ck(cudaMallocAsync(&items, (size_t)std::max<int64_t>(nitems, 1) * 4, st), "malloc bins")) break;
-        // the fill uses bcnt as its cursor: start it at the bin starts
-        if (!ck(cudaMemcpyAsync(bcnt, bstart, cb, cudaMemcpyDeviceToDevice, st), "cursor")) break;
-        k3_bin_fill<<<nb, 256, 0, st>>>(d_boxes, n, G, (unsigned long long *)bcnt, items);
-        const unsigned cbk = (unsigned)((ncells + 127) / 128);
-        k3_cell_lists<false><<<cbk, 128, 0, st>>>(d_boxes, G, bstart, items, ncells, lcnt, nullptr, nullptr);
-        launch_scan_i64(lcnt, ncells + 1, lstart, sums, grand + 1, st);
-        if (!ck(cudaGetLastError(), "cell count")) break;
-        int64_t total = 0;
-        if (!ck(cudaMemcpyAsync(&total, grand + 1, 8, cudaMemcpyDeviceToHost, st), "list total")) break;
-        if (!ck(cudaStreamSynchronize(st), "list total")) break;
-        if (total > (int64_t)UINT32_MAX / 2) {
-            set_error("build_grid3: more than 2^31 list entries; use fewer cells per box");
-            rc = FRW_E_ARG;
-            break;
+        if (rc != FRW_OK) break;
+        if (!up.empty()) {
+            if (!ck(cudaMallocAsync(&B.up, up.size() * sizeof(Level3), st), "malloc levels")) break;
+            if (!ck(cudaMemcpyAsync(B.up, up.data(), up.size() * sizeof(Level3), cudaMemcpyHostToDevice, st),
+                    "levels"))
+                break;
         }
-        B.entries = total;
-        if (!ck(cudaMallocAsync(&B.lists, (size_t)std::max<int64_t>(total, 1) * 32, st), "malloc lists")) break;
-        k3_cell_lists<true><<<cbk, 128, 0, st>>>(d_boxes, G, bstart, items, ncells, nullptr, lstart, B.lists);
-        k3_cells_pack<<<cbk, 128, 0, st>>>(lstart, lcnt, ncells, B.cells, maxlen);
-        if (!ck(cudaGetLastError(), "cell fill")) break;
-        unsigned long long ml = 0;
-        if (!ck(cudaMemcpyAsync(&ml, maxlen, 8, cudaMemcpyDeviceToHost, st), "max list")) break;
         if (!ck(cudaEventRecord(ev[1], st), "event")) break;
         if (!ck(cudaEventSynchronize(ev[1]), "grid sync")) break;
-        B.max_list = (int32_t)ml;
+        B.max_list = (int32_t)max_list;
         cudaEventElapsedTime(&B.build_ms, ev[0], ev[1]);
     } while (0);
-    for (void *p : {(void *)bcnt, (void *)bstart, (void *)lcnt, (void *)lstart, (void *)sums, (void *)grand,
-                    (void *)items, (void *)maxlen})
-        if (p) cudaFreeAsync(p, st);
+    if (need) cudaFreeAsync(need, st);
+    if (need_up) cudaFreeAsync(need_up, st);
     if (rc != FRW_OK) {
         free_grid3(&B, st);
         return rc;

@@ -210,6 +210,9 @@ class Layout3Info(C.Structure):
         ("max_list", C.c_int32),
         ("mean_list", C.c_double),
         ("build_ms", C.c_float),
+        ("levels", C.c_int32),
+        ("deferred_cells", C.c_int64),
+        ("upper_entries", C.c_int64),
     ]
 
 

@@ -59,6 +59,9 @@ frw_status frw3_deriv_green_cube(double a, double eta, double dzeta, double dg[3
 /* ---- layouts ---- */
 /* boxes: host array of n*6 floats (x0,y0,z0,x1,y1,z1), x0 < x1, y0 < y1,
  * z0 < z1, interiors pairwise disjoint (checked; touching faces allowed).
+ * The device grid has cells_per_box x n cells; cells far from every box
+ * (empty regions, wide bounds) defer to coarser grids, so the build visits a
+ * bounded number of bins per cell however sparse the layout is.
  * bounds: 6 doubles (x0,y0,z0,x1,y1,z1) or NULL for the bounding box grown
  * by int(0.01 * x extent) on every side (the 2-D reader's rule,
  * CPU/Parser.cpp:51-87).  cells_per_box: cell-grid density (<= 0: 8). */
@@ -82,6 +85,9 @@ typedef struct frw3_layout_info {
     int32_t max_list;       /* longest list */
     double mean_list;       /* mean list length over cells */
     float build_ms;         /* device time of the grid build */
+    int32_t levels;         /* grid levels: 1 + the coarser levels that far cells defer to */
+    int64_t deferred_cells; /* finest-level cells far from every box (looked up one level up) */
+    int64_t upper_entries;  /* list entries of the coarser levels */
 } frw3_layout_info;
 frw_status frw3_layout_info_get(const frw3_layout *layout, frw3_layout_info *info);
 /* The layout's boxes (n*6 floats, input order). */

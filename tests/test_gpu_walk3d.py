@@ -52,6 +52,34 @@ def test_query3_bit_exact(n, cells):
     assert info.max_list >= 1 and info.list_entries >= info.grid[0] * info.grid[1] * info.grid[2]
 
 
+@pytest.mark.parametrize("case", ["two_clusters", "wide_bounds"])
+def test_query3_sparse_layouts_use_coarser_levels(case):
+    """Layouts with large empty regions: cells far from every box defer to
+    coarser grid levels (bounded build work); queries and walks still equal
+    the oracle's everywhere, far points included."""
+    a = _layout(0xF4A7 + 60, 1500, 300.0, 300.0)
+    if case == "two_clusters":
+        b = np.vstack([a, _layout(0xF4A7 + 61, 1500, 300.0, 300.0) + np.float32(1700)])
+        bounds = None
+    else:
+        b = a
+        bounds = np.array([-5000.0, -5000.0, -5000.0, 5300.0, 5300.0, 5300.0])
+    B = O.Boxes3(b, bounds, grid=True)
+    rng = np.random.default_rng(17)
+    pts = _hard_points(b, B.bounds, rng, 20000)
+    with frw.Layout3.from_boxes(b, bounds) as L:
+        info = L.info
+        d, k = L.query(pts)
+        e, h, bb, w = L.walk_trace(0, 0, 3000, 23)
+    assert info.levels > 1 and info.deferred_cells > 0 and info.build_ms < 1000
+    d_o, k_o = B.nearest(pts)
+    assert np.array_equal(d, d_o) and np.array_equal(k, k_o)
+    assert (d > 500).sum() > 100  # far points were exercised
+    e_o, h_o, b_o, w_o = B.walks(B.cfg(target=0, seed=23), 0, 3000)
+    assert np.array_equal(e, e_o) and np.array_equal(h, h_o) and np.array_equal(bb, b_o)
+    assert _bits_equal(w, w_o)
+
+
 def test_query3_touching_and_explicit_bounds():
     # two boxes sharing a face, a third far away; explicit bounds
     b = np.array([[0, 0, 0, 10, 10, 10], [10, 0, 0, 20, 10, 10], [100, 100, 100, 101, 103, 107]], np.float32)
