@@ -57,13 +57,14 @@ def test_query3_sparse_layouts_use_coarser_levels(case):
     """Layouts with large empty regions: cells far from every box defer to
     coarser grid levels (bounded build work); queries and walks still equal
     the oracle's everywhere, far points included."""
-    a = _layout(0xF4A7 + 60, 1500, 300.0, 300.0)
+    a = frw.generate_layout3(0xF4A7 + 60, 1500, 400.0, 400.0, 5, 30, 5, 30, 2)
     if case == "two_clusters":
-        b = np.vstack([a, _layout(0xF4A7 + 61, 1500, 300.0, 300.0) + np.float32(1700)])
+        c = frw.generate_layout3(0xF4A7 + 61, 1500, 400.0, 400.0, 5, 30, 5, 30, 2)
+        b = np.vstack([a, c + np.float32(2600)])
         bounds = None
     else:
         b = a
-        bounds = np.array([-5000.0, -5000.0, -5000.0, 5300.0, 5300.0, 5300.0])
+        bounds = np.array([-5000.0, -5000.0, -5000.0, 5400.0, 5400.0, 5400.0])
     B = O.Boxes3(b, bounds, grid=True)
     rng = np.random.default_rng(17)
     pts = _hard_points(b, B.bounds, rng, 20000)
