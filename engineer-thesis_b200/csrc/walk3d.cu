@@ -125,6 +125,41 @@ __device__ __forceinline__ void for_ring(const Grid3 &G, int cx, int cy, int cz,
         }
 }
 
+// List entries (pairs of float4) ordered by (d_c in hi.w, box index in lo.w).
+__device__ __forceinline__ bool entry_less(const float4 *e, int64_t a, int64_t b) {
+    const float ka = e[2 * a + 1].w, kb = e[2 * b + 1].w;
+    return ka < kb || (ka == kb && __float_as_int(e[2 * a].w) < __float_as_int(e[2 * b].w));
+}
+__device__ __forceinline__ void entry_swap(float4 *e, int64_t a, int64_t b) {
+    const float4 lo = e[2 * a], hi = e[2 * a + 1];
+    e[2 * a] = e[2 * b];
+    e[2 * a + 1] = e[2 * b + 1];
+    e[2 * b] = lo;
+    e[2 * b + 1] = hi;
+}
+__device__ __forceinline__ void sift_down(float4 *e, int64_t root, int64_t end) {
+    for (int64_t c = 2 * root + 1; c < end; c = 2 * root + 1) {
+        if (c + 1 < end && entry_less(e, c, c + 1)) c++;
+        if (!entry_less(e, root, c)) return;
+        entry_swap(e, root, c);
+        root = c;
+    }
+}
+// One thread's list, in place: insertion for short lists (the usual case),
+// heapsort for the long ones of coarse cells facing a dense cluster.
+__device__ void sort_entries(float4 *e, int64_t m) {
+    if (m <= 32) {
+        for (int64_t a = 1; a < m; a++)
+            for (int64_t b = a; b > 0 && entry_less(e, b, b - 1); b--) entry_swap(e, b, b - 1);
+        return;
+    }
+    for (int64_t r = m / 2 - 1; r >= 0; r--) sift_down(e, r, m);
+    for (int64_t end = m - 1; end > 0; end--) {
+        entry_swap(e, 0, end);
+        sift_down(e, 0, end);
+    }
+}
+
 // Per cell: the nearest-box distance D of its centre (ring search over the
 // bins: boxes in ring r are at least (2r - 1) h away), then every box within
 // R = D + 2h + margin, each counted once (in the first cell, in index order,
@@ -201,24 +236,16 @@ __global__ void k3_cell_lists(const float *__restrict__ boxes, Grid3 G, const in
                     if (fx != x || fy != y || fz != z) continue;
                     if (box_dist(px, py, pz, lo, hi) > R) continue;
                     if (kFill) {
-                        // insertion by (distance from the centre, index): a
-                        // query stops at the first entry that cannot win
-                        const double dc = box_dist(px, py, pz, lo, hi);
-                        hi.w = __double2float_rd(dc);
-                        int64_t at = out + m;
-                        while (at > out) {
-                            const float4 plo = lists[2 * (at - 1)], phi = lists[2 * (at - 1) + 1];
-                            if (phi.w < hi.w || (phi.w == hi.w && __float_as_int(plo.w) < i)) break;
-                            lists[2 * at] = plo;
-                            lists[2 * at + 1] = phi;
-                            at--;
-                        }
-                        lists[2 * at] = lo;
-                        lists[2 * at + 1] = hi;
+                        hi.w = __double2float_rd(box_dist(px, py, pz, lo, hi));
+                        lists[2 * (out + m)] = lo;
+                        lists[2 * (out + m) + 1] = hi;
                     }
                     m++;
                 }
             }
+    // order by (distance from the centre, index): a query stops at the first
+    // entry that cannot win
+    if (kFill) sort_entries(lists + 2 * out, m);
     if (!kFill) {
         cnt[c] = m;
         flag[c] = 0;
