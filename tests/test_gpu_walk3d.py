@@ -111,6 +111,42 @@ def test_walk3_trace_bit_exact(nsample, offset, first, stream):
     assert (e == 7).mean() > 0.5 and (e == frw.END_ABORTED).sum() == 0
 
 
+def test_walk3_trace_max_table_and_launch_shapes():
+    """The largest cube table (n = 100: 60,000 bins) and every launch shape
+    give the same walks: results depend only on (seed, stream, walk index)."""
+    b = _layout(0xF4A7 + 56, 250, 900.0, 300.0)
+    B = O.Boxes3(b)
+    e_o, h_o, b_o, w_o = B.walks(B.cfg(target=4, seed=31, nsample=100), 5, 3000)
+    with frw.Layout3.from_boxes(b) as L:
+        for bps, rm in ((0, 4), (1, 1), (2, 32), (4, 0)):
+            o = frw.opts3(nsample=100, blocks_per_sm=bps, refill_min=rm)
+            e, h, b1, w = L.walk_trace(4, 5, 3000, 31, o)
+            assert np.array_equal(e, e_o) and np.array_equal(h, h_o) and np.array_equal(b1, b_o), (bps, rm)
+            assert _bits_equal(w, w_o)
+            r = L.walk(4, 3000, 31, frw.opts3(nsample=100, blocks_per_sm=bps, refill_min=rm, first_walk=5))
+            ks, cnt = np.unique(e_o[e_o >= 0], return_counts=True)
+            assert np.array_equal(r.conductor, ks) and np.array_equal(r.hits, cnt)
+    assert b_o.max() >= 30_000  # bins of the later faces were drawn
+
+
+def test_query3_device_memory():
+    """frw3_query_batch on device arrays (torch tensors) equals the host call."""
+    import torch
+
+    b = _layout(0xF4A7 + 57, 800, 1200.0, 300.0)
+    rng = np.random.default_rng(8)
+    with frw.Layout3.from_boxes(b) as L:
+        bd = L.bounds
+        pts = bd[:3] + rng.random((50_000, 3)) * (bd[3:] - bd[:3])
+        d_h, k_h = L.query(pts)
+        pt = torch.as_tensor(pts, device="cuda")
+        d = torch.empty(len(pts), dtype=torch.float64, device="cuda")
+        k = torch.empty(len(pts), dtype=torch.int64, device="cuda")
+        L.query_device(pt, d, k)
+        torch.cuda.synchronize()
+    assert _bits_equal(d.cpu().numpy(), d_h) and np.array_equal(k.cpu().numpy(), k_h)
+
+
 def test_walk3_trace_hop_cap_and_shell():
     b = _layout(0xF4A7 + 51, 120, 500.0, 150.0)
     B = O.Boxes3(b)
