@@ -555,6 +555,35 @@ frw_status frw3_walk(const frw3_layout *L, int64_t target, uint64_t walks, uint6
     return FRW_OK;
 }
 
+frw_status frw3_walk_device(const frw3_layout *L, int64_t target, uint64_t walks, uint64_t seed, const frw3_opts *opts,
+                            uint64_t *hits, double *sum_w, double *sum_w2, uint64_t *stats, uint32_t *status,
+                            void *stream) {
+    if (!L || !hits || !sum_w || !sum_w2 || !stats || !status) {
+        set_error("frw3_walk_device: null argument");
+        return FRW_E_ARG;
+    }
+    frw3_opts o;
+    frw3_opts_default(&o);
+    if (opts) o = *opts;
+    Walk3Params P;
+    double shell;
+    frw_status rc = prepare_walk(L, target, o.first_walk, walks, seed, &o, &P, &shell);
+    if (rc) return rc;
+    if (walks == 0) return FRW_OK;
+    Dev3Guard g(L->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    Scratch3 s(st);
+    FRW_CK(cudaMallocAsync(&s.p, 8, st));
+    FRW_CK(cudaMemsetAsync(s.p, 0, 8, st));
+    P.counter = (unsigned long long *)s.p;
+    P.hits = (unsigned long long *)hits;
+    P.sum_w = sum_w;
+    P.sum_w2 = sum_w2;
+    P.stats = (unsigned long long *)stats;
+    P.L.status = status;  // lookup failures go to the caller's word
+    return launch_walk3(P, walk_blocks(L->device, o.blocks_per_sm), st);
+}
+
 frw_status frw3_walk_trace(const frw3_layout *L, int64_t target, uint64_t first_walk, uint64_t walks, uint64_t seed,
                            const frw3_opts *o, int64_t *end, int32_t *hops, int32_t *bin1, double *weight, int mem,
                            void *stream) {

@@ -275,6 +275,8 @@ _SIGS = {
     "frw3_query_batch": ([_VP, _VP, C.c_int64, _VP, _VP, C.c_int, _VP], C.c_int),
     "frw3_opts_default": ([C.POINTER(Opts3)], None),
     "frw3_walk": ([_VP, C.c_int64, C.c_uint64, C.c_uint64, C.POINTER(Opts3), C.POINTER(Result3), _VP], C.c_int),
+    "frw3_walk_device": ([_VP, C.c_int64, C.c_uint64, C.c_uint64, C.POINTER(Opts3), _VP, _VP, _VP, _VP, _VP, _VP],
+                         C.c_int),
     "frw3_walk_trace": ([_VP, C.c_int64, C.c_uint64, C.c_uint64, C.c_uint64, C.POINTER(Opts3), _VP, _VP, _VP,
                          _VP, C.c_int, _VP], C.c_int),
     "frw3_generate_layout": ([C.c_uint64, C.c_int64, C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_int32,
@@ -837,6 +839,15 @@ class Layout3:
         m = min(r.n_entries, cap)
         return WalkResult(r.walks, r.escaped, r.aborted, r.hops_total, np.array(r.gauss[:]), r.fraction_other,
                           r.kernel_ms, cond[:m], hits[:m], c[:m], se[:m], s1[:m], s2[:m], {"shell": r.shell})
+
+    def walk_device(self, target: int, walks: int, seed: int, o: Opts3 | None, hits, sum_w, sum_w2, stats, status,
+                    stream: int = 0):
+        """frw3_walk_device on torch CUDA tensors (uint64/float64 rows of n
+        entries, uint64 stats[4], int32 status[1]); stream-ordered, no sync."""
+        _check(lib().frw3_walk_device(self._h, target, walks, seed, C.byref(o) if o else None,
+                                      C.c_void_p(hits.data_ptr()), C.c_void_p(sum_w.data_ptr()),
+                                      C.c_void_p(sum_w2.data_ptr()), C.c_void_p(stats.data_ptr()),
+                                      C.c_void_p(status.data_ptr()), stream or None))
 
     def walk_trace(self, target: int, first: int, walks: int, seed: int, o: Opts3 | None = None):
         o = o or opts3()

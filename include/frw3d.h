@@ -137,6 +137,18 @@ typedef struct frw3_result {
  * launch configuration. */
 frw_status frw3_walk(const frw3_layout *layout, int64_t target, uint64_t walks, uint64_t seed,
                      const frw3_opts *opts, frw3_result *result, void *stream);
+/* The same walks accumulated into caller-owned DEVICE arrays on the layout's
+ * device, stream-ordered, without host synchronisation (the 3-D twin of
+ * frw_walk_device): for every box k (arrays of n entries) hits[k] += walks
+ * ending on k, sum_w[k] += their weights, sum_w2[k] += the squared weights;
+ * stats[0..3] += escaped, aborted, clearance queries, walks done;
+ * *status |= grid lookup failure bits (never expected; nonzero: treat as
+ * FRW_E_KERNEL).  The caller clears the arrays once; runs over disjoint walk
+ * ranges add up, and so do the arrays of several devices (one all-reduce).
+ * A walk counter comes from the device's stream-ordered memory pool. */
+frw_status frw3_walk_device(const frw3_layout *layout, int64_t target, uint64_t walks, uint64_t seed,
+                            const frw3_opts *opts, uint64_t *hits, double *sum_w, double *sum_w2, uint64_t *stats,
+                            uint32_t *status, void *stream);
 /* Per-walk records (arrays of `walks` entries, any may be NULL): end box
  * (-1 escaped, -2 aborted), clearance queries, first-hop bin (-1 none) and
  * the capacitance weight c. */

@@ -179,6 +179,37 @@ def test_walk3_rows_match_oracle():
     assert r.extra["shell"] == B.shell
 
 
+def test_walk3_device_rows_match_host_rows():
+    """frw3_walk_device accumulates into device arrays without a host sync;
+    two calls over disjoint walk ranges equal one frw3_walk over their union."""
+    import torch
+
+    b = _layout(0xF4A7 + 58, 600, 1200.0, 300.0)
+    n = len(b)
+    with frw.Layout3.from_boxes(b) as L:
+        ref = L.walk(9, 200_000, 0xD3)
+        hits = torch.zeros(n, dtype=torch.int64, device="cuda")
+        sw = torch.zeros(n, dtype=torch.float64, device="cuda")
+        sw2 = torch.zeros(n, dtype=torch.float64, device="cuda")
+        stats = torch.zeros(4, dtype=torch.int64, device="cuda")
+        status = torch.zeros(1, dtype=torch.int32, device="cuda")
+        L.walk_device(9, 120_000, 0xD3, frw.opts3(first_walk=0), hits, sw, sw2, stats, status)
+        L.walk_device(9, 80_000, 0xD3, frw.opts3(first_walk=120_000), hits, sw, sw2, stats, status)
+        L.walk_device(9, 0, 0xD3, None, hits, sw, sw2, stats, status)  # zero walks: nothing added
+        torch.cuda.synchronize()
+        with pytest.raises(frw.FrwError) as e:
+            L.walk_device(n, 10, 1, None, hits, sw, sw2, stats, status)
+        assert e.value.status == frw.E_ARG
+    h = hits.cpu().numpy()
+    k = np.nonzero(h)[0]
+    assert np.array_equal(k, ref.conductor) and np.array_equal(h[k], ref.hits)
+    np.testing.assert_allclose(sw.cpu().numpy()[k], ref.sum_w, rtol=1e-12, atol=1e-12 * np.abs(ref.sum_w).max())
+    np.testing.assert_allclose(sw2.cpu().numpy()[k], ref.sum_w2, rtol=1e-12)
+    st = stats.cpu().numpy()
+    assert st[3] == 200_000 and st[0] == ref.escaped and st[1] == ref.aborted and st[2] == ref.hops_total
+    assert int(status.cpu()[0]) == 0
+
+
 def test_walk3_disjoint_ranges_add_up():
     b = _layout(0xF4A7 + 53, 200, 800.0, 250.0)
     with frw.Layout3.from_boxes(b) as L:
