@@ -216,6 +216,7 @@ frw_status prepare_walk(const frw3_layout *L, int64_t target, uint64_t first, ui
         P->magic_nn = (uint32_t)((((uint64_t)1 << 32) + (uint64_t)(T->n * T->n) - 1) / (uint64_t)(T->n * T->n));
     }
     P->refill_min = o->refill_min < 1 ? 1 : (o->refill_min > 32 ? 32 : o->refill_min);
+    P->start_strata = o->start_strata;
     const float *tb = L->boxes.data() + 6 * target;
     for (int c = 0; c < 3; c++) {
         P->G[c] = (double)tb[c] - o->gauss_offset;
@@ -481,6 +482,7 @@ void frw3_opts_default(frw3_opts *o) {
     o->first_walk = 0;
     o->blocks_per_sm = 0;
     o->refill_min = 4;
+    o->start_strata = 0;
 }
 
 frw_status frw3_walk(const frw3_layout *L, int64_t target, uint64_t walks, uint64_t seed, const frw3_opts *o,

@@ -96,6 +96,7 @@ struct Walk3Params {
     int n, nb;
     uint32_t magic_n, magic_nn;  // ceil(2^32 / n), ceil(2^32 / n^2) (n > 1)
     int refill_min;              // refill idle lanes once this many are idle (1..32)
+    uint32_t start_strata;       // 0 = off; S: walk w starts in stratum w mod S
     double G[6];  // Gaussian box
     double S;     // its area
     int64_t target;

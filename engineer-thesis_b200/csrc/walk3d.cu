@@ -360,7 +360,10 @@ __device__ __forceinline__ void start_walk(const Walk3Params &P, Walker &W, uint
     W.idx = j;
     W.rnd = block3(P, P.first + j, 0);
     W.rblk = 0;
-    const double u0 = (double)W.rnd.x * 0x1p-32, u1 = (double)W.rnd.y * 0x1p-32;
+    double u0 = (double)W.rnd.x * 0x1p-32;
+    const double u1 = (double)W.rnd.y * 0x1p-32;
+    if (P.start_strata)  // stratum (walk mod S) of the surface, by the first uniform
+        u0 = __ddiv_rn(__dadd_rn((double)(uint32_t)((P.first + j) % P.start_strata), u0), (double)P.start_strata);
     const double *G = P.G;
     const double w = __dsub_rn(G[3], G[0]), h = __dsub_rn(G[4], G[1]), d = __dsub_rn(G[5], G[2]);
     const double axy = __dmul_rn(w, h), axz = __dmul_rn(w, d), ayz = __dmul_rn(h, d);

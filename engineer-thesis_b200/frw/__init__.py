@@ -174,6 +174,7 @@ class Opts3(C.Structure):
         ("first_walk", C.c_uint64),
         ("blocks_per_sm", C.c_int32),
         ("refill_min", C.c_int32),
+        ("start_strata", C.c_uint32),
     ]
 
 
@@ -721,7 +722,7 @@ def deriv_green_cube(a: float, eta: float, dzeta: float) -> np.ndarray:
 
 
 def opts3(gauss_offset=1.0, shell=0.0, hop_cap=100000, permittivity=PERMITTIVITY, stream_id=0, nsample=NSAMPLE3,
-          first_walk=0, blocks_per_sm=0, refill_min=4) -> Opts3:
+          first_walk=0, blocks_per_sm=0, refill_min=4, start_strata=0) -> Opts3:
     o = Opts3()
     lib().frw3_opts_default(C.byref(o))
     o.gauss_offset = gauss_offset
@@ -733,6 +734,7 @@ def opts3(gauss_offset=1.0, shell=0.0, hop_cap=100000, permittivity=PERMITTIVITY
     o.first_walk = first_walk
     o.blocks_per_sm = blocks_per_sm
     o.refill_min = refill_min
+    o.start_strata = start_strata
     return o
 
 

@@ -113,6 +113,11 @@ typedef struct frw3_opts {
     int32_t blocks_per_sm; /* 0: library choice */
     int32_t refill_min;    /* a warp starts new walks once this many lanes are idle (default 4; 0 or 1: at
                               once; <= 32).  Results do not depend on it. */
+    uint32_t start_strata; /* 0 = off; S > 0: walk w starts in stratum w mod S of the Gaussian surface (its
+                              first uniform u0 becomes (w mod S + u0) / S, which orders the surface by
+                              face and position), as frw_opts.start_strata does in 2-D.  Unbiased when the
+                              walk range covers every stratum equally; the reported standard error stays the
+                              i.i.d. one, an upper bound. */
 } frw3_opts;
 void frw3_opts_default(frw3_opts *opts);
 

@@ -442,6 +442,8 @@ int oc3_walk_run(const double *boxes, int64_t n, const double bounds[6], const o
     for (uint64_t k = 0; k < count; k++) {
         uint64_t wk = first + k;
         double u0 = draw32(cfg->seed, cfg->stream, wk, 0) * (1.0 / 4294967296.0);
+        if (cfg->start_strata)
+            u0 = ((double)(uint32_t)(wk % cfg->start_strata) + u0) / (double)cfg->start_strata;
         double u1 = draw32(cfg->seed, cfg->stream, wk, 1) * (1.0 / 4294967296.0);
         double p[3], sgn;
         int axis;

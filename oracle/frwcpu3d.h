@@ -78,6 +78,7 @@ typedef struct oc3_cfg {
     uint64_t seed;
     uint32_t stream;
     int nsample;         /* cube table resolution n (6 n^2 bins) */
+    uint32_t start_strata; /* 0 = off; S > 0: walk w starts in stratum w mod S of the surface */
 } oc3_cfg;
 
 /* Walks first .. first+count-1 (grid may be NULL: brute force).  Per walk:

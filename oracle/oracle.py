@@ -71,6 +71,7 @@ class Cfg3(C.Structure):
         ("seed", C.c_uint64),
         ("stream", C.c_uint32),
         ("nsample", C.c_int),
+        ("start_strata", C.c_uint32),
     ]
 
 
@@ -489,9 +490,10 @@ class Boxes3:
         lib().oc3_query_batch(_p(self.boxes), self.n, g, _p(p), len(p), _p(d), _p(k, _I64))
         return d, k
 
-    def cfg(self, target=0, offset=1.0, shell=None, hop_cap=100000, seed=0, stream=0, nsample=NSAMPLE3):
+    def cfg(self, target=0, offset=1.0, shell=None, hop_cap=100000, seed=0, stream=0, nsample=NSAMPLE3,
+            start_strata=0):
         return Cfg3(target, offset, self.shell if shell is None else shell, hop_cap, PERMITTIVITY, seed, stream,
-                    nsample)
+                    nsample, start_strata)
 
     def walks(self, cfg: Cfg3, first: int, count: int):
         end = np.zeros(count, dtype=np.int64)

@@ -210,6 +210,23 @@ def test_walk3_device_rows_match_host_rows():
     assert int(status.cpu()[0]) == 0
 
 
+def test_walk3_stratified_start_bit_exact_and_unbiased():
+    """start_strata: walks equal the oracle's; C_00 agrees with unstratified
+    runs within errors and its spread over seeds is no larger."""
+    b = _layout(0xF4A7 + 59, 300, 900.0, 300.0)
+    B = O.Boxes3(b)
+    e_o, h_o, b_o, w_o = B.walks(B.cfg(target=2, seed=41, start_strata=64), 1 << 33, 3000)
+    with frw.Layout3.from_boxes(b) as L:
+        e, h, b1, w = L.walk_trace(2, 1 << 33, 3000, 41, frw.opts3(start_strata=64))
+        assert np.array_equal(e, e_o) and np.array_equal(h, h_o) and np.array_equal(b1, b_o)
+        assert _bits_equal(w, w_o)
+        n, S = 1 << 16, 1024
+        plain = np.array([L.walk(2, n, 100 + k).row(2)[1] for k in range(24)])
+        strat = np.array([L.walk(2, n, 100 + k, frw.opts3(start_strata=S)).row(2)[1] for k in range(24)])
+    assert abs(plain.mean() - strat.mean()) <= 4 * np.hypot(plain.std(ddof=1), strat.std(ddof=1)) / np.sqrt(24)
+    assert strat.std(ddof=1) <= 1.25 * plain.std(ddof=1)
+
+
 def test_walk3_disjoint_ranges_add_up():
     b = _layout(0xF4A7 + 53, 200, 800.0, 250.0)
     with frw.Layout3.from_boxes(b) as L:
