@@ -586,6 +586,125 @@ frw_status frw3_walk_device(const frw3_layout *L, int64_t target, uint64_t walks
     return launch_walk3(P, walk_blocks(L->device, o.blocks_per_sm), st);
 }
 
+frw_status frw3_walk_batch(const frw3_layout *L, const int64_t *targets, int32_t ntargets, uint64_t walks_per_target,
+                           uint64_t seed, const frw3_opts *opts, frw3_result *results, void *stream) {
+    if (!L || !targets || !results || ntargets < 1) {
+        set_error("frw3_walk_batch: null argument or no targets");
+        return FRW_E_ARG;
+    }
+    const int64_t n = L->n;
+    if ((int64_t)ntargets * n > (int64_t(1) << 27)) {
+        set_error("frw3_walk_batch: targets x boxes must stay below 2^27 (rows of every target are kept)");
+        return FRW_E_ARG;
+    }
+    if (walks_per_target && (uint64_t)ntargets > UINT64_MAX / walks_per_target) {
+        set_error("frw3_walk_batch: walk count overflows");
+        return FRW_E_ARG;
+    }
+    frw3_opts o;
+    frw3_opts_default(&o);
+    if (opts) o = *opts;
+    Walk3Params P;
+    double shell;
+    // validates the options and the first target; builds the shared parameters
+    frw_status rc = prepare_walk(L, targets[0], o.first_walk, walks_per_target, seed, &o, &P, &shell);
+    if (rc) return rc;
+    std::vector<Job3> jobs((size_t)ntargets);
+    for (int32_t t = 0; t < ntargets; t++) {
+        const int64_t k = targets[t];
+        if (k < 0 || k >= n) {
+            set_error("frw3_walk_batch: target " + std::to_string(t) + " out of range");
+            return FRW_E_ARG;
+        }
+        const float *tb = L->boxes.data() + 6 * k;
+        for (int c = 0; c < 3; c++) {
+            jobs[t].G[c] = (double)tb[c] - o.gauss_offset;
+            jobs[t].G[3 + c] = (double)tb[3 + c] + o.gauss_offset;
+        }
+        const double gw = jobs[t].G[3] - jobs[t].G[0], gh = jobs[t].G[4] - jobs[t].G[1],
+                     gd = jobs[t].G[5] - jobs[t].G[2];
+        jobs[t].S = 2.0 * (gw * gh) + 2.0 * (gw * gd) + 2.0 * (gh * gd);
+        jobs[t].target = k;
+    }
+    Dev3Guard g(L->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    const uint64_t total = (uint64_t)ntargets * walks_per_target;
+    // scratch: counter | stats[4 T] | hits[T n] | sum_w[T n] | sum_w2[T n] | jobs
+    const size_t nrow = (size_t)ntargets * (size_t)n;
+    const size_t words = 1 + 4 * (size_t)ntargets + 3 * nrow;
+    const size_t bytes = words * 8 + jobs.size() * sizeof(Job3);
+    Scratch3 s(st);
+    FRW_CK(cudaMallocAsync(&s.p, bytes, st));
+    FRW_CK(cudaMemsetAsync(s.p, 0, words * 8, st));
+    unsigned long long *u = (unsigned long long *)s.p;
+    Job3 *d_jobs = (Job3 *)(u + words);
+    FRW_CK(cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(Job3), cudaMemcpyHostToDevice, st));
+    P.counter = u;
+    P.stats = u + 1;
+    P.hits = u + 1 + 4 * ntargets;
+    P.sum_w = (double *)(P.hits + nrow);
+    P.sum_w2 = P.sum_w + nrow;
+    P.jobs = d_jobs;
+    P.walks_per_job = walks_per_target;
+    P.nboxes = n;
+    P.walks = total;
+    Events ev(2);
+    if (!ev.ok(2)) return cuda_fail(cudaErrorUnknown, "event create");
+    FRW_CK(cudaEventRecord(ev[0], st));
+    if (total > 0) {
+        rc = launch_walk3_batch(P, walk_blocks(L->device, o.blocks_per_sm), st);
+        if (rc) return rc;
+    }
+    FRW_CK(cudaEventRecord(ev[1], st));
+    std::vector<unsigned long long> h(words);
+    FRW_CK(cudaMemcpyAsync(h.data(), s.p, words * 8, cudaMemcpyDeviceToHost, st));
+    FRW_CK(cudaStreamSynchronize(st));
+    rc = check_grid_status(L, st);
+    if (rc) return rc;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev[0], ev[1]);
+    const unsigned long long *hits_all = h.data() + 1 + 4 * ntargets;
+    const double *sw_all = (const double *)(hits_all + nrow), *sw2_all = sw_all + nrow;
+    for (int32_t t = 0; t < ntargets; t++) {
+        const unsigned long long *stt = h.data() + 1 + 4 * t;
+        if (stt[3] != walks_per_target) {
+            set_error("3-D batch: target " + std::to_string(t) + " finished " + std::to_string(stt[3]) + " of " +
+                      std::to_string(walks_per_target) + " walks");
+            return FRW_E_KERNEL;
+        }
+        frw3_result *res = results + t;
+        const unsigned long long *hits = hits_all + (size_t)t * n;
+        const double *sw = sw_all + (size_t)t * n, *sw2 = sw2_all + (size_t)t * n;
+        const int64_t tk = targets[t];
+        res->walks = walks_per_target;
+        res->escaped = stt[0];
+        res->aborted = stt[1];
+        res->hops_total = stt[2];
+        memcpy(res->gauss, jobs[t].G, sizeof(res->gauss));
+        res->shell = shell;
+        res->kernel_ms = ms;
+        res->fraction_other =
+            walks_per_target ? (double)(walks_per_target - hits[tk]) / (double)walks_per_target : 0.0;
+        int64_t k = 0;
+        for (int64_t i = 0; i < n; i++) {
+            if (!hits[i]) continue;
+            if (k < res->capacity) {
+                const double N = (double)walks_per_target, m = sw[i] / N;
+                const double var = std::max(sw2[i] / N - m * m, 0.0);
+                if (res->conductor) res->conductor[k] = i;
+                if (res->hits) res->hits[k] = hits[i];
+                if (res->cap) res->cap[k] = m;
+                if (res->cap_se) res->cap_se[k] = walks_per_target > 1 ? sqrt(var / (N - 1)) : 0.0;
+                if (res->sum_w) res->sum_w[k] = sw[i];
+                if (res->sum_w2) res->sum_w2[k] = sw2[i];
+            }
+            k++;
+        }
+        res->n_entries = k;
+    }
+    return FRW_OK;
+}
+
 frw_status frw3_walk_trace(const frw3_layout *L, int64_t target, uint64_t first_walk, uint64_t walks, uint64_t seed,
                            const frw3_opts *o, int64_t *end, int32_t *hops, int32_t *bin1, double *weight, int mem,
                            void *stream) {

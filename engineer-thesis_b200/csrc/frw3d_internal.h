@@ -87,6 +87,13 @@ struct Cube3Tables {
     double *offs = nullptr;     // [n]
 };
 
+// One target of a batched run: its Gaussian box, area and box index.
+struct Job3 {
+    double G[6];
+    double S;
+    int64_t target;
+};
+
 struct Walk3Params {
     Dev3Layout L;
     const uint32_t *thr;
@@ -111,6 +118,11 @@ struct Walk3Params {
     unsigned long long *hits;
     double *sum_w, *sum_w2;
     unsigned long long *stats;
+    // batched runs (k_walk3<true>): walk j is walk j % walks_per_job of job
+    // j / walks_per_job; rows and stats of job t start at t * nboxes, 4 t
+    const Job3 *jobs;
+    uint64_t walks_per_job;
+    int64_t nboxes;
     // records (trace mode), indexed by walk - first
     int64_t *rec_end;
     int32_t *rec_hops, *rec_bin;
@@ -135,6 +147,7 @@ void attach_grid3(Dev3Layout &L, const Grid3Buffers &g, const double bounds[6]);
 frw_status launch_query3(const Dev3Layout &L, const double *d_pts, int64_t n, double *d_clear,
                          int64_t *d_nearest, cudaStream_t stream);
 frw_status launch_walk3(const Walk3Params &P, int blocks, cudaStream_t stream);
+frw_status launch_walk3_batch(const Walk3Params &P, int blocks, cudaStream_t stream);
 int walk3_max_blocks_per_sm();
 int walk3_threads();
 

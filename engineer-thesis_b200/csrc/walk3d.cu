@@ -352,11 +352,22 @@ struct Walker {
     uint64_t idx;  // walk index relative to P.first
     uint32_t rblk;
     int hops, b1, axis;
+    int job;       // batched runs: the walk's job
 };
 
 // Start point on the Gaussian box: faces z0, z1, y0, y1, x0, x1 by area from
 // u0 (its remainder places the first coordinate), u1 the second.
+template <bool kMulti>
 __device__ __forceinline__ void start_walk(const Walk3Params &P, Walker &W, uint64_t j) {
+    const double *G = P.G;
+    double S = P.S;
+    if (kMulti) {  // walk j of the batch is walk j % walks_per_job of job j / walks_per_job
+        const uint64_t q = j / P.walks_per_job;
+        W.job = (int)q;
+        j -= q * P.walks_per_job;
+        G = P.jobs[q].G;
+        S = __ldg(&P.jobs[q].S);
+    }
     W.idx = j;
     W.rnd = block3(P, P.first + j, 0);
     W.rblk = 0;
@@ -364,10 +375,9 @@ __device__ __forceinline__ void start_walk(const Walk3Params &P, Walker &W, uint
     const double u1 = (double)W.rnd.y * 0x1p-32;
     if (P.start_strata)  // stratum (walk mod S) of the surface, by the first uniform
         u0 = __ddiv_rn(__dadd_rn((double)(uint32_t)((P.first + j) % P.start_strata), u0), (double)P.start_strata);
-    const double *G = P.G;
     const double w = __dsub_rn(G[3], G[0]), h = __dsub_rn(G[4], G[1]), d = __dsub_rn(G[5], G[2]);
     const double axy = __dmul_rn(w, h), axz = __dmul_rn(w, d), ayz = __dmul_rn(h, d);
-    double s = __dmul_rn(u0, P.S);
+    double s = __dmul_rn(u0, S);
     int f = 0;
     double a = axy;
     for (; f < 5; f++) {
@@ -425,6 +435,32 @@ __device__ __forceinline__ void land(const Walk3Params &P, const double *s_offs,
     }
 }
 
+// kMulti: a batch of targets of one layout (jobs); every lane keeps its
+// sums for one job at a time and flushes them when it starts a walk of
+// another job (jobs are contiguous walk ranges, so that is rare).
+template <bool kMulti>
+__device__ __forceinline__ void flush_job(const Walk3Params &P, int job, unsigned long long &tn, double &ts,
+                                          double &ts2, unsigned long long &n_esc, unsigned long long &n_ab,
+                                          unsigned long long &n_hops, unsigned long long &n_done) {
+    if (!kMulti || job < 0) return;
+    const int64_t t = __ldg(&P.jobs[job].target), row = (int64_t)job * P.nboxes + t;
+    if (tn) {
+        atomicAdd(P.hits + row, tn);
+        atomicAdd(P.sum_w + row, ts);
+        atomicAdd(P.sum_w2 + row, ts2);
+    }
+    unsigned long long *st = P.stats + 4 * (int64_t)job;
+    if (n_esc) atomicAdd(st + 0, n_esc);
+    if (n_ab) atomicAdd(st + 1, n_ab);
+    if (n_done) {
+        atomicAdd(st + 2, n_hops);
+        atomicAdd(st + 3, n_done);
+    }
+    tn = n_esc = n_ab = n_hops = n_done = 0;
+    ts = ts2 = 0.0;
+}
+
+template <bool kMulti>
 __global__ void __launch_bounds__(kW3Threads, kW3MinBlocks) k_walk3(const Walk3Params P) {
     __shared__ uint16_t s_guide[1 << kGuide3Bits];
     __shared__ double s_offs[FRW3_NSAMPLE_MAX];
@@ -441,6 +477,7 @@ __global__ void __launch_bounds__(kW3Threads, kW3MinBlocks) k_walk3(const Walk3P
     double ts = 0.0, ts2 = 0.0;
     uint64_t next = 0, cend = 0;
     bool exhausted = false;
+    int acc_job = -1;  // batched runs: the job the lane's sums belong to
 
     for (;;) {
         // refill idle lanes from the warp's chunk, claiming chunks as needed
@@ -463,7 +500,11 @@ __global__ void __launch_bounds__(kW3Threads, kW3MinBlocks) k_walk3(const Walk3P
             const uint64_t avail = cend - next;
             const unsigned rank = __popc(idle & lt);
             if (!active && rank < avail) {
-                start_walk(P, W, next + rank);
+                start_walk<kMulti>(P, W, next + rank);
+                if (kMulti && W.job != acc_job) {
+                    flush_job<kMulti>(P, acc_job, tn, ts, ts2, n_esc, n_ab, n_hops, n_done);
+                    acc_job = W.job;
+                }
                 active = true;
             }
             next += (uint64_t)__popc(idle) < avail ? (uint64_t)__popc(idle) : avail;
@@ -503,11 +544,24 @@ __global__ void __launch_bounds__(kW3Threads, kW3MinBlocks) k_walk3(const Walk3P
         }
         // the walk ended
         double c = 0.0;
+        const double S = kMulti ? __ldg(&P.jobs[W.job].S) : P.S;
+        const int64_t target = kMulti ? __ldg(&P.jobs[W.job].target) : P.target;
         if (W.b1 >= 0) {
             const double wv = __ldg(P.w + 3 * W.b1 + W.axis);
-            c = __ddiv_rn(__dmul_rn(__dmul_rn(P.perm, P.S), __dmul_rn(W.sgn, wv)), W.a0);
+            c = __ddiv_rn(__dmul_rn(__dmul_rn(P.perm, S), __dmul_rn(W.sgn, wv)), W.a0);
         }
-        if (trace) {
+        if (kMulti) {
+            if (end == target) {
+                tn++;
+                ts = __dadd_rn(ts, c);
+                ts2 = __dadd_rn(ts2, __dmul_rn(c, c));
+            } else if (end >= 0) {
+                const int64_t row = (int64_t)W.job * P.nboxes + end;
+                atomicAdd(P.hits + row, 1ull);
+                atomicAdd(P.sum_w + row, c);
+                atomicAdd(P.sum_w2 + row, __dmul_rn(c, c));
+            }
+        } else if (trace) {
             if (P.rec_end) P.rec_end[W.idx] = end;
             if (P.rec_hops) P.rec_hops[W.idx] = W.hops;
             if (P.rec_bin) P.rec_bin[W.idx] = W.b1;
@@ -528,6 +582,10 @@ __global__ void __launch_bounds__(kW3Threads, kW3MinBlocks) k_walk3(const Walk3P
         active = false;
     }
 
+    if (kMulti) {  // every lane flushes its last job's sums
+        flush_job<kMulti>(P, acc_job, tn, ts, ts2, n_esc, n_ab, n_hops, n_done);
+        return;
+    }
     // warp totals -> global rows
 #pragma unroll
     for (int o = 16; o; o >>= 1) {
@@ -815,14 +873,20 @@ frw_status launch_query3(const Dev3Layout &L, const double *d_pts, int64_t n, do
 }
 
 frw_status launch_walk3(const Walk3Params &P, int blocks, cudaStream_t st) {
-    k_walk3<<<blocks, kW3Threads, 0, st>>>(P);
+    k_walk3<false><<<blocks, kW3Threads, 0, st>>>(P);
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? FRW_OK : cuda_fail(e, "k_walk3");
 }
 
+frw_status launch_walk3_batch(const Walk3Params &P, int blocks, cudaStream_t st) {
+    k_walk3<true><<<blocks, kW3Threads, 0, st>>>(P);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? FRW_OK : cuda_fail(e, "k_walk3 batch");
+}
+
 int walk3_max_blocks_per_sm() {
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk3, kW3Threads, 0) != cudaSuccess) return 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk3<false>, kW3Threads, 0) != cudaSuccess) return 1;
     return std::max(b, 1);
 }
 

@@ -278,6 +278,8 @@ _SIGS = {
     "frw3_walk": ([_VP, C.c_int64, C.c_uint64, C.c_uint64, C.POINTER(Opts3), C.POINTER(Result3), _VP], C.c_int),
     "frw3_walk_device": ([_VP, C.c_int64, C.c_uint64, C.c_uint64, C.POINTER(Opts3), _VP, _VP, _VP, _VP, _VP, _VP],
                          C.c_int),
+    "frw3_walk_batch": ([_VP, _I64, C.c_int32, C.c_uint64, C.c_uint64, C.POINTER(Opts3), C.POINTER(Result3), _VP],
+                        C.c_int),
     "frw3_walk_trace": ([_VP, C.c_int64, C.c_uint64, C.c_uint64, C.c_uint64, C.POINTER(Opts3), _VP, _VP, _VP,
                          _VP, C.c_int, _VP], C.c_int),
     "frw3_generate_layout": ([C.c_uint64, C.c_int64, C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_int32,
@@ -841,6 +843,33 @@ class Layout3:
         m = min(r.n_entries, cap)
         return WalkResult(r.walks, r.escaped, r.aborted, r.hops_total, np.array(r.gauss[:]), r.fraction_other,
                           r.kernel_ms, cond[:m], hits[:m], c[:m], se[:m], s1[:m], s2[:m], {"shell": r.shell})
+
+    def walk_batch(self, targets, walks_per_target: int, seed: int, o: Opts3 | None = None,
+                   capacity: int | None = None, stream: int = 0):
+        """frw3_walk_batch: one WalkResult per target, from one launch."""
+        t = np.ascontiguousarray(targets, dtype=np.int64)
+        cap = self.n if capacity is None else capacity
+        T = len(t)
+        arrs = [(np.zeros(cap, np.int64), np.zeros(cap, np.uint64), np.zeros(cap), np.zeros(cap), np.zeros(cap),
+                 np.zeros(cap)) for _ in range(T)]
+        rs = (Result3 * T)()
+        for r, (cond, hits, c, se, s1, s2) in zip(rs, arrs):
+            r.capacity = cap
+            r.conductor = _ptr(cond, _I64)
+            r.hits = _ptr(hits, C.POINTER(C.c_uint64))
+            r.cap = _ptr(c, _D)
+            r.cap_se = _ptr(se, _D)
+            r.sum_w = _ptr(s1, _D)
+            r.sum_w2 = _ptr(s2, _D)
+        _check(lib().frw3_walk_batch(self._h, _ptr(t, _I64), T, walks_per_target, seed, C.byref(o) if o else None,
+                                     rs, stream or None))
+        out = []
+        for r, (cond, hits, c, se, s1, s2) in zip(rs, arrs):
+            m = min(r.n_entries, cap)
+            out.append(WalkResult(r.walks, r.escaped, r.aborted, r.hops_total, np.array(r.gauss[:]),
+                                  r.fraction_other, r.kernel_ms, cond[:m], hits[:m], c[:m], se[:m], s1[:m], s2[:m],
+                                  {"shell": r.shell}))
+        return out
 
     def walk_device(self, target: int, walks: int, seed: int, o: Opts3 | None, hits, sum_w, sum_w2, stats, status,
                     stream: int = 0):

@@ -154,6 +154,17 @@ frw_status frw3_walk(const frw3_layout *layout, int64_t target, uint64_t walks, 
 frw_status frw3_walk_device(const frw3_layout *layout, int64_t target, uint64_t walks, uint64_t seed,
                             const frw3_opts *opts, uint64_t *hits, double *sum_w, double *sum_w2, uint64_t *stats,
                             uint32_t *status, void *stream);
+/* Several targets of one layout in one persistent launch (rows of a
+ * capacitance matrix): walks_per_target walks from each of targets[0..T-1],
+ * results[t] filled as frw3_walk fills its result (caller-owned rows, the
+ * launch's kernel_ms in every entry).  Walk i of target t draws the same
+ * random numbers as walk i of frw3_walk(target t) with the same seed and
+ * options, so each row equals that call's (the reference's getAvgPathLen
+ * runs one target per call, CPU/getAvgPathLen.cpp:35-114).  T x n must stay
+ * below 2^27: every target's full row is accumulated on the device. */
+frw_status frw3_walk_batch(const frw3_layout *layout, const int64_t *targets, int32_t ntargets,
+                           uint64_t walks_per_target, uint64_t seed, const frw3_opts *opts, frw3_result *results,
+                           void *stream);
 /* Per-walk records (arrays of `walks` entries, any may be NULL): end box
  * (-1 escaped, -2 aborted), clearance queries, first-hop bin (-1 none) and
  * the capacitance weight c. */

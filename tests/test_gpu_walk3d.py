@@ -227,6 +227,29 @@ def test_walk3_stratified_start_bit_exact_and_unbiased():
     assert strat.std(ddof=1) <= 1.25 * plain.std(ddof=1)
 
 
+def test_walk3_batch_rows_equal_single_target_runs():
+    """frw3_walk_batch: one launch over several targets (a duplicate
+    included) gives each target the row of its own frw3_walk."""
+    b = _layout(0xF4A7 + 62, 400, 1000.0, 300.0)
+    targets = [3, 17, 250, 3, 399]
+    o = frw.opts3(first_walk=1 << 20, stream_id=2)
+    with frw.Layout3.from_boxes(b) as L:
+        batch = L.walk_batch(targets, 40_000, 0xBA7C, o)
+        singles = [L.walk(t, 40_000, 0xBA7C, o) for t in targets]
+        empty = L.walk_batch([1, 2], 0, 5)
+        with pytest.raises(frw.FrwError) as e:
+            L.walk_batch([1, 400], 10, 5)
+        assert e.value.status == frw.E_ARG
+    for t, rb, rs in zip(targets, batch, singles):
+        assert np.array_equal(rb.conductor, rs.conductor) and np.array_equal(rb.hits, rs.hits), t
+        np.testing.assert_allclose(rb.sum_w, rs.sum_w, rtol=1e-12, atol=1e-12 * np.abs(rs.sum_w).max())
+        np.testing.assert_allclose(rb.sum_w2, rs.sum_w2, rtol=1e-12)
+        assert (rb.escaped, rb.aborted, rb.hops_total) == (rs.escaped, rs.aborted, rs.hops_total)
+        assert rb.fraction_other == rs.fraction_other and np.array_equal(rb.gauss, rs.gauss)
+        assert rb.row(t)[1] > 0
+    assert all(r.walks == 0 and len(r.conductor) == 0 for r in empty)
+
+
 def test_walk3_disjoint_ranges_add_up():
     b = _layout(0xF4A7 + 53, 200, 800.0, 250.0)
     with frw.Layout3.from_boxes(b) as L:
