@@ -210,16 +210,25 @@ void oc3_nearest(const double *boxes, int64_t n, const double p[3], double *d, i
     *id = bi;
 }
 
-/* Cell grid: cubic cells over the bounds, each listing the boxes that
- * overlap it; a query scans rings of cells around the query's cell until
- * the ring's inner distance exceeds the best distance found. */
+/* Cell grid: cubic cells over the bounds, each binning the boxes that
+ * overlap it.  A ring search over the bins (rings of cells around the
+ * query's cell until a ring's inner distance exceeds the best distance)
+ * answers any point exactly.  For speed each cell also keeps a candidate
+ * list: every box within D_c + 2h + margin of its centre (D_c = the centre's
+ * nearest-box distance, h = half a cell side), sorted by that distance; the
+ * nearest box of any point of the cell is on it, and a scan can stop at the
+ * first entry whose centre distance minus (h + margin) exceeds the best. */
 struct oc3_grid {
     const double *boxes;
     int64_t n;
-    double o[3], side, inv;
+    double o[3], side, inv, h, margin;
     int64_t nc[3];
     int64_t *start, *items;
+    int64_t *lstart, *lbox; /* candidate lists: cell c holds lbox[lstart[c] .. lstart[c+1]) */
+    double *lkey;           /* each entry's distance from its cell centre */
 };
+
+static int build_lists(oc3_grid *g);
 
 static int64_t cell_clamp(double v, double o, double inv, int64_t nc) {
     double t = floor((v - o) * inv);
@@ -282,6 +291,21 @@ oc3_grid *oc3_grid_create(const double *boxes, int64_t n, const double bounds[6]
             g->start[0] = 0;
         }
     }
+    double M = 16.0;
+    for (int c = 0; c < 3; c++) {
+        double a = fabs(bounds[c]) > fabs(bounds[3 + c]) ? fabs(bounds[c]) : fabs(bounds[3 + c]);
+        if (4.0 * a > M) M = 4.0 * a;
+        if (4.0 * ext[c] > M) M = 4.0 * ext[c];
+    }
+    g->h = 0.5 * g->side;
+    g->margin = ldexp(M, -30); /* far above the rounding of a cell index or a distance */
+    if (!build_lists(g)) {     /* without lists every query takes the ring search */
+        free(g->lstart);
+        free(g->lbox);
+        free(g->lkey);
+        g->lstart = g->lbox = NULL;
+        g->lkey = NULL;
+    }
     return g;
 }
 
@@ -289,10 +313,13 @@ void oc3_grid_destroy(oc3_grid *g) {
     if (!g) return;
     free(g->start);
     free(g->items);
+    free(g->lstart);
+    free(g->lbox);
+    free(g->lkey);
     free(g);
 }
 
-void oc3_grid_nearest(const oc3_grid *g, const double p[3], double *d, int64_t *id) {
+static void ring_nearest(const oc3_grid *g, const double p[3], double *d, int64_t *id) {
     int64_t c0[3];
     for (int c = 0; c < 3; c++) c0[c] = cell_clamp(p[c], g->o[c], g->inv, g->nc[c]);
     double best = INFINITY;
@@ -335,6 +362,100 @@ void oc3_grid_nearest(const oc3_grid *g, const double p[3], double *d, int64_t *
                     }
                 }
             }
+        }
+    }
+    *d = best;
+    *id = bi;
+}
+
+typedef struct { double key; int64_t box; } cand3;
+static int cand3_cmp(const void *a, const void *b) {
+    const cand3 *x = (const cand3 *)a, *y = (const cand3 *)b;
+    if (x->key != y->key) return x->key < y->key ? -1 : 1;
+    return x->box < y->box ? -1 : (x->box > y->box);
+}
+
+/* The per-cell candidate lists (count, then fill), deduplicated with a
+ * per-box stamp of the last cell that took the box. */
+static int build_lists(oc3_grid *g) {
+    int64_t total = g->nc[0] * g->nc[1] * g->nc[2];
+    int64_t *stamp = (int64_t *)malloc(sizeof(int64_t) * (size_t)(g->n ? g->n : 1));
+    cand3 *buf = (cand3 *)malloc(sizeof(cand3) * (size_t)(g->n ? g->n : 1));
+    g->lstart = (int64_t *)calloc((size_t)total + 1, sizeof(int64_t));
+    if (!stamp || !buf || !g->lstart) { free(stamp); free(buf); return 0; }
+    for (int pass = 0; pass < 2; pass++) {
+        for (int64_t i = 0; i < g->n; i++) stamp[i] = -1;
+        for (int64_t cid = 0; cid < total; cid++) {
+            int64_t cc[3] = {cid % g->nc[0], (cid / g->nc[0]) % g->nc[1], cid / (g->nc[0] * g->nc[1])};
+            double pc[3], D;
+            int64_t nid;
+            for (int c = 0; c < 3; c++) pc[c] = g->o[c] + ((double)cc[c] + 0.5) * g->side;
+            ring_nearest(g, pc, &D, &nid);
+            double R = D + 2.0 * g->h + g->margin;
+            int64_t rr = (int64_t)ceil(R / g->side) + 1, m = 0;
+            int64_t lo[3], hi[3];
+            for (int c = 0; c < 3; c++) {
+                lo[c] = cc[c] - rr < 0 ? 0 : cc[c] - rr;
+                hi[c] = cc[c] + rr >= g->nc[c] ? g->nc[c] - 1 : cc[c] + rr;
+            }
+            for (int64_t z = lo[2]; z <= hi[2]; z++)
+                for (int64_t y = lo[1]; y <= hi[1]; y++)
+                    for (int64_t x = lo[0]; x <= hi[0]; x++) {
+                        int64_t q = (z * g->nc[1] + y) * g->nc[0] + x;
+                        for (int64_t k = g->start[q]; k < g->start[q + 1]; k++) {
+                            int64_t i = g->items[k];
+                            if (stamp[i] == cid) continue;
+                            stamp[i] = cid;
+                            double v = box_dist(g->boxes + 6 * i, pc);
+                            if (v > R) continue;
+                            buf[m].key = v;
+                            buf[m].box = i;
+                            m++;
+                        }
+                    }
+            if (pass == 0) {
+                g->lstart[cid + 1] = m;
+            } else {
+                qsort(buf, (size_t)m, sizeof(cand3), cand3_cmp);
+                for (int64_t k = 0; k < m; k++) {
+                    g->lbox[g->lstart[cid] + k] = buf[k].box;
+                    g->lkey[g->lstart[cid] + k] = buf[k].key;
+                }
+            }
+        }
+        if (pass == 0) {
+            for (int64_t c = 0; c < total; c++) g->lstart[c + 1] += g->lstart[c];
+            size_t ne = (size_t)(g->lstart[total] ? g->lstart[total] : 1);
+            g->lbox = (int64_t *)malloc(sizeof(int64_t) * ne);
+            g->lkey = (double *)malloc(sizeof(double) * ne);
+            if (!g->lbox || !g->lkey) { free(stamp); free(buf); return 0; }
+        }
+    }
+    free(stamp);
+    free(buf);
+    return 1;
+}
+
+void oc3_grid_nearest(const oc3_grid *g, const double p[3], double *d, int64_t *id) {
+    int64_t c0[3];
+    for (int c = 0; c < 3; c++) {
+        double t = floor((p[c] - g->o[c]) * g->inv);
+        if (!(t >= 0.0) || t >= (double)g->nc[c] || !g->lstart) { /* outside the grid: the ring search */
+            ring_nearest(g, p, d, id);
+            return;
+        }
+        c0[c] = (int64_t)t;
+    }
+    int64_t cid = (c0[2] * g->nc[1] + c0[1]) * g->nc[0] + c0[0];
+    double best = INFINITY, lim = g->h + g->margin;
+    int64_t bi = -1;
+    for (int64_t k = g->lstart[cid]; k < g->lstart[cid + 1]; k++) {
+        if (g->lkey[k] - lim > best) break; /* it and every later entry are farther */
+        int64_t i = g->lbox[k];
+        double v = box_dist(g->boxes + 6 * i, p);
+        if (v < best || (v == best && i < bi)) {
+            best = v;
+            bi = i;
         }
     }
     *d = best;
@@ -424,13 +545,27 @@ int oc3_walk_run(const double *boxes, int64_t n, const double bounds[6], const o
                  int32_t *hops_out, int32_t *bin_out, double *weight_out) {
     if (cfg->target < 0 || cfg->target >= n || cfg->nsample < 1) return OC_E_ARG;
     int N = cfg->nsample, nb = 6 * N * N;
-    double *g = (double *)malloc(sizeof(double) * (size_t)nb * 4);
-    double *intg = (double *)malloc(sizeof(double) * (size_t)(nb + 1));
-    double *w = (double *)malloc(sizeof(double) * (size_t)nb * 3);
-    if (!g || !intg || !w) { free(g); free(intg); free(w); return OC_E_OOM; }
-    double *dgx = g + nb, *dgy = g + 2 * nb, *dgz = g + 3 * nb;
-    oc3_cube_green_table(N, g, dgx, dgy, dgz, intg);
-    oc3_weight_table(N, intg, dgx, dgy, dgz, w);
+    /* the table of the last resolution used is kept (a 50 x 50 table takes
+     * about a third of a second to evaluate); the oracle is single-threaded */
+    static int cached_n = 0;
+    static double *g = NULL, *intg = NULL, *w = NULL;
+    if (cached_n != N) {
+        free(g);
+        free(intg);
+        free(w);
+        cached_n = 0;
+        g = (double *)malloc(sizeof(double) * (size_t)nb * 4);
+        intg = (double *)malloc(sizeof(double) * (size_t)(nb + 1));
+        w = (double *)malloc(sizeof(double) * (size_t)nb * 3);
+        if (!g || !intg || !w) {
+            free(g); free(intg); free(w);
+            g = intg = w = NULL;
+            return OC_E_OOM;
+        }
+        oc3_cube_green_table(N, g, g + nb, g + 2 * nb, g + 3 * nb, intg);
+        oc3_weight_table(N, intg, g + nb, g + 2 * nb, g + 3 * nb, w);
+        cached_n = N;
+    }
     const double *T = boxes + 6 * cfg->target;
     double G[6];
     for (int c = 0; c < 3; c++) {
@@ -476,8 +611,5 @@ int oc3_walk_run(const double *boxes, int64_t n, const double bounds[6], const o
         bin_out[k] = b1;
         weight_out[k] = c;
     }
-    free(g);
-    free(intg);
-    free(w);
     return OC_OK;
 }
