@@ -125,10 +125,24 @@ def test_oracle_grid_nearest_equals_brute_force():
     k = rng.integers(0, len(b), 1000)
     pts[:1000] = b[k, :3] - rng.integers(0, 3, (1000, 3))
     pts[1000:1500] = (b[k[:500], :3] + b[k[:500], 3:]) / 2
+    pts[1500:1510] = B.bounds[3:] + 5.0  # outside the grid: the ring search
     d1, k1 = B.nearest(pts, use_grid=False)
     d2, k2 = B.nearest(pts, use_grid=True)
     assert np.array_equal(d1, d2) and np.array_equal(k1, k2)
     assert np.all(d1[1000:1500] == 0)
+
+
+def test_oracle_grid_lists_exact_on_a_sparse_layout():
+    # one cluster inside bounds ten times wider: coarse cells far from every box
+    b = frw.generate_layout3(0xF4A7 + 22, 1500, 400.0, 400.0, 5, 30, 5, 20, 2)
+    bounds = np.array([-5000.0] * 3 + [5400.0] * 3)
+    G = O.Boxes3(b, bounds, grid=True)
+    rng = np.random.default_rng(22)
+    pts = bounds[:3] + rng.random((8000, 3)) * (bounds[3:] - bounds[:3])
+    pts[:2000] = rng.random((2000, 3)) * 420 - 10  # in and around the cluster
+    d1, k1 = G.nearest(pts, use_grid=False)
+    d2, k2 = G.nearest(pts, use_grid=True)
+    assert np.array_equal(d1, d2) and np.array_equal(k1, k2)
 
 
 def test_oracle_walks_grid_equals_brute_force_and_weights_balance():
