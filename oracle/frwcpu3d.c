@@ -237,7 +237,8 @@ static int64_t cell_clamp(double v, double o, double inv, int64_t nc) {
     return (int64_t)t;
 }
 
-oc3_grid *oc3_grid_create(const double *boxes, int64_t n, const double bounds[6], double boxes_per_cell) {
+oc3_grid *oc3_grid_create(const double *boxes, int64_t n, const double bounds[6], double boxes_per_cell,
+                          int with_lists) {
     oc3_grid *g = (oc3_grid *)calloc(1, sizeof(oc3_grid));
     if (!g) return NULL;
     g->boxes = boxes;
@@ -299,7 +300,7 @@ oc3_grid *oc3_grid_create(const double *boxes, int64_t n, const double bounds[6]
     }
     g->h = 0.5 * g->side;
     g->margin = ldexp(M, -30); /* far above the rounding of a cell index or a distance */
-    if (!build_lists(g)) {     /* without lists every query takes the ring search */
+    if (with_lists && !build_lists(g)) { /* without lists every query takes the ring search */
         free(g->lstart);
         free(g->lbox);
         free(g->lkey);

@@ -59,9 +59,12 @@ double oc3_default_shell(const double *boxes, int64_t n);
 void oc3_nearest(const double *boxes, int64_t n, const double p[3], double *d, int64_t *id);
 
 /* A uniform cell grid over the bounds with the boxes binned by overlap; its
- * nearest-box answers equal oc3_nearest's. */
+ * nearest-box answers equal oc3_nearest's.  with_lists: also build per-cell
+ * candidate lists (fast queries; the build costs seconds at 10^6 boxes),
+ * else every query runs a ring search over the bins. */
 typedef struct oc3_grid oc3_grid;
-oc3_grid *oc3_grid_create(const double *boxes, int64_t n, const double bounds[6], double boxes_per_cell);
+oc3_grid *oc3_grid_create(const double *boxes, int64_t n, const double bounds[6], double boxes_per_cell,
+                          int with_lists);
 void oc3_grid_destroy(oc3_grid *g);
 void oc3_grid_nearest(const oc3_grid *g, const double p[3], double *d, int64_t *id);
 

@@ -130,7 +130,7 @@ def lib():
         L.oc3_default_shell.argtypes = [_D, C.c_int64]
         L.oc3_default_shell.restype = C.c_double
         L.oc3_nearest.argtypes = [_D, C.c_int64, _D, _D, _I64]
-        L.oc3_grid_create.argtypes = [_D, C.c_int64, _D, C.c_double]
+        L.oc3_grid_create.argtypes = [_D, C.c_int64, _D, C.c_double, C.c_int]
         L.oc3_grid_create.restype = C.c_void_p
         L.oc3_grid_destroy.argtypes = [C.c_void_p]
         L.oc3_grid_nearest.argtypes = [C.c_void_p, _D, _D, _I64]
@@ -469,12 +469,16 @@ def layout_bounds3(boxes) -> np.ndarray:
 class Boxes3:
     """A 3-D layout for the oracle: brute-force or cell-grid nearest box and walks."""
 
-    def __init__(self, boxes, bounds=None, grid: bool = False, boxes_per_cell: float = 2.0):
+    def __init__(self, boxes, bounds=None, grid: bool = False, boxes_per_cell: float = 2.0, lists=None):
+        """grid: answer through a cell grid (equal to the brute force);
+        lists: per-cell candidate lists for speed (default: up to 2e5 boxes)."""
         self.boxes = np.ascontiguousarray(boxes, dtype=np.float64)
         self.n = len(self.boxes)
         self.bounds = layout_bounds3(self.boxes) if bounds is None else np.ascontiguousarray(bounds, np.float64)
         self.shell = float(lib().oc3_default_shell(_p(self.boxes), self.n))
-        self._g = lib().oc3_grid_create(_p(self.boxes), self.n, _p(self.bounds), boxes_per_cell) if grid else None
+        with_lists = int(self.n <= 200_000 if lists is None else bool(lists))
+        self._g = (lib().oc3_grid_create(_p(self.boxes), self.n, _p(self.bounds), boxes_per_cell, with_lists)
+                   if grid else None)
 
     def __del__(self):
         g, self._g = getattr(self, "_g", None), None

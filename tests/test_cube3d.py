@@ -115,9 +115,10 @@ def test_cube_table_normalisation_and_symmetry():
     assert np.all(np.isfinite(w))
 
 
-def test_oracle_grid_nearest_equals_brute_force():
+@pytest.mark.parametrize("lists", [True, False])
+def test_oracle_grid_nearest_equals_brute_force(lists):
     b = frw.generate_layout3(0xF4A7 + 20, 400, 1200.0, 400.0)
-    B = O.Boxes3(b, grid=True, boxes_per_cell=1.0)
+    B = O.Boxes3(b, grid=True, boxes_per_cell=1.0, lists=lists)
     rng = np.random.default_rng(5)
     lo, hi = B.bounds[:3], B.bounds[3:]
     pts = lo + rng.random((3000, 3)) * (hi - lo)
