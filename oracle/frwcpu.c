@@ -768,9 +768,15 @@ static double draw(uint64_t seed, uint32_t stream, uint64_t walk, uint32_t hop) 
 int oc_walk_run(const oc_grid *g, const double *rects, const oc_walk_cfg *cfg, uint64_t first,
                 uint64_t count, int64_t *end_out, int32_t *hops_out, int32_t *bin_out,
                 double *weight_out, double *cv_out) {
-    double gtab[OC_NSAMPLE], intg[OC_NSAMPLE + 1], wx[OC_NSAMPLE], wy[OC_NSAMPLE];
-    oc_green_table(OC_NSAMPLE, gtab, intg);
-    oc_weight_table(OC_NSAMPLE, intg, wx, wy);
+    /* the tables are the same for every call: evaluated once (the oracle is
+     * single-threaded) */
+    static int ready = 0;
+    static double gtab[OC_NSAMPLE], intg[OC_NSAMPLE + 1], wx[OC_NSAMPLE], wy[OC_NSAMPLE];
+    if (!ready) {
+        oc_green_table(OC_NSAMPLE, gtab, intg);
+        oc_weight_table(OC_NSAMPLE, intg, wx, wy);
+        ready = 1;
+    }
     double G[4];
     oc_walk_gauss_surface(g, rects, cfg, G);
     double L = 2 * (G[2] - G[0]) + 2 * (G[3] - G[1]);
