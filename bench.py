@@ -2,23 +2,29 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-Workload (one "step"): 1e7 floating random walks from conductor 0 of a
-10,000-rectangle layout on [0,1e4]^2 (integer corners, sizes 5-50, L-inf gap
->= 2, seed 0xF4A7+2), Gaussian surface = target grown by 1 unit, uniform start,
-capacitance row accumulated.  Synthetic data: the reference ships no benchmark
-suite.  Under torchrun every rank runs its own 1e7 walks (Philox stream =
-rank; weak scaling) and the per-conductor rows are summed with one NCCL
-all-reduce inside the step.
+Workload of one step (`config`, the same in both arms): 1e8 floating random
+walks from conductor 0 of a 10^6-rectangle layout on [0,1e5]^2 (integer
+corners, sizes 5-50, L-inf gap >= 2, seed 0xF4A7+3), with the reference's own
+walk definition: Gaussian surface = the target scaled by 1.5 and bisected
+until it clears its neighbours (creatGaussianSurfFrom), start point = a
+Green-CDF bin mapped on that surface (RandomWalk), estimator = per-conductor
+end counts (getAvgPathLen).  Synthetic data: the reference ships no benchmark
+suite.  Under torchrun every rank runs its own 1e8 walks (Philox stream =
+rank; weak scaling) and the per-conductor rows are summed once per step: each
+rank's nonzero rows only (frw_rows_compact), one NCCL all-gather.
 
 `value`  : walks/s with the layout resident in HBM and the rows left on the
            device (frw_walk_device; device events, max over ranks).
-`e2e`    : walks/s through the public C ABI from pinned host rects: layout
-           upload + tree build + walks + result rows back, every step.
+`e2e`    : walks/s through the C ABI from pinned host rects: layout upload +
+           tree and cell-list build + walks + result rows back, every step.
 `--impl reference`: the reference's own CPU walk (RandomWalk as shipped,
-           compiled from its sources into oracle/_ref) on all host cores.
-`walk3d` : the 3-D walk over box conductors with the reference's unit-cube
-           Green's function (10^4 boxes, 1e7 walks per step), its clearance
-           queries, its e2e rate and its CPU restatement's rate.
+           compiled from its sources into oracle/_ref) on all host cores, on
+           the same layout (made by the oracle's generator: no product code
+           is loaded in that process) and the same walk definition.
+Sub-lines: `c2` (10^4 rects, capacitance row, offset-1 surface), `c3_capacitance`
+(10^6 rects, capacitance row), `collision_queries`, `time_to_0.1pct_rel_se`
+(plain vs control variate on 10^6 rects), `batched` (256 layouts) and
+`walk3d` (the 3-D walk over box conductors).
 """
 from __future__ import annotations
 
@@ -38,9 +44,15 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "engineer-thesis_b200"))
 
-WORKLOAD = dict(workload="frw-c2-10k-rects-1e7-walks", rects=10_000, domain=1e4, walks=10_000_000,
-                target=0, gauss="offset-1", start="uniform", layout_seed=0xF4A7 + 2)
-METRIC = "walks/s (plain FRW, 10k-rect layout, 1e7 walks/step, capacitance row); time to 0.1% rel. SE plain vs CV"
+WORKLOAD = dict(workload="frw-c3-1e6-rects-1e8-walks", rects=1_000_000, domain=1e5, walks=100_000_000, target=0,
+                gauss="target scaled by 1.5, bisected to clear its neighbours (reference creatGaussianSurfFrom)",
+                start="Green-CDF bin on the Gaussian perimeter (reference RandomWalk)",
+                estimator="per-conductor end counts, fraction ending elsewhere (reference getAvgPathLen)",
+                layout_seed=0xF4A7 + 3,
+                l2="working set above the 126 MB L2 (cell lists 0.8 GB); the GPU arm also writes 256 MiB "
+                   "between steps")
+METRIC = "walks/s (plain FRW, 10^6-rect layout, 1e8 walks/step, reference surface, start and estimator)"
+PROFILE = os.path.join(ROOT, "profiles", "walk_kernel_c3.md")
 
 
 def algorithmic_bytes_per_query(n_rects: int) -> int:
@@ -56,19 +68,21 @@ def measured_peak_hbm():
     return 6650.0, "fallback"
 
 
-def profiled_traffic(walks_per_launch: int):
-    """DRAM bytes of one walk-kernel launch of `walks_per_launch` walks, scaled
-    from the committed ncu capture (a smaller launch of the same kernel and
-    layout; the traffic is accumulator flushes, proportional to walks)."""
-    p = os.path.join(ROOT, "profiles", "walk_kernel_c2.md")
-    if not os.path.exists(p):
-        return None
-    txt = open(p).read()
-    m = re.search(r"dram_bytes_per_launch\s*=\s*([0-9.eE+]+)", txt)
-    w = re.search(r"walks_per_launch\s*=\s*([0-9.eE+]+)", txt)
-    if not (m and w):
-        return None
-    return float(m.group(1)) * walks_per_launch / float(w.group(1))
+def profile_figures(path=PROFILE):
+    """key = value lines of a committed ncu summary (numbers only)."""
+    if not os.path.exists(path):
+        return {}
+    out = {}
+    for m in re.finditer(r"^\s*([a-z0-9_]+)\s*=\s*([0-9.eE+-]+)\s*$", open(path).read(), re.M):
+        out[m.group(1)] = float(m.group(2))
+    return out
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
 
 
 class Clocks:
@@ -113,56 +127,71 @@ class Clocks:
                 "reasons": reasons}
 
 
-# ------------------------------------------------------------ reference arm
-def _ref_worker(args):
-    rects, bounds, target, seconds, wid, mode = args
+# ------------------------------------------------------------ CPU legs
+# Worker processes build their layout index once, in the pool initialiser
+# (outside every timed call), from the oracle's generator -- the product
+# library is never loaded in them.
+_W = {}
+
+
+def _cpu_init(kind, seed, n, domain, target):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
-    R = O.Ref(rects=rects, bounds=bounds)
+    rects = O.generate_layout(seed, n, domain)
+    bounds = O.layer_bounds(rects)
+    _W.update(kind=kind, target=target, O=O)
+    if kind == "reference":
+        _W["R"] = O.Ref(rects=rects, bounds=bounds)
+    else:
+        G = O.Grid(rects, bounds)
+        _W["G"] = G
+        if kind == "port":  # the benchmark's own walk definition (reference surface and start)
+            _W["cfg"] = G.walk_cfg(target=target, gauss_mode=O.GAUSS_SCALE, gauss_param=1.5,
+                                   start_mode=O.START_GREEN, seed=7, stream=os.getpid() & 0xFFFF)
+        else:  # "port_capacitance": offset-1 surface, uniform start, capacitance weights
+            _W["cfg"] = G.walk_cfg(target=target, gauss_mode=O.GAUSS_OFFSET, gauss_param=1.0,
+                                   start_mode=O.START_UNIFORM, seed=7, stream=os.getpid() & 0xFFFF)
+        _W["next"] = 0
+
+
+def _cpu_run(args):
+    seconds, wid, mode = args
     done, k, t0 = 0, 0, time.perf_counter()
     while time.perf_counter() - t0 < seconds:
-        if mode == "shipped":  # per-walk rng_init, as RandomWalk does
-            R.walks_as_shipped(target, 4)
-            done += 4
-        else:  # the same walk loop with JKISS seeded once per batch
-            R.walks_seeded(target, 64, seed=(wid + 1, k + 7, 0x5EED, 0xC0FFEE))
-            done += 64
+        if _W["kind"] == "reference":
+            if mode == "shipped":  # RandomWalk itself: per-walk rng_init, as shipped
+                _W["R"].walks_as_shipped(_W["target"], 4)
+                done += 4
+            else:  # the same walk loop with JKISS seeded once per 64 walks
+                _W["R"].walks_seeded(_W["target"], 64, seed=(wid + 1, k + 7, 0x5EED, 0xC0FFEE))
+                done += 64
+        else:
+            _W["G"].walks(_W["cfg"], _W["next"], 1024)
+            _W["next"] += 1024
+            done += 1024
         k += 1
-    return done, time.perf_counter() - t0
+    return done
 
 
-def _port_worker(args):
-    rects, bounds, target, seconds, wid = args
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
+class CpuLeg:
+    """`cores` single-threaded worker processes on one layout."""
 
-    G = O.Grid(rects, bounds)
-    cfg = G.walk_cfg(target=target, gauss_mode=O.GAUSS_OFFSET, gauss_param=1.0, start_mode=O.START_UNIFORM,
-                     seed=7, stream=wid)
-    done, t0 = 0, time.perf_counter()
-    while time.perf_counter() - t0 < seconds:
-        G.walks(cfg, done, 2048)
-        done += 2048
-    return done, time.perf_counter() - t0
+    def __init__(self, kind, cores, seed, n, domain, target):
+        self.cores = cores
+        self.pool = mp.get_context("spawn").Pool(cores, initializer=_cpu_init,
+                                                 initargs=(kind, seed, n, domain, target))
+        self.run(0.05, "seeded")  # every worker has built its index
 
+    def run(self, seconds, mode="shipped"):
+        """(walks/s over the call's wall time, walks)."""
+        t0 = time.perf_counter()
+        done = sum(self.pool.map(_cpu_run, [(seconds, i, mode) for i in range(self.cores)], chunksize=1))
+        return done / (time.perf_counter() - t0), done
 
-def port_rate(rects, bounds, target, seconds, cores):
-    """Walks/s of the FP64 CPU restatement (the oracle, uniform grid index,
-    the benchmark's own offset-1 surface and capacitance weights) on `cores`
-    processes."""
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(cores) as pool:
-        res = pool.map(_port_worker, [(rects, bounds, target, seconds, i) for i in range(cores)])
-    return sum(d for d, _ in res) / max(t for _, t in res), sum(d for d, _ in res)
-
-
-def reference_rate(rects, bounds, target, seconds, cores, mode="shipped"):
-    """Walks/s of the reference CPU walk on `cores` processes."""
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(cores) as pool:
-        res = pool.map(_ref_worker, [(rects, bounds, target, seconds, i, mode) for i in range(cores)])
-    return sum(d for d, _ in res) / max(t for _, t in res), sum(d for d, _ in res)
+    def close(self):
+        self.pool.terminate()
+        self.pool.join()
 
 
 def reference_available():
@@ -170,43 +199,69 @@ def reference_available():
 
 
 def run_reference(args):
+    """The reference arm: RandomWalk as shipped on every host core, on the
+    benchmark's layout and walk definition; each step a bounded sample."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    import frw
-
-    rects = frw.generate_layout(WORKLOAD["layout_seed"], WORKLOAD["rects"], WORKLOAD["domain"]).astype(np.float64)
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
-
-    bounds = O.layer_bounds(rects)
     if not reference_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/librefcpu.so not built "
                           "(needs the reference sources at build time)"}))
         return 0
-    cores = os.cpu_count() or 1
+    W = WORKLOAD
+    cores = host_cores()
     step_s = 2.0
+    leg = CpuLeg("reference", cores, W["layout_seed"], W["rects"], W["domain"], W["target"])
     for _ in range(args.warmup):
-        reference_rate(rects, bounds, WORKLOAD["target"], 0.5, cores)
-    t0 = time.perf_counter()
-    total, rates = 0, []
+        leg.run(0.5)
+    total, wall = 0, 0.0
     for _ in range(args.steps):
-        rate, n = reference_rate(rects, bounds, WORKLOAD["target"], step_s, cores)
-        rates.append(rate)  # walks / the slowest worker's own time (process start-up excluded)
+        t0 = time.perf_counter()
+        _, n = leg.run(step_s)
+        wall += time.perf_counter() - t0
         total += n
-    el = time.perf_counter() - t0
-    v = statistics.mean(rates)
-    cfg = dict(WORKLOAD, gauss="reference scale 1.5", start="reference Green CDF", walks=f"~{step_s}s sample/step")
+    leg.close()
+    v = total / wall
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": "walks/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": cfg,
+        "config": dict(W),
         "cpu_baseline": {"value": v, "unit": "walks/s", "cores": cores, "kind": "reference",
-                         "sample": f"RandomWalk as shipped (per-walk rng_init), {args.steps} x {step_s}s on "
-                                   f"{cores} processes, {total} walks"},
+                         "sample": f"RandomWalk as shipped (per-walk rng_init), {args.steps} x {step_s}s of walks on "
+                                   f"{cores} processes, {total} walks; layout from the oracle's generator, "
+                                   "reference CPU quadtree built once per process outside the timing"},
         "e2e": {"value": v, "unit": "walks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
     return 0
+
+
+def cpu_baselines(seconds):
+    """Rank 0 at N = 1, before any GPU work: the reference as shipped, its walk
+    loop seeded once, and the FP64 restatement, all on the headline layout."""
+    W = WORKLOAD
+    cores = host_cores()
+    out = {}
+    if reference_available():
+        leg = CpuLeg("reference", cores, W["layout_seed"], W["rects"], W["domain"], W["target"])
+        rate, n = leg.run(seconds)
+        rate1, n1 = leg.run(seconds / 2, "seeded")
+        leg.close()
+        out = {"value": rate, "unit": "walks/s", "cores": cores, "kind": "reference", "per_core": rate / cores,
+               "sample": f"reference RandomWalk as shipped (per-walk rng_init, its CPU quadtree) on the headline "
+                         f"layout and walk definition, {seconds:.0f}s on {cores} processes, {n} walks",
+               "seeded_once": {"value": rate1, "per_core": rate1 / cores,
+                               "sample": f"the same reference walk loop with JKISS seeded once per 64 walks, "
+                                         f"{seconds / 2:.0f}s on {cores} processes, {n1} walks"}}
+    leg = CpuLeg("port", cores, W["layout_seed"], W["rects"], W["domain"], W["target"])
+    rate2, n2 = leg.run(seconds / 4)
+    leg.close()
+    port = {"value": rate2, "unit": "walks/s", "cores": cores, "kind": "port", "per_core": rate2 / cores,
+            "sample": f"the FP64 CPU restatement (oracle/, complete queries on a uniform grid index) on the "
+                      f"headline layout and walk definition, {seconds / 4:.1f}s on {cores} processes, {n2} walks"}
+    if out:
+        out["port"] = port
+        return out
+    return port
 
 
 # ------------------------------------------------------------ headline runs
@@ -281,16 +336,16 @@ def time_to_rel_se(frw, device, stream):
             "agree_sigma": abs(p["c00"] - c["c00"]) / np.hypot(p["c00"] * p["rel_se"], c["c00"] * c["rel_se"])}
 
 
-# ------------------------------------------------------------ queries and C3
-def query_rates(frw, L, device, stream):
-    """drawBiggestSquareAtPoint + checkCollisons(point) per point, batched:
-    the 1e5-point check set (uniform in the bounds, seed 0x0C2) and a 1e7-point
-    batch (inputs and outputs 560 MB, larger than L2), device buffers."""
+# ------------------------------------------------------------ queries
+def query_rates(frw, L, device, stream, sets):
+    """drawBiggestSquareAtPoint + checkCollisons(point) per point, batched on
+    device buffers: (name, points, seed, repetitions) per set, points uniform
+    in the layout's bounds."""
     import torch
 
     b = L.bounds
     out = {}
-    for name, n, seed, reps in (("check_1e5", 100_000, 0x0C2, 20), ("batch_1e7", 10_000_000, 0x0C2 + 1, 5)):
+    for name, n, seed, reps in sets:
         rng = np.random.default_rng(seed)
         pts = np.stack([rng.uniform(b[0], b[2], n), rng.uniform(b[1], b[3], n)], 1)
         p = torch.as_tensor(pts, device=device)
@@ -310,37 +365,60 @@ def query_rates(frw, L, device, stream):
     return out
 
 
-C3 = dict(workload="frw-c3-1e6-rects-1e8-walks", rects=1_000_000, domain=1e5, walks=100_000_000, target=0,
-          layout_seed=0xF4A7 + 3)
+# ------------------------------------------------------------ sub-lines on the capacitance estimator
+C2 = dict(workload="frw-c2-10k-rects-1e7-walks", rects=10_000, domain=1e4, walks=10_000_000, target=0,
+          gauss="offset-1", start="uniform", estimator="capacitance row", layout_seed=0xF4A7 + 2)
+C3CAP = dict(workload="frw-c3-1e6-rects-1e8-walks-capacitance", rects=1_000_000, domain=1e5, walks=100_000_000,
+             target=0, gauss="offset-1", start="uniform", estimator="capacitance row", layout_seed=0xF4A7 + 3)
 
 
-def c3_run(frw, device, stream, steps):
-    """C3: 10^6 rects, 1e8 walks per step, full capacitance row (offset-1
-    surface, uniform start).  Per-walk records and row sums of this layout
-    equal the FP64 oracle's (GPU test on a 2e5-walk sub-range)."""
+def device_rows_run(frw, W, o, device, stream, steps, flush):
+    """walks/s of frw_walk_device on layout W (rows left on the device, L2
+    flushed between steps), the C_00 row and the mean hop count."""
     import torch
 
-    rects = frw.generate_layout(C3["layout_seed"], C3["rects"], C3["domain"])
-    frw.Layout.from_rects(rects, device=device).close()  # first build grows the memory pool
+    rects = frw.generate_layout(W["layout_seed"], W["rects"], W["domain"])
     L = frw.Layout.from_rects(rects, device=device)
-    o = frw.capacitance_opts(1.0)
-    L.walk(C3["target"], 1_000_000, seed=1, o=o, stream=stream.cuda_stream)
+    n = L.n
+    dev = torch.device("cuda", device)
+    rows_i = torch.zeros(n + 4, dtype=torch.int64, device=dev)
+    rows_f = torch.zeros(2 * n, dtype=torch.float64, device=dev)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+
+    def step(seed):
+        rows_i.zero_()
+        rows_f.zero_()
+        L.walk_device(W["target"], W["walks"], seed, o, rows_i[:n], rows_f[:n], rows_f[n:], rows_i[n:], status,
+                      stream.cuda_stream)
+
+    for i in range(3):
+        step(900 + i)
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    res = [L.walk(C3["target"], C3["walks"], seed=300 + k, o=o, stream=stream.cuda_stream) for k in range(steps)]
-    e1.record(stream)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for i in range(steps):
+        flush.zero_()
+        ev[i][0].record(stream)
+        step(700 + i)
+        ev[i][1].record(stream)
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / steps
-    r = res[-1]
-    c, se = r.row(C3["target"])[1:]
-    info = L.info
-    L_cells_ms = L.cells.build_ms
+    if int(status.item()) != 0:
+        raise RuntimeError(f"walk kernel reported status {int(status.item()):#x}")
+    ms = statistics.median(a.elapsed_time(b) for a, b in ev)
+    ri, rf = rows_i.cpu().numpy(), rows_f.cpu().numpy()
+    st = ri[n:]
+    nw = float(W["walks"])
+    m1 = rf[W["target"]] / nw
+    var = max(rf[n + W["target"]] / nw - m1 * m1, 0.0) * nw / (nw - 1.0)
+    hbar = float(st[2]) / float(st[3])
+    bq = algorithmic_bytes_per_query(W["rects"])
+    peak, kind = measured_peak_hbm()
+    ach = W["walks"] * hbar * bq / (ms * 1e-3) / 1e9
+    out = {"workload": W["workload"], "config": W, "kernel_ms": ms, "walks_per_s": W["walks"] / (ms * 1e-3),
+           "mean_hops": hbar, "c00": m1, "c00_rel_se": float(np.sqrt(var / nw) / abs(m1)) if m1 else None,
+           "conductors_reached": int((ri[:n] > 0).sum()),
+           "roofline_frac": ach / peak, "roofline_note": f"{bq} B/query x {hbar:.2f} queries/walk of {kind} HBM"}
     L.close()
-    return {"workload": C3["workload"], "ms_per_step": ms, "walks_per_s": C3["walks"] / (ms * 1e-3),
-            "mean_hops": r.hops_total / C3["walks"], "c00": c, "c00_rel_se": se / abs(c),
-            "conductors_reached": int(len(r.conductor)), "tree_build_ms": info.build_ms,
-            "cell_build_ms": L_cells_ms}
+    return out
 
 
 # ------------------------------------------------------------ 3-D path
@@ -500,17 +578,23 @@ def main():
     ap.add_argument("--no-headline", action="store_true", help="skip the time-to-0.1%% plain vs CV runs")
     ap.add_argument("--no-batched", action="store_true", help="skip the 256-layout batched runs")
     ap.add_argument("--no-3d", action="store_true", help="skip the 3-D walk runs")
+    ap.add_argument("--no-sub", action="store_true", help="skip the C2 / C3-capacitance / query sub-lines")
     args = ap.parse_args()
     if args.walks:
         WORKLOAD["walks"] = args.walks
     if args.impl == "reference":
         return run_reference(args)
 
-    import torch
-
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    # CPU baseline first (spawned pools, before any GPU work), rank 0 at N=1 only
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baselines(args.cpu_seconds)
+
+    import torch
+
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
@@ -524,33 +608,10 @@ def main():
 
     W = WORKLOAD
     rects = frw.generate_layout(W["layout_seed"], W["rects"], W["domain"])
-    # CPU baseline first (spawned pool, before heavy GPU work), rank 0 at N=1 only
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline and reference_available():
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import oracle as O
-
-        cores = os.cpu_count() or 1
-        rb = rects.astype(np.float64), O.layer_bounds(rects.astype(np.float64))
-        rate, n = reference_rate(*rb, W["target"], args.cpu_seconds, cores)
-        rate1, n1 = reference_rate(*rb, W["target"], args.cpu_seconds / 2, cores, mode="seeded")
-        rate2, n2 = port_rate(*rb, W["target"], args.cpu_seconds / 4, cores)
-        cpu = {"value": rate, "unit": "walks/s", "cores": cores, "kind": "reference",
-               "sample": f"reference RandomWalk as shipped (per-walk rng_init, reference scale-1.5 surface and "
-                         f"Green-CDF start) on the same layout and target, {args.cpu_seconds:.0f}s on {cores} "
-                         f"processes, {n} walks",
-               "per_core": rate / cores,
-               "seeded_once": {"value": rate1, "per_core": rate1 / cores,
-                               "sample": f"the same walk loop with JKISS seeded once per 64 walks, "
-                                         f"{args.cpu_seconds / 2:.0f}s on {cores} processes, {n1} walks"},
-               "port": {"value": rate2, "per_core": rate2 / cores,
-                        "sample": f"the FP64 CPU restatement (oracle/, uniform grid index, offset-1 surface, "
-                                  f"capacitance weights), {args.cpu_seconds / 4:.1f}s on {cores} processes, "
-                                  f"{n2} walks"}}
-
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
-    o = frw.capacitance_opts(1.0, stream_id=shard.plan(W["walks"], rank)["stream"])
+    o = frw.opts(stream_id=shard.plan(W["walks"], rank)["stream"])  # the reference's walk definition
+    frw.Layout.from_rects(rects, device=local).close()  # the first build grows the memory pool
     L = frw.Layout.from_rects(rects, device=local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
 
@@ -560,6 +621,12 @@ def main():
     rows_i = torch.zeros(n + 4, dtype=torch.int64, device=dev)
     rows_f = torch.zeros(2 * n, dtype=torch.float64, device=dev)
     status = torch.zeros(1, dtype=torch.int32, device=dev)
+    if dist is not None:  # the exchange: each rank's nonzero rows, all-gathered (NCCL), summed on every rank
+        cap = min(n, 1 << 16)
+        sbuf = shard.sparse_buffer(cap, dev)
+        s_count, s_stats, s_idx, s_hits, s_w, s_w2 = shard.sparse_views(sbuf, cap)
+        sum_i, sum_f = torch.zeros_like(rows_i), torch.zeros_like(rows_f)
+        overflow = torch.zeros((), dtype=torch.bool, device=dev)
 
     def step(seed, kev=None):
         rows_i.zero_()
@@ -570,9 +637,14 @@ def main():
                       stream.cuda_stream)
         if kev:
             kev[1].record(stream)
-        if dist is not None:  # the one exchange: the rows summed over ranks (NCCL)
-            dist.all_reduce(rows_i)
-            dist.all_reduce(rows_f)
+        if dist is not None:
+            L.rows_compact(rows_i[:n], rows_f[:n], rows_f[n:], s_idx, s_hits, s_w, s_w2, s_count,
+                           stream.cuda_stream)
+            s_stats.copy_(rows_i[n:])
+            g = shard.gather_sparse(sbuf, world)
+            sum_i.zero_()
+            sum_f.zero_()
+            overflow.logical_or_(shard.merge_sparse(g, n, cap, sum_i, sum_f))
 
     for i in range(args.warmup):
         step(1000 + i)
@@ -592,19 +664,22 @@ def main():
         dist.barrier()
     if int(status.item()) != 0:
         raise RuntimeError(f"walk kernel reported status {int(status.item()):#x}")
+    if dist is not None and bool(overflow.item()):
+        raise RuntimeError(f"a rank reached more than {cap} conductors in one step: sparse exchange too small")
     kern_ms = [a.elapsed_time(b) for a, b in kev]
     t_ms = sum(a.elapsed_time(b) for a, b in ev)
     if dist is not None:
         t = torch.tensor([t_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_ms = float(t.item())
-    last_i, last_f = rows_i.cpu().numpy(), rows_f.cpu().numpy()  # the last step, all ranks
+    last_i = (rows_i if dist is None else sum_i).cpu().numpy()  # the last step, all ranks
     stats = last_i[n:]
     assert int(stats[3]) == W["walks"] * world, stats
     walks_total = W["walks"] * args.steps * world
     value = walks_total / (t_ms * 1e-3)
 
-    # e2e through the public ABI from pinned host memory
+    # e2e through the public ABI from pinned host memory, every step:
+    # layout upload + tree and cell-list build + walks + rows back
     pinned = torch.from_numpy(rects).pin_memory()
     ptr = pinned.data_ptr()
     import ctypes
@@ -631,61 +706,75 @@ def main():
         torch.cuda.synchronize()
         e2e_ms = e0.elapsed_time(e1) / e2e_steps
 
-    queries = query_rates(frw, L, dev, stream) if rank == 0 and world == 1 else None
-    c3 = c3_run(frw, local, stream, 3) if rank == 0 and world == 1 and not args.no_batched else None
-    headline = batched = None
-    if rank == 0 and world == 1 and not args.no_headline:
-        headline = time_to_rel_se(frw, local, stream)
-    if rank == 0 and world == 1 and not args.no_batched:
-        batched = batched_run(frw, local, stream, 3)
-    walk3d = None
-    if rank == 0 and world == 1 and not args.no_3d:
-        walk3d = walk3d_run(frw, local, stream, 3, 0.0 if args.no_cpu_baseline else 2.0,
-                            min(os.cpu_count() or 1, 16))
+    solo = rank == 0 and world == 1
+    sub = {}
+    if solo and not args.no_sub:
+        sub["collision_queries"] = query_rates(frw, L, dev, stream, [("c3_batch_1e7", 10_000_000, 0x0C3, 5)])
+    L.close()
+    if solo and not args.no_sub:
+        sub["c2"] = device_rows_run(frw, C2, frw.capacitance_opts(1.0), local, stream, 10, flush)
+        with frw.Layout.from_rects(frw.generate_layout(C2["layout_seed"], C2["rects"], C2["domain"]),
+                                   device=local) as L2:
+            sub["collision_queries"].update(query_rates(frw, L2, dev, stream,
+                                                        [("c2_check_1e5", 100_000, 0x0C2, 20),
+                                                         ("c2_batch_1e7", 10_000_000, 0x0C2 + 1, 5)]))
+        sub["c3_capacitance"] = device_rows_run(frw, C3CAP, frw.capacitance_opts(1.0), local, stream, 5, flush)
+    if solo and not args.no_headline:
+        sub["time_to_0.1pct_rel_se"] = time_to_rel_se(frw, local, stream)
+    if solo and not args.no_batched:
+        sub["batched"] = batched_run(frw, local, stream, 3)
+    if solo and not args.no_3d:
+        sub["walk3d"] = walk3d_run(frw, local, stream, 3, 0.0 if args.no_cpu_baseline else 2.0,
+                                   min(host_cores(), 16))
 
     if rank == 0:
-        nw = float(W["walks"] * world)
-        m1 = last_f[W["target"]] / nw
-        var = max(last_f[n + W["target"]] / nw - m1 * m1, 0.0) * nw / (nw - 1.0)
-        rel_se = float(np.sqrt(var / nw) / abs(m1))
         hbar = float(stats[2]) / float(stats[3])
         bq = algorithmic_bytes_per_query(W["rects"])
         kms = statistics.median(kern_ms)
-        achieved = W["walks"] * hbar * bq / (kms * 1e-3) / 1e9
+        kernel_walks_s = W["walks"] / (kms * 1e-3)
+        achieved = kernel_walks_s * hbar * bq / 1e9
         peak, peak_kind = measured_peak_hbm()
-        traffic = profiled_traffic(W["walks"])
+        clocks = clk.summary()
+        prof = profile_figures()
+        traffic = None
+        if "dram_bytes_per_launch" in prof and "walks_per_launch" in prof:
+            traffic = prof["dram_bytes_per_launch"] * W["walks"] / prof["walks_per_launch"]
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "algorithmic_bytes_per_walk": hbar * bq,
+                "note": f"k_walk; algorithmic {bq} B/query (the tree query's bytes at 10^6 rects) x {hbar:.2f} "
+                        f"queries/walk; peak {peak_kind}; the cell lists and tree are read through L2, so "
+                        "issue_frac is the bound the kernel sits on"}
+        if "l2_bytes_per_walk" in prof:
+            roof["l2_bytes_per_walk"] = prof["l2_bytes_per_walk"]
+        if "warp_instructions_per_walk" in prof and clocks.get("sm_mhz"):
+            sms = torch.cuda.get_device_properties(dev).multi_processor_count
+            issue = kernel_walks_s * prof["warp_instructions_per_walk"] / (sms * 4 * clocks["sm_mhz"] * 1e6)
+            roof["issue_frac"] = issue
+            roof["warp_instructions_per_walk"] = prof["warp_instructions_per_walk"]
+            if "threads_per_instruction" in prof:
+                roof["threads_per_instruction"] = prof["threads_per_instruction"]
         out = {
             "metric": METRIC, "value": value, "unit": "walks/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(W, l2="flushed between steps (256 MiB write)", parallelism=f"walks x{world}",
-                           time_to_rel_se_1e3_s=t_ms / args.steps * 1e-3 * (rel_se / 1e-3) ** 2,
-                           c00_rel_se_per_step=rel_se, mean_hops=hbar),
+            "config": dict(W),
+            "stats": {"mean_hops": hbar, "kernel_ms_median": kms, "kernel_walks_per_s": kernel_walks_s,
+                      "queries_per_s": kernel_walks_s * hbar, "escaped_last_step": int(stats[0]),
+                      "conductors_reached_last_step": int((last_i[:n] > 0).sum()),
+                      "fraction_other_last_step": 1.0 - float(last_i[W["target"]]) / float(stats[3]),
+                      "parallelism": f"walks x{world}", "query_semantics": "complete (the reference GPU "
+                      "traversal's); the reference CPU tree as shipped misses collisions"},
             "e2e": {"value": W["walks"] / (e2e_ms * 1e-3), "unit": "walks/s",
                     "h2d_bytes_per_step": W["rects"] * 16 + 32,
                     "d2h_bytes_per_step": nrows * 32 + 64},
-            "gpu_launches": 2 * args.steps,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "note": f"walk kernel; algorithmic {bq} B/query (the tree query's bytes) x {hbar:.2f} "
-                                 f"queries/walk; peak {peak_kind} (cell lists and tree are L2-resident, so HBM is an "
-                                 "upper-bound denominator)"},
-            "clocks": clk.summary(),
+            "gpu_launches": (2 if world == 1 else 3) * args.steps,
+            "roofline": roof,
+            "clocks": clocks,
         }
-        if queries:
-            out["collision_queries"] = queries
-        if c3:
-            out["c3"] = c3
-        if headline:
-            out["time_to_0.1pct_rel_se"] = headline
-        if batched:
-            out["batched"] = batched
-        if walk3d:
-            out["walk3d"] = walk3d
+        out.update(sub)
         if cpu:
             out["cpu_baseline"] = cpu
         print(json.dumps(out))
-    L.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

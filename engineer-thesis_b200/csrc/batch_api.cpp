@@ -315,7 +315,7 @@ frw_status frw_batch_tune(frw_batch *B, uint64_t trial_walks, frw_tuning *chosen
                 float ms = 0.f;
                 for (int rep = 0; rep < 2 && !rc; rep++) {  // first run warms caches
                     rc = enqueue_run(B, d_tj, jobs[0], tot, t, B->cs, k0, k1);
-                    if (!rc && cudaStreamSynchronize(B->cs) != cudaSuccess) rc = FRW_E_CUDA;
+                    if (!rc) rc = wait_stream(B->cs, "frw_batch_tune: trial");
                     if (!rc) cudaEventElapsedTime(&ms, k0, k1);
                 }
                 if (rc) break;
@@ -324,10 +324,7 @@ frw_status frw_batch_tune(frw_batch *B, uint64_t trial_walks, frw_tuning *chosen
                     best.ms = ms;
                 }
             }
-    if (rc) {
-        if (rc == FRW_E_CUDA) set_error("frw_batch_tune: trial launch failed");
-        return rc;
-    }
+    if (rc) return rc;
     B->tuning = best;
     if (chosen) *chosen = best;
     return build_graph(B);
@@ -357,6 +354,11 @@ frw_status frw_batch_run(frw_batch *B, uint64_t seed, frw_result *results, void 
     uint32_t status = 0;
     std::vector<unsigned long long> stats(4 * (size_t)B->njobs);
     std::vector<double> gauss(4 * (size_t)B->njobs);
+    {
+        WaitScope ws(B->opts.timeout_ms);
+        frw_status rc = wait_stream(B->cs, "frw_batch_run");
+        if (rc) return rc;
+    }
     FRW_CK(cudaMemcpyAsync(&cnt, B->d_cnt, 8, cudaMemcpyDeviceToHost, B->cs));
     FRW_CK(cudaMemcpyAsync(&status, B->d_status, 4, cudaMemcpyDeviceToHost, B->cs));
     FRW_CK(cudaMemcpyAsync(stats.data(), B->d_stats, stats.size() * 8, cudaMemcpyDeviceToHost, B->cs));

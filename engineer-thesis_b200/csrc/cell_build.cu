@@ -281,9 +281,8 @@ frw_status build_cells(const DevLayout &Lin, double cells_per_rect, int cap, cud
         if (!ck(cudaGetLastError(), "cell count")) break;
         int64_t total = 0;
         unsigned long long novf = 0;
-        if (!ck(cudaMemcpyAsync(&total, grand, 8, cudaMemcpyDeviceToHost, st), "cell total")) break;
-        if (!ck(cudaMemcpyAsync(&novf, ovf, 8, cudaMemcpyDeviceToHost, st), "cell overflow")) break;
-        if (!ck(cudaStreamSynchronize(st), "cell total")) break;
+        if ((rc = read_back(&total, grand, 8, st, "build_cells: list total"))) break;
+        if ((rc = read_back(&novf, ovf, 8, st, "build_cells: overflow count"))) break;
         if (total > INT32_MAX) {
             set_error("build_cells: more than 2^31 list entries; use fewer cells per rect");
             rc = FRW_E_ARG;
@@ -296,7 +295,7 @@ frw_status build_cells(const DevLayout &Lin, double cells_per_rect, int cap, cud
         if (total > 0) k_cell_fill<<<blocks, 128, 0, st>>>(L, G, start, C.cells, C.crects, C.cids, ncells);
         if (!ck(cudaGetLastError(), "cell fill")) break;
         if (!ck(cudaEventRecord(e1, st), "event")) break;
-        if (!ck(cudaEventSynchronize(e1), "cell sync")) break;
+        if ((rc = wait_event(e1, "build_cells"))) break;
         cudaEventElapsedTime(&C.build_ms, e0, e1);
     } while (0);
     for (void *p : {(void *)cnt, (void *)start, (void *)sums, (void *)grand, (void *)ovf})

@@ -758,11 +758,9 @@ frw_status net_alloc(Net *n, cudaStream_t st) {
     return FRW_OK;
 }
 
-void net_free(Net *n) {
-    cudaFree(n->p);
-    cudaFree(n->w1);
-    cudaFree(n->w2);
-    cudaFree(n->w2t);
+void net_free(Net *n, cudaStream_t st) {
+    for (void *q : {(void *)n->p, (void *)n->w1, (void *)n->w2, (void *)n->w2t})
+        if (q) cudaFreeAsync(q, st);
     *n = Net();
 }
 

@@ -28,7 +28,8 @@ struct Net {
 };
 
 frw_status net_alloc(Net *n, cudaStream_t st);
-void net_free(Net *n);
+// Releases the parameters in the order of `st` (after work queued there).
+void net_free(Net *n, cudaStream_t st);
 frw_status net_upload(Net *n, const float *host_params, cudaStream_t st);
 frw_status net_refresh_bf16(const Net &n, cudaStream_t st);
 

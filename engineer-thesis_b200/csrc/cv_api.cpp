@@ -140,6 +140,7 @@ frw_status frw_cv_train(const frw_layout *layout, int64_t target, const frw_opts
         return FRW_E_ARG;
     }
     SetDevice sd(v.device);
+    WaitScope ws(walk_opts->timeout_ms);
     const double *tables;
     int sms;
     rc = device_tables(v.device, &tables, &sms);
@@ -152,7 +153,7 @@ frw_status frw_cv_train(const frw_layout *layout, int64_t target, const frw_opts
     M->view = v;
     M->train_walks = co.train_walks;
     auto fail = [&](frw_status r) {
-        cv::net_free(&M->net);
+        cv::net_free(&M->net, st);
         if (M->phi) cudaFreeAsync(M->phi, st);
         delete M;
         return r;
@@ -200,9 +201,8 @@ frw_status frw_cv_train(const frw_layout *layout, int64_t target, const frw_opts
         }
         if (rc) return fail(rc);
         double wsum = 0.0;
-        e = cudaMemcpyAsync(&wsum, d_wsum, 8, cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) return fail(cuda_fail(e, "frw_cv_train: training set"));
+        rc = read_back(&wsum, d_wsum, 8, st, "frw_cv_train: training set");
+        if (rc) return fail(rc);
         if (!(wsum > 0)) {
             set_error("frw_cv_train: no training walk has a first hop");
             return fail(FRW_E_ARG);
@@ -232,9 +232,8 @@ frw_status frw_cv_train(const frw_layout *layout, int64_t target, const frw_opts
         if (rc) return fail(rc);
         cudaEventRecord(e1, st);
         std::vector<double> losses(steps);
-        e = cudaMemcpyAsync(losses.data(), d_loss, (size_t)steps * 8, cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) return fail(cuda_fail(e, "frw_cv_train: loss read-back"));
+        rc = read_back(losses.data(), d_loss, (size_t)steps * 8, st, "frw_cv_train: training");
+        if (rc) return fail(rc);
         double l = 0;
         for (int s = steps - steps_per_epoch; s < steps; s++) l += losses[s];
         M->train_loss = l / steps_per_epoch;
@@ -274,11 +273,11 @@ frw_status frw_cv_train(const frw_layout *layout, int64_t target, const frw_opts
                                       walk_opts->exact_perimeter != 0, M->net, d_mu, M->phi, st);
         if (rc) return fail(rc);
         uint32_t hs = 0;
-        e = cudaMemcpyAsync(&M->mean_term, d_mu, 8, cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(&hs, d_status, 4, cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess) e = cudaEventRecord(e2, st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        e = cudaEventRecord(e2, st);
         if (e != cudaSuccess) return fail(cuda_fail(e, "frw_cv_train: quadrature"));
+        rc = read_back(&M->mean_term, d_mu, 8, st, "frw_cv_train: quadrature");
+        if (!rc) rc = read_back(&hs, d_status, 4, st, "frw_cv_train: quadrature");
+        if (rc) return fail(rc);
         if (hs) {
             set_error("frw_cv_train: a kernel reported an internal limit during the quadrature");
             return fail(FRW_E_KERNEL);
@@ -315,6 +314,7 @@ frw_status frw_cv_walk(const frw_cv *M, uint64_t walks, uint64_t seed, frw_cv_re
         return FRW_E_ARG;
     }
     SetDevice sd(M->view.device);
+    WaitScope ws(M->opts.timeout_ms);
     cudaStream_t st = (cudaStream_t)stream;
     const uint64_t chunk = std::min<uint64_t>(walks, 1ull << 23);
     Buf B(st);
@@ -341,11 +341,7 @@ frw_status frw_cv_walk(const frw_cv *M, uint64_t walks, uint64_t seed, frw_cv_re
     }
     cudaEventRecord(e1, st);
     double h[4] = {0, 0, 0, 0};
-    if (!rc) {
-        e = cudaMemcpyAsync(h, d_sums, 32, cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) rc = cuda_fail(e, "frw_cv_walk: read-back");
-    }
+    if (!rc) rc = read_back(h, d_sums, 32, st, "frw_cv_walk");
     float ms = 0;
     if (!rc) cudaEventElapsedTime(&ms, e0, e1);
     if (rc) return rc;
@@ -366,7 +362,7 @@ frw_status frw_cv_destroy(frw_cv *M) {
     if (!M) return FRW_OK;
     SetDevice sd(M->view.device);
     cudaError_t e = cudaDeviceSynchronize();  // nothing may still read the table
-    cv::net_free(&M->net);
+    cv::net_free(&M->net, nullptr);
     if (M->phi) cudaFreeAsync(M->phi, nullptr);
     delete M;
     FRW_CK(e);
@@ -410,10 +406,9 @@ frw_status frw_mlp_forward(const float *params, const float *x, int64_t n, float
         for (int64_t i = 0; i < n * 16; i++) hb[i] = __float2bfloat16_rn(x[i]);
         FRW_CK(cudaMemcpyAsync(d_x, hb.data(), n * 32, cudaMemcpyHostToDevice, st));
         rc = cv::launch_forward(net, d_x, n, d_out, st);
-        if (!rc) FRW_CK(cudaMemcpyAsync(out, d_out, n * 4, cudaMemcpyDeviceToHost, st));
-        if (!rc) FRW_CK(cudaStreamSynchronize(st));
+        if (!rc) rc = read_back(out, d_out, n * 4, st, "frw_mlp_forward");
     }
-    cv::net_free(&net);
+    cv::net_free(&net, st);
     return rc;
 }
 
@@ -450,11 +445,10 @@ frw_status frw_mlp_grad(const float *params, const float *x, const float *y, con
         FRW_CK(cudaMemsetAsync(d_g, 0, cv::kParams * 4, st));
         FRW_CK(cudaMemsetAsync(d_l, 0, 8, st));
         rc = cv::launch_train_grad(net, d_x, d_y, d_wt, n, (float)inv_wsum, d_g, d_l, st);
-        if (!rc) FRW_CK(cudaMemcpyAsync(grad, d_g, cv::kParams * 4, cudaMemcpyDeviceToHost, st));
-        if (!rc && loss) FRW_CK(cudaMemcpyAsync(loss, d_l, 8, cudaMemcpyDeviceToHost, st));
-        if (!rc) FRW_CK(cudaStreamSynchronize(st));
+        if (!rc) rc = read_back(grad, d_g, cv::kParams * 4, st, "frw_mlp_grad");
+        if (!rc && loss) rc = read_back(loss, d_l, 8, st, "frw_mlp_grad");
     }
-    cv::net_free(&net);
+    cv::net_free(&net, st);
     return rc;
 }
 
@@ -477,9 +471,7 @@ frw_status frw_cv_features(const frw_layout *layout, int64_t target, const doubl
     const double *r = v.rects + 4 * target;
     rc = cv::launch_features(v.dl, make_double4(r[0], r[1], r[2], r[3]), (int)target, d_rec, n, nullptr, d_f, st);
     if (rc) return rc;
-    FRW_CK(cudaMemcpyAsync(out, d_f, n * 64, cudaMemcpyDeviceToHost, st));
-    FRW_CK(cudaStreamSynchronize(st));
-    return FRW_OK;
+    return read_back(out, d_f, n * 64, st, "frw_cv_features");
 }
 
 }  // extern "C"

@@ -179,8 +179,8 @@ struct Scratch3 {
 // on the whole chain of grid levels, which the build rules out).
 frw_status check_grid_status(const frw3_layout *L, cudaStream_t st) {
     uint32_t h = 0;
-    FRW_CK(cudaMemcpyAsync(&h, L->grid.status, 4, cudaMemcpyDeviceToHost, st));
-    FRW_CK(cudaStreamSynchronize(st));
+    frw_status rc = read_back(&h, L->grid.status, 4, st, "3-D grid status");
+    if (rc) return rc;
     if (h) {
         set_error("3-D grid: a lookup found no candidate list on any level");
         return FRW_E_KERNEL;
@@ -355,8 +355,7 @@ frw_status frw3_layout_create(const float *boxes, int64_t n, const double *bound
     }
     rc = build_grid3(L->d_boxes, n, L->bounds, cells_per_box > 0 ? cells_per_box : 8.0, st, &L->grid);
     if (rc) {
-        cudaFreeAsync(L->d_boxes, st);
-        cudaStreamSynchronize(st);
+        cudaFreeAsync(L->d_boxes, st);  // stream-ordered: after any build work still queued
         return rc;
     }
     attach_grid3(L->dl, L->grid, L->bounds);
@@ -465,9 +464,12 @@ frw_status frw3_query_batch(const frw3_layout *L, const double *pts, int64_t n, 
     FRW_CK(cudaMemcpyAsync(dp, pts, pb, cudaMemcpyHostToDevice, st));
     frw_status rc = launch_query3(L->dl, dp, n, dc, dn, st);
     if (rc) return rc;
+    rc = check_grid_status(L, st);  // bounded wait for the queries, then the grid status
+    if (rc) return rc;
     if (clear) FRW_CK(cudaMemcpyAsync(clear, dc, cb, cudaMemcpyDeviceToHost, st));
     if (nearest) FRW_CK(cudaMemcpyAsync(nearest, dn, nbt, cudaMemcpyDeviceToHost, st));
-    return check_grid_status(L, st);
+    FRW_CK(cudaStreamSynchronize(st));
+    return FRW_OK;
 }
 
 void frw3_opts_default(frw3_opts *o) {
@@ -518,8 +520,8 @@ frw_status frw3_walk(const frw3_layout *L, int64_t target, uint64_t walks, uint6
     }
     FRW_CK(cudaEventRecord(ev[1], st));
     std::vector<unsigned long long> h(5 + 3 * (size_t)n);
-    FRW_CK(cudaMemcpyAsync(h.data(), s.p, bytes, cudaMemcpyDeviceToHost, st));
-    FRW_CK(cudaStreamSynchronize(st));
+    rc = read_back(h.data(), s.p, bytes, st, "frw3_walk");
+    if (rc) return rc;
     float ms = 0;
     cudaEventElapsedTime(&ms, ev[0], ev[1]);
     const unsigned long long *stats = h.data() + 1, *hits = h.data() + 5;
@@ -657,8 +659,8 @@ frw_status frw3_walk_batch(const frw3_layout *L, const int64_t *targets, int32_t
     }
     FRW_CK(cudaEventRecord(ev[1], st));
     std::vector<unsigned long long> h(words);
-    FRW_CK(cudaMemcpyAsync(h.data(), s.p, words * 8, cudaMemcpyDeviceToHost, st));
-    FRW_CK(cudaStreamSynchronize(st));
+    rc = read_back(h.data(), s.p, words * 8, st, "frw3_walk_batch");
+    if (rc) return rc;
     rc = check_grid_status(L, st);
     if (rc) return rc;
     float ms = 0;
@@ -744,6 +746,8 @@ frw_status frw3_walk_trace(const frw3_layout *L, int64_t target, uint64_t first_
         return FRW_E_ARG;
     }
     rc = launch_walk3(P, walk_blocks(L->device, o->blocks_per_sm), st);
+    if (rc) return rc;
+    rc = wait_stream(st, "frw3_walk_trace");
     if (rc) return rc;
     if (mem == FRW_MEM_HOST) {
         if (end) FRW_CK(cudaMemcpyAsync(end, P.rec_end, W * 8, cudaMemcpyDeviceToHost, st));

@@ -13,8 +13,11 @@
 #include <time.h>
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <map>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -99,6 +102,33 @@ frw_status device_ctx(int dev, DeviceCtx **out) {
     return FRW_OK;
 }
 
+std::atomic<int64_t> g_wait_default_us{0};  // process-wide wait limit, microseconds (0: none)
+thread_local double t_wait_ms = -1.0;         // limit of the call in progress (< 0: the default)
+
+// Polls `ev` until it completes or the limit in force passes.
+frw_status poll_event(cudaEvent_t ev, const char *what) {
+    const double lim = wait_limit_ms();
+    if (lim <= 0) {
+        cudaError_t e = cudaEventSynchronize(ev);
+        return e == cudaSuccess ? FRW_OK : cuda_fail(e, what);
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int k = 0;; k++) {
+        cudaError_t e = cudaEventQuery(ev);
+        if (e == cudaSuccess) return FRW_OK;
+        if (e != cudaErrorNotReady) return cuda_fail(e, what);
+        const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        if (ms > lim) {
+            set_error(std::string(what) + ": the host wait limit of " + std::to_string(lim) +
+                      " ms passed before the device finished (its work keeps running; buffers it uses are "
+                      "released in stream order)");
+            return FRW_E_TIMEOUT;
+        }
+        if (k < 64) std::this_thread::yield();
+        else std::this_thread::sleep_for(std::chrono::microseconds(k < 1024 ? 20 : 200));
+    }
+}
+
 // The message of a nonzero kernel status word.
 frw_status status_error(uint32_t h) {
     if (h) {
@@ -116,8 +146,8 @@ frw_status status_error(uint32_t h) {
 // Reads the kernel status word (after the stream has drained).
 frw_status check_status(const uint32_t *d_status, cudaStream_t st) {
     uint32_t h = 0;
-    FRW_CK(cudaMemcpyAsync(&h, d_status, 4, cudaMemcpyDeviceToHost, st));
-    FRW_CK(cudaStreamSynchronize(st));
+    frw_status rc = read_back(&h, d_status, 4, st, "status read-back");
+    if (rc) return rc;
     return status_error(h);
 }
 
@@ -139,6 +169,10 @@ frw_status validate_opts(const frw_opts *o) {
     }
     if (!(o->gauss_param >= 0) || o->hop_cap < 1) {
         set_error("frw_opts.gauss_param / hop_cap");
+        return FRW_E_ARG;
+    }
+    if (!(o->timeout_ms >= 0)) {
+        set_error("frw_opts.timeout_ms must be >= 0");
         return FRW_E_ARG;
     }
     if (o->start_grid && o->start_mode != FRW_START_UNIFORM) {
@@ -283,8 +317,8 @@ frw_status run_walks(const frw_layout *lay, int64_t target, uint64_t first_walk,
     rc = launch_compact(d_acc_n, d_acc_s, d_acc_s2, rows, d_row, d_cn, d_cs, d_cs2, &h->cnt, st);
     if (rc) return rc;
     Hdr hh;
-    FRW_CK(cudaMemcpyAsync(&hh, h, offsetof(Hdr, tgt), cudaMemcpyDeviceToHost, st));
-    FRW_CK(cudaStreamSynchronize(st));
+    rc = read_back(&hh, h, offsetof(Hdr, tgt), st, "walk results");
+    if (rc) return rc;
     rc = status_error(hh.status);
     if (rc) return rc;
     const unsigned long long h_cnt = hh.cnt;
@@ -316,6 +350,39 @@ frw_status run_walks(const frw_layout *lay, int64_t target, uint64_t first_walk,
 }  // namespace
 
 void set_error(const std::string &msg) { g_err = msg; }
+
+double wait_limit_ms() {
+    return t_wait_ms >= 0 ? t_wait_ms : (double)g_wait_default_us.load(std::memory_order_relaxed) * 1e-3;
+}
+
+WaitScope::WaitScope(double ms) : prev(t_wait_ms) {
+    if (ms > 0) t_wait_ms = ms;
+}
+WaitScope::~WaitScope() { t_wait_ms = prev; }
+
+frw_status wait_event(cudaEvent_t ev, const char *what) { return poll_event(ev, what); }
+
+frw_status wait_stream(cudaStream_t st, const char *what) {
+    if (wait_limit_ms() <= 0) {
+        cudaError_t e = cudaStreamSynchronize(st);
+        return e == cudaSuccess ? FRW_OK : cuda_fail(e, what);
+    }
+    cudaEvent_t ev;
+    cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_fail(e, what);
+    e = cudaEventRecord(ev, st);
+    frw_status rc = e == cudaSuccess ? poll_event(ev, what) : cuda_fail(e, what);
+    cudaEventDestroy(ev);
+    return rc;
+}
+
+frw_status read_back(void *host, const void *dev, size_t bytes, cudaStream_t st, const char *what) {
+    frw_status rc = wait_stream(st, what);
+    if (rc) return rc;
+    cudaError_t e = cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // only this copy is left on the stream
+    return e == cudaSuccess ? FRW_OK : cuda_fail(e, what);
+}
 
 frw_status layout_view(const frw_layout *L, LayoutView *out) {
     if (!L) {
@@ -369,6 +436,17 @@ frw_status frw_device_check(int device) {
     DeviceCtx *c;
     return device_ctx(device, &c);
 }
+
+frw_status frw_set_wait_limit(double ms) {
+    if (!(ms >= 0) || ms > 1e12) {
+        set_error("frw_set_wait_limit: ms must be in [0, 1e12]");
+        return FRW_E_ARG;
+    }
+    g_wait_default_us.store((int64_t)(ms * 1e3), std::memory_order_relaxed);
+    return FRW_OK;
+}
+
+double frw_get_wait_limit(void) { return (double)g_wait_default_us.load(std::memory_order_relaxed) * 1e-3; }
 
 frw_status frw_green_table(double *g, double *intg) {
     green_tables(g, intg, nullptr, nullptr);
@@ -494,6 +572,35 @@ frw_status frw_layout_create(const float *rects, int64_t n, const double *bounds
     if (rc) return fail(rc);
     attach_cells(dl, L->cells);
     *out = L;
+    return FRW_OK;
+}
+
+frw_status frw_parse_layout(const char *path, int layer, double *rects_out, int64_t capacity, int64_t *n_out,
+                            double *bounds_out, int32_t *layers_out) {
+    if (!path || !n_out) {
+        set_error("frw_parse_layout: null argument");
+        return FRW_E_ARG;
+    }
+    *n_out = 0;
+    std::vector<double> r;
+    int nl = 0;
+    frw_status rc = parse_layout_file(path, layer, &r, &nl);
+    if (layers_out) *layers_out = nl;
+    if (rc) return rc;
+    const int64_t n = (int64_t)r.size() / 4;
+    *n_out = n;
+    if (bounds_out) {
+        if (n) reference_bounds(r.data(), n, bounds_out);
+        else memset(bounds_out, 0, 4 * sizeof(double));
+    }
+    if (rects_out) {
+        if (capacity < n) {
+            set_error("frw_parse_layout: layer " + std::to_string(layer) + " has " + std::to_string(n) +
+                      " rects, capacity " + std::to_string(capacity));
+            return FRW_E_ARG;
+        }
+        if (n) memcpy(rects_out, r.data(), r.size() * sizeof(double));
+    }
     return FRW_OK;
 }
 
@@ -639,11 +746,14 @@ frw_status frw_query_batch(const frw_layout *L, const double *pts, int64_t n, do
     }
     frw_status rc = launch_query(L->dl, dp, n, ds, dh, d_status, st);
     if (rc) return rc;
+    rc = check_status(d_status, st);  // bounded wait for the queries, then their status
+    if (rc) return rc;
     if (mem == FRW_MEM_HOST) {
         FRW_CK(cudaMemcpyAsync(sq, ds, n * 32, cudaMemcpyDeviceToHost, st));
         FRW_CK(cudaMemcpyAsync(hit, dh, n * 8, cudaMemcpyDeviceToHost, st));
+        FRW_CK(cudaStreamSynchronize(st));
     }
-    return check_status(d_status, st);
+    return FRW_OK;
 }
 
 frw_status frw_box_collides_batch(const frw_layout *L, const double *boxes, int64_t n, const double *ignore,
@@ -676,8 +786,13 @@ frw_status frw_box_collides_batch(const frw_layout *L, const double *boxes, int6
     }
     frw_status rc = launch_box_collides(L->dl, db, n, ignore != nullptr, ignore, dout, d_status, st);
     if (rc) return rc;
-    if (mem == FRW_MEM_HOST) FRW_CK(cudaMemcpyAsync(out, dout, n, cudaMemcpyDeviceToHost, st));
-    return check_status(d_status, st);
+    rc = check_status(d_status, st);
+    if (rc) return rc;
+    if (mem == FRW_MEM_HOST) {
+        FRW_CK(cudaMemcpyAsync(out, dout, n, cudaMemcpyDeviceToHost, st));
+        FRW_CK(cudaStreamSynchronize(st));
+    }
+    return FRW_OK;
 }
 
 frw_status frw_gauss_surface(const frw_layout *L, int64_t target, const frw_opts *opts, double out[4],
@@ -687,6 +802,7 @@ frw_status frw_gauss_surface(const frw_layout *L, int64_t target, const frw_opts
     if (opts) o = *opts;
     frw_status rc = validate_opts(&o);
     if (rc) return rc;
+    WaitScope ws(o.timeout_ms);
     if (!L || !out || target < 0 || target >= L->n) {
         set_error("frw_gauss_surface: bad arguments");
         return FRW_E_ARG;
@@ -703,8 +819,9 @@ frw_status frw_gauss_surface(const frw_layout *L, int64_t target, const frw_opts
     FRW_CK(cudaMemcpyAsync(d_t, L->rects.data() + 4 * target, 32, cudaMemcpyHostToDevice, st));
     rc = launch_gauss(L->dl, d_t, 1, o.gauss_mode, o.gauss_param, d_o, d_status, st);
     if (rc) return rc;
-    FRW_CK(cudaMemcpyAsync(out, d_o, 32, cudaMemcpyDeviceToHost, st));
-    return check_status(d_status, st);
+    rc = check_status(d_status, st);
+    if (rc) return rc;
+    return read_back(out, d_o, 32, st, "frw_gauss_surface");
 }
 
 frw_status frw_walk(const frw_layout *L, int64_t target, uint64_t walks, uint64_t seed, const frw_opts *opts,
@@ -714,6 +831,7 @@ frw_status frw_walk(const frw_layout *L, int64_t target, uint64_t walks, uint64_
     if (opts) o = *opts;
     frw_status rc = validate_opts(&o);
     if (rc) return rc;
+    WaitScope ws(o.timeout_ms);
     if (!L || !res) {
         set_error("frw_walk: null argument");
         return FRW_E_ARG;
@@ -819,6 +937,22 @@ frw_status frw_walk_device(const frw_layout *L, int64_t target, uint64_t walks, 
     return launch_walk(P, 256, blocks, st);
 }
 
+frw_status frw_rows_compact(const frw_layout *L, const uint64_t *hits, const double *sum_w, const double *sum_w2,
+                            int64_t capacity, int64_t *idx, uint64_t *out_hits, double *out_sum_w, double *out_sum_w2,
+                            uint64_t *count, void *stream) {
+    if (!L || !hits || !sum_w || !sum_w2 || !count || capacity < 0 ||
+        (capacity > 0 && (!idx || !out_hits || !out_sum_w || !out_sum_w2))) {
+        set_error("frw_rows_compact: null argument or negative capacity");
+        return FRW_E_ARG;
+    }
+    DeviceGuard g(L->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    FRW_CK(cudaMemsetAsync(count, 0, 8, st));
+    return launch_compact(reinterpret_cast<const unsigned long long *>(hits), sum_w, sum_w2, L->n, idx,
+                          reinterpret_cast<unsigned long long *>(out_hits), out_sum_w, out_sum_w2,
+                          reinterpret_cast<unsigned long long *>(count), st, capacity);
+}
+
 frw_status frw_walk_trace(const frw_layout *L, int64_t target, uint64_t first_walk, uint64_t walks, uint64_t seed,
                           const frw_opts *opts, int64_t *end, int32_t *hops, int32_t *bin1, double *weight,
                           int mem, void *stream) {
@@ -827,6 +961,7 @@ frw_status frw_walk_trace(const frw_layout *L, int64_t target, uint64_t first_wa
     if (opts) o = *opts;
     frw_status rc = validate_opts(&o);
     if (rc) return rc;
+    WaitScope ws(o.timeout_ms);
     if (!L) {
         set_error("frw_walk_trace: null layout");
         return FRW_E_ARG;

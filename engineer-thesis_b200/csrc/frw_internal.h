@@ -114,6 +114,26 @@ struct WalkParams {
 void set_error(const std::string &msg);
 frw_status cuda_fail(cudaError_t e, const char *what);
 
+// Bounded host waits.  The limit in force on the calling thread (ms; <= 0:
+// none) is the process-wide default (frw_set_wait_limit) unless a WaitScope
+// set another for the call.  A wait that outlives it returns FRW_E_TIMEOUT
+// and leaves the stream's work running: every buffer that work uses is
+// released in stream order (cudaFreeAsync on the same stream), so nothing is
+// freed under it, and no copy into host memory has been enqueued yet (reads
+// of device results always come after a completed wait).
+double wait_limit_ms();
+struct WaitScope {
+    double prev;
+    explicit WaitScope(double ms);  // ms <= 0 keeps the limit in force
+    ~WaitScope();
+};
+// Waits until everything enqueued on `st` so far has finished.
+frw_status wait_stream(cudaStream_t st, const char *what);
+// Waits for a recorded event.
+frw_status wait_event(cudaEvent_t e, const char *what);
+// Bounded wait for `st`, then a synchronous copy of a small device result.
+frw_status read_back(void *host, const void *dev, size_t bytes, cudaStream_t st, const char *what);
+
 // CUDA events destroyed at scope exit, error paths included.
 struct Events {
     cudaEvent_t e[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -197,10 +217,11 @@ frw_status launch_gauss_jobs(const WalkJob *d_jobs, const double *d_targets, int
 // walk.cu
 frw_status launch_walk(const WalkParams &P, int threads, int blocks, cudaStream_t stream);
 int walk_max_blocks_per_sm(int threads, bool multi);
-// Compacts the nonzero accumulator rows: returns their count through *d_count.
+// Compacts the nonzero accumulator rows (at most cap of them written; cap < 0:
+// rows): their count, written or not, goes to *d_count.
 frw_status launch_compact(const unsigned long long *acc_n, const double *acc_s, const double *acc_s2,
                           int64_t rows, int64_t *out_row, unsigned long long *out_n, double *out_s,
-                          double *out_s2, unsigned long long *d_count, cudaStream_t stream);
+                          double *out_s2, unsigned long long *d_count, cudaStream_t stream, int64_t cap = -1);
 
 // host_green.cpp
 void green_tables(double *g, double *intg, double *wx, double *wy);

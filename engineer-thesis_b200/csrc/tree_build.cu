@@ -464,9 +464,8 @@ frw_status build_tree(const float4 *d_rects_in, int32_t n, const double bounds[4
                                               reinterpret_cast<int *>(tot));
             if (!ck(cudaGetLastError(), "split")) break;
             int h[4] = {0, 0, 0, 0};
-            if (!ck(cudaMemcpyAsync(h, tot, 16, cudaMemcpyDeviceToHost, st), "split result")) break;
             if (!ck(cudaEventRecord(e1, st), "event")) break;
-            if (!ck(cudaEventSynchronize(e1), "build sync")) break;
+            if ((rc = read_back(h, tot, 16, st, "build_tree: split result"))) break;
             if (h[2]) {
                 set_error("build_tree: too many levels");
                 rc = FRW_E_KERNEL;
@@ -496,8 +495,7 @@ frw_status build_tree(const float4 *d_rects_in, int32_t n, const double bounds[4
             k_split_count<<<(nfr + 255) / 256, 256, 0, st>>>(k0, fa, nfr, leaf_max, cnt);
             k_scan_excl<unsigned long long><<<1, 1024, 0, st>>>(cnt, nfr, tot);
             unsigned long long h_tot = 0;
-            if (!ck(cudaMemcpyAsync(&h_tot, tot, 8, cudaMemcpyDeviceToHost, st), "scan total")) break;
-            if (!ck(cudaStreamSynchronize(st), "split sync")) break;
+            if ((rc = read_back(&h_tot, tot, 8, st, "build_tree: scan total"))) break;
             int new_nodes = (int)(h_tot >> 32), next = (int)(h_tot & 0xFFFFFFFFull);
             k_split_emit<<<(nfr + 255) / 256, 256, 0, st>>>(k0, fa, nfr, leaf_max, cnt, nodes, T.nref, fb);
             if (!ck(cudaGetLastError(), "split")) break;
@@ -520,7 +518,7 @@ frw_status build_tree(const float4 *d_rects_in, int32_t n, const double bounds[4
         T.depth = depth;
         T.bytes = (int64_t)n * 20 + (int64_t)nodes * 80;
         if (!ck(cudaEventRecord(e1, st), "event")) break;
-        if (!ck(cudaEventSynchronize(e1), "build sync")) break;
+        if ((rc = wait_event(e1, "build_tree"))) break;
         float ms = 0;
         cudaEventElapsedTime(&ms, e0, e1);
         if (build_ms) *build_ms = ms;

@@ -410,10 +410,12 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
     if (st) atomicOr(P.status, st);
 }
 
+// Rows with a nonzero count, in no particular order; entries past `cap` are
+// counted but not written (the caller compares *count with cap).
 __global__ void k_compact(const unsigned long long *__restrict__ acc_n, const double *__restrict__ acc_s,
                           const double *__restrict__ acc_s2, int64_t rows, int64_t *__restrict__ out_row,
                           unsigned long long *__restrict__ out_n, double *__restrict__ out_s,
-                          double *__restrict__ out_s2, unsigned long long *count) {
+                          double *__restrict__ out_s2, unsigned long long *count, unsigned long long cap) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const bool keep = i < rows && acc_n[i] > 0;
     const unsigned m = __ballot_sync(kFull, keep);
@@ -422,8 +424,8 @@ __global__ void k_compact(const unsigned long long *__restrict__ acc_n, const do
     unsigned long long base = 0;
     if (lane == leader) base = atomicAdd(count, (unsigned long long)__popc(m));
     base = __shfl_sync(kFull, base, leader);
-    if (keep) {
-        const unsigned long long o = base + __popc(m & ((1u << lane) - 1u));
+    const unsigned long long o = base + __popc(m & ((1u << lane) - 1u));
+    if (keep && o < cap) {
         out_row[o] = i;
         out_n[o] = acc_n[i];
         out_s[o] = acc_s[i];
@@ -453,10 +455,11 @@ frw_status launch_walk(const WalkParams &P, int threads, int blocks, cudaStream_
 
 frw_status launch_compact(const unsigned long long *acc_n, const double *acc_s, const double *acc_s2,
                           int64_t rows, int64_t *out_row, unsigned long long *out_n, double *out_s,
-                          double *out_s2, unsigned long long *d_count, cudaStream_t stream) {
+                          double *out_s2, unsigned long long *d_count, cudaStream_t stream, int64_t cap) {
     if (rows <= 0) return FRW_OK;
     k_compact<<<(unsigned)((rows + 255) / 256), 256, 0, stream>>>(acc_n, acc_s, acc_s2, rows, out_row, out_n,
-                                                                  out_s, out_s2, d_count);
+                                                                  out_s, out_s2, d_count,
+                                                                  (unsigned long long)(cap < 0 ? rows : cap));
     FRW_CK(cudaGetLastError());
     return FRW_OK;
 }

@@ -687,8 +687,7 @@ frw_status build_level(const float *d_boxes, int64_t n, const Grid3 &G, const ui
         launch_scan_i64(bcnt, ncells + 1, bstart, sums, grand, st);
         if (!ck(cudaGetLastError(), "bin count")) break;
         int64_t nitems = 0;
-        if (!ck(cudaMemcpyAsync(&nitems, grand, 8, cudaMemcpyDeviceToHost, st), "bin total")) break;
-        if (!ck(cudaStreamSynchronize(st), "bin total")) break;
+        if ((rc = read_back(&nitems, grand, 8, st, "build_grid3: bin total"))) break;
         if (nitems > INT32_MAX) {
             set_error("build_grid3: more than 2^31 bin entries; use fewer cells per box");
             rc = FRW_E_ARG;
@@ -705,9 +704,8 @@ frw_status build_level(const float *d_boxes, int64_t n, const Grid3 &G, const ui
         if (!ck(cudaGetLastError(), "cell count")) break;
         int64_t total = 0;
         unsigned long long ndef = 0;
-        if (!ck(cudaMemcpyAsync(&total, grand + 1, 8, cudaMemcpyDeviceToHost, st), "list total")) break;
-        if (!ck(cudaMemcpyAsync(&ndef, dev_stats, 8, cudaMemcpyDeviceToHost, st), "deferred")) break;
-        if (!ck(cudaStreamSynchronize(st), "list total")) break;
+        if ((rc = read_back(&total, grand + 1, 8, st, "build_grid3: list total"))) break;
+        if ((rc = read_back(&ndef, dev_stats, 8, st, "build_grid3: deferred cells"))) break;
         if (total > (int64_t)INT32_MAX) {
             set_error("build_grid3: more than 2^31 list entries; use fewer cells per box");
             rc = FRW_E_ARG;
@@ -720,8 +718,7 @@ frw_status build_level(const float *d_boxes, int64_t n, const Grid3 &G, const ui
                                                  nullptr, nullptr, lstart, out->lists);
         k3_cells_pack<<<cbk, 128, 0, st>>>(lstart, lcnt, flag, ncells, out->cells, dev_stats + 1);
         if (!ck(cudaGetLastError(), "cell fill")) break;
-        if (!ck(cudaMemcpyAsync(&out->max_list, dev_stats + 1, 8, cudaMemcpyDeviceToHost, st), "max list")) break;
-        if (!ck(cudaStreamSynchronize(st), "grid level")) break;
+        if ((rc = read_back(&out->max_list, dev_stats + 1, 8, st, "build_grid3: longest list"))) break;
     } while (0);
     for (void *p : {(void *)bcnt, (void *)bstart, (void *)lcnt, (void *)lstart, (void *)sums, (void *)grand,
                     (void *)items, (void *)flag, (void *)dev_stats})
@@ -850,7 +847,7 @@ frw_status build_grid3(const float *d_boxes, int64_t n, const double bounds[6], 
                 break;
         }
         if (!ck(cudaEventRecord(ev[1], st), "event")) break;
-        if (!ck(cudaEventSynchronize(ev[1]), "grid sync")) break;
+        if ((rc = wait_event(ev[1], "build_grid3"))) break;
         B.max_list = (int32_t)max_list;
         cudaEventElapsedTime(&B.build_ms, ev[0], ev[1]);
     } while (0);

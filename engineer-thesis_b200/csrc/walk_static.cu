@@ -139,17 +139,17 @@ extern "C" frw_status frw_walk_trace_static(const frw_layout *layout, int64_t ta
         rc = launch_walk(P, 256, (int)blocks, st);
     }
     if (!rc) {
-        // status word and completed-walk count (host stack, no allocation)
+        // status word and completed-walk count (host stack, no allocation),
+        // read once the stream has drained within the call's wait limit
+        WaitScope ws(o.timeout_ms);
         uint32_t h_status = 0;
         unsigned long long h_stats[4] = {0, 0, 0, 0};
-        e = cudaMemcpyAsync(&h_status, status, 4, cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(h_stats, stats, 32, cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) rc = cuda_fail(e, "frw_walk_trace_static: result read-back");
-        else if (h_status) {
+        rc = read_back(&h_status, status, 4, st, "frw_walk_trace_static");
+        if (!rc) rc = read_back(h_stats, stats, 32, st, "frw_walk_trace_static");
+        if (!rc && h_status) {
             set_error("frw_walk_trace_static: kernel reported an internal limit");
             rc = FRW_E_KERNEL;
-        } else if (h_stats[3] != walks) {
+        } else if (!rc && h_stats[3] != walks) {
             set_error("frw_walk_trace_static: walk kernel did not finish every walk");
             rc = FRW_E_KERNEL;
         }

@@ -65,6 +65,7 @@ class Opts(C.Structure):
         ("start_grid", C.c_uint32),
         ("first_walk", C.c_uint64),
         ("start_strata", C.c_uint32),
+        ("timeout_ms", C.c_double),
     ]
 
 
@@ -230,6 +231,10 @@ _SIGS = {
     "frw_device_check": ([C.c_int], C.c_int),
     "frw_green_table": ([_D, _D], C.c_int),
     "frw_layout_from_file": ([C.c_char_p, C.c_int, C.c_int, C.POINTER(_VP)], C.c_int),
+    "frw_rows_compact": ([_VP, _VP, _VP, _VP, C.c_int64, _VP, _VP, _VP, _VP, _VP, _VP], C.c_int),
+    "frw_set_wait_limit": ([C.c_double], C.c_int),
+    "frw_get_wait_limit": ([], C.c_double),
+    "frw_parse_layout": ([C.c_char_p, C.c_int, _D, C.c_int64, _I64, _D, _I32], C.c_int),
     "frw_layout_create": ([_F, C.c_int64, _D, C.c_int, _VP, C.POINTER(_VP)], C.c_int),
     "frw_layout_destroy": ([_VP], C.c_int),
     "frw_layout_info_get": ([_VP, C.POINTER(LayoutInfo)], C.c_int),
@@ -322,6 +327,15 @@ def device_check(device: int = 0) -> None:
     _check(lib().frw_device_check(device))
 
 
+def set_wait_limit(ms: float) -> None:
+    """Process-wide bound on the library's host waits (0: none); see frw.h."""
+    _check(lib().frw_set_wait_limit(float(ms)))
+
+
+def wait_limit() -> float:
+    return float(lib().frw_get_wait_limit())
+
+
 def green_table():
     """(g[200], intg[201]) -- precompute_unit_square_green's g and intg."""
     g = np.zeros(NSAMPLE)
@@ -332,7 +346,7 @@ def green_table():
 
 def opts(gauss_mode=GAUSS_SCALE, gauss_param=1.5, start_mode=START_GREEN, exact_perimeter=False,
          hop_cap=100000, stream_id=0, blocks_per_sm=0, refill_min=1, permittivity=PERMITTIVITY,
-         start_grid=0, first_walk=0, start_strata=0) -> Opts:
+         start_grid=0, first_walk=0, start_strata=0, timeout_ms=0.0) -> Opts:
     o = Opts()
     lib().frw_opts_default(C.byref(o))
     o.gauss_mode = gauss_mode
@@ -347,6 +361,7 @@ def opts(gauss_mode=GAUSS_SCALE, gauss_param=1.5, start_mode=START_GREEN, exact_
     o.start_grid = start_grid
     o.first_walk = first_walk
     o.start_strata = start_strata
+    o.timeout_ms = timeout_ms
     return o
 
 
@@ -359,6 +374,18 @@ def generate_layout(seed: int, n: int, domain: float, wmin: int = 5, wmax: int =
     out = np.zeros((n, 4), dtype=np.float32)
     _check(lib().frw_generate_layout(seed, n, domain, wmin, wmax, gap, _ptr(out, _F)))
     return out
+
+
+def parse_layout(path: str, layer: int = 0):
+    """The product's layout reader on the host (Parser::parse + getLayerAt +
+    getLayerSize): (rects (n, 4) float64 in file order, bounds[4], layers)."""
+    n = C.c_int64()
+    nl = C.c_int32()
+    b = np.zeros(4)
+    _check(lib().frw_parse_layout(path.encode(), layer, None, 0, C.byref(n), _ptr(b, _D), C.byref(nl)))
+    out = np.zeros((n.value, 4))
+    _check(lib().frw_parse_layout(path.encode(), layer, _ptr(out, _D), n.value, C.byref(n), None, None))
+    return out, b, int(nl.value)
 
 
 def write_layout(path: str, rects, name: str = "layer") -> None:
@@ -522,6 +549,16 @@ class Layout:
                                      C.c_void_p(hits.data_ptr()), C.c_void_p(sum_w.data_ptr()),
                                      C.c_void_p(sum_w2.data_ptr()), C.c_void_p(stats.data_ptr()),
                                      C.c_void_p(status.data_ptr()), stream or None))
+
+    def rows_compact(self, hits, sum_w, sum_w2, idx, out_hits, out_sum_w, out_sum_w2, count, stream: int = 0):
+        """frw_rows_compact on torch CUDA tensors: the nonzero rows of
+        frw_walk_device's arrays, at most len(idx) of them, count (uint64[1])
+        = how many there are.  Stream-ordered, no sync."""
+        _check(lib().frw_rows_compact(self._h, C.c_void_p(hits.data_ptr()), C.c_void_p(sum_w.data_ptr()),
+                                      C.c_void_p(sum_w2.data_ptr()), idx.shape[0], C.c_void_p(idx.data_ptr()),
+                                      C.c_void_p(out_hits.data_ptr()), C.c_void_p(out_sum_w.data_ptr()),
+                                      C.c_void_p(out_sum_w2.data_ptr()), C.c_void_p(count.data_ptr()),
+                                      stream or None))
 
     def cv_features(self, target: int, rec4) -> np.ndarray:
         q = np.ascontiguousarray(rec4, dtype=np.float64).reshape(-1, 4)
@@ -737,6 +774,7 @@ def opts3(gauss_offset=1.0, shell=0.0, hop_cap=100000, permittivity=PERMITTIVITY
     o.blocks_per_sm = blocks_per_sm
     o.refill_min = refill_min
     o.start_strata = start_strata
+    o.timeout_ms = timeout_ms
     return o
 
 

@@ -12,6 +12,8 @@
  *   frw_layout_from_file / frw_layout_create   <- createQuadTree
  *       (Cuda/mainkernels.h:10, Cuda/createquadtree.cu:16-87) and the layout
  *       reader d_Parser/Parser (Cuda/d_parser.cpp:16-130, CPU/Parser.cpp:15-125)
+ *   frw_parse_layout                           <- Parser::parse + getLayerAt +
+ *       getLayerSize (CPU/Parser.cpp:15-87), host only
  *   frw_layout_destroy                         <- freeQuadTreeManager
  *       (Cuda/mainkernels.h:13, Cuda/freequadtreemanager.cu:3-11)
  *   frw_query_batch                            <- d_QuadTree::drawBiggestSquareAtPoint
@@ -49,7 +51,7 @@ typedef int frw_status;
 #define FRW_E_CUDA (-3)     /* a CUDA runtime call failed */
 #define FRW_E_OOM (-4)      /* device or host allocation failed */
 #define FRW_E_HOPCAP (-5)   /* reserved: walks hit the hop cap (reported as counts, not failure) */
-#define FRW_E_TIMEOUT (-6)  /* a bounded host wait expired */
+#define FRW_E_TIMEOUT (-6)  /* a bounded host wait expired (frw_set_wait_limit, frw_opts.timeout_ms) */
 #define FRW_E_DEVICE (-7)   /* no usable sm_100 device */
 #define FRW_E_KERNEL (-8)   /* a kernel reported an internal limit (see frw_last_error) */
 
@@ -64,6 +66,18 @@ const char *frw_last_error(void);
  * reference's SM >= 3.5 dynamic-parallelism check, Cuda/initCuda.cu:14-31). */
 frw_status frw_device_check(int device);
 
+/* Bound on every host wait of the library, in ms (0, the default: none);
+ * a call's frw_opts.timeout_ms, when set, replaces it for that call.  When a
+ * wait passes the bound the call returns FRW_E_TIMEOUT: its device work keeps
+ * running, ordered before later work on the same stream; the buffers that
+ * work uses are released only after it (stream-ordered frees), and no result
+ * has been copied into caller memory.  The destroy calls (frw_layout_destroy,
+ * frw_cv_destroy, frw_batch_destroy, frw3_layout_destroy) wait for the device
+ * without a bound, like cudaFree.  The reference has no such bound: its
+ * wrappers end in cudaDeviceSynchronize (Cuda/getAvgPathLenCUDA.cu:50-80). */
+frw_status frw_set_wait_limit(double ms);
+double frw_get_wait_limit(void);
+
 /* ---- Green's function table ---- */
 /* g[FRW_NSAMPLE] and the normalised cumulative intg[FRW_NSAMPLE+1] of the
  * unit-square surface Green's function seen from the centre; bit-identical to
@@ -76,6 +90,19 @@ frw_status frw_green_table(double *g, double *intg);
  * computes the reference bounds (bbox grown by int(0.01*width) on both axes,
  * CPU/Parser.cpp:51-87) and builds the device quadtree on `device`. */
 frw_status frw_layout_from_file(const char *path, int layer, int device, frw_layout **out);
+/* The reader alone, on the host (no device is touched): Parser::parse +
+ * getLayerAt + getLayerSize (CPU/Parser.cpp:15-87) for layer `layer` of
+ * `path`.  *n_out receives the layer's rect count; when rects_out is not NULL
+ * and capacity >= *n_out, the rects (file order, n*4 doubles) are written
+ * there, else FRW_E_ARG reports the count needed.  bounds_out (nullable)
+ * receives the reference bounds, layers_out (nullable) the number of closed
+ * layers.  As in the reference, a line of 50 or more characters ends the
+ * reading (std::istream::getline into a 50-byte buffer fails there) and the
+ * lines after it are ignored.  A rect line without exactly four numbers
+ * (undefined in the reference) is FRW_E_IO with its line number; a layer
+ * that the file does not close is FRW_E_ARG. */
+frw_status frw_parse_layout(const char *path, int layer, double *rects_out, int64_t capacity, int64_t *n_out,
+                            double *bounds_out, int32_t *layers_out);
 /* rects_xyxy: host array of n*4 floats (x0,y0,x1,y1), y downwards; every
  * coordinate must be an integer-or-float value exactly representable in
  * FP32 with |c| < 2^24.  bounds: NULL for the reference rule, else 4
@@ -172,6 +199,8 @@ typedef struct frw_opts {
                                 for either start mode.  Unbiased when the walk range covers every
                                 stratum equally (walks and first_walk multiples of S); the reported
                                 standard error stays the i.i.d. one, an upper bound. */
+    double timeout_ms;       /* bound on this call's host waits, in ms (0: the process-wide limit of
+                                frw_set_wait_limit, by default none); see frw_set_wait_limit */
 } frw_opts;
 void frw_opts_default(frw_opts *opts);
 
@@ -217,6 +246,19 @@ frw_status frw_walk_device(const frw_layout *layout, int64_t target, uint64_t wa
                            const frw_opts *opts, uint64_t *hits, double *sum_w, double *sum_w2,
                            uint64_t *stats, uint32_t *status, void *stream);
 
+/* Sparse form of frw_walk_device's rows, for the multi-GPU exchange (no
+ * reference counterpart: the reference runs on one GPU).  For every conductor
+ * k of the layout with hits[k] > 0 one entry (k, hits[k], sum_w[k],
+ * sum_w2[k]) goes to the DEVICE arrays idx, out_hits, out_sum_w, out_sum_w2,
+ * in no particular order, at most `capacity` of them; *count (device) is set
+ * to the number of such conductors, written or not -- above `capacity` the
+ * caller has to retry with more room.  Stream-ordered, no host sync.  A
+ * step's walks reach a few hundred conductors of a 10^6-rect layout, so
+ * ranks exchange these entries instead of 3 * n dense numbers. */
+frw_status frw_rows_compact(const frw_layout *layout, const uint64_t *hits, const double *sum_w,
+                            const double *sum_w2, int64_t capacity, int64_t *idx, uint64_t *out_hits,
+                            double *out_sum_w, double *out_sum_w2, uint64_t *count, void *stream);
+
 /* Same walks with per-walk records (device or host arrays of `walks`
  * entries; any may be NULL): end conductor (layer index, -1 escaped,
  * -2 aborted), hop count, first-hop bin and the walk's capacitance weight
@@ -239,10 +281,13 @@ frw_status frw_walk_trace(const frw_layout *layout, int64_t target, uint64_t fir
  * (1.5 MiB, held by every GPU that loads the library until exit); larger
  * layouts are rejected with FRW_E_ARG.  The first call on a device resolves
  * the array's address (cudaGetSymbolAddress) -- make that first call before
- * any stream capture.  All calls share the array and the call clears it
- * first, so calls that overlap on the GPU (other streams or threads) race:
- * serialise them.  Returns after the stream has drained (the kernel status
- * word is checked).  Results equal frw_walk_trace's. */
+ * any stream capture.  The address is kept for the life of the process: a
+ * host application that resets the device (cudaDeviceReset) must not call
+ * this entry point on that device afterwards.  All calls share the array and
+ * the call clears it first, so calls that overlap on the GPU (other streams
+ * or threads) race: serialise them.  Returns after the stream has drained
+ * (the kernel status word is checked; opts->timeout_ms bounds that wait).
+ * Results equal frw_walk_trace's. */
 frw_status frw_walk_trace_static(const frw_layout *layout, int64_t target, uint64_t first_walk,
                                  uint64_t walks, uint64_t seed, const frw_opts *opts, int64_t *end,
                                  int32_t *hops, int32_t *bin1, double *weight, void *stream);

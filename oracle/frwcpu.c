@@ -902,3 +902,78 @@ void oc_cv_features(const double *rects, int64_t n, int64_t target, const double
         else for (int q = 8; q < 16; q++) f[q] = 16.f;
     }
 }
+
+/* ---------------------------------------------------------------- layouts */
+/* splitmix64 (Steele, Lea and Flood, "Fast splittable pseudorandom number
+ * generators", OOPSLA 2014). */
+static uint64_t sm64_next(uint64_t *s) {
+    uint64_t z = (*s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+static int64_t sm64_range(uint64_t *s, int64_t a, int64_t b) {
+    return a + (int64_t)(sm64_next(s) % (uint64_t)(b - a + 1));
+}
+
+/* Rejection against accepted rects bucketed by the cell of their lower
+ * corner; cells are wider than wmax + gap, so every rect within `gap` of a
+ * candidate has its lower corner in the candidate's cell range widened by
+ * one cell on each side. */
+int oc_generate_layout(uint64_t seed, int64_t n, double domain, int wmin, int wmax, double gap,
+                       double *out) {
+    if (n <= 0 || wmin < 1 || wmax < wmin || domain < wmax || gap < 0 || domain >= 16777216.0)
+        return OC_E_ARG;
+    const int64_t D = (int64_t)floor(domain);
+    const int64_t cs = (int64_t)wmax + (int64_t)ceil(gap) + 1;
+    const int64_t nc = D / cs + 1;
+    if (nc > (1 << 20)) return OC_E_ARG;
+    int32_t *head = (int32_t *)malloc((size_t)(nc * nc) * sizeof(int32_t));
+    int32_t *next = (int32_t *)malloc((size_t)n * sizeof(int32_t));
+    if (!head || !next) {
+        free(head);
+        free(next);
+        return OC_E_OOM;
+    }
+    for (int64_t i = 0; i < nc * nc; i++) head[i] = -1;
+    uint64_t s = seed;
+    int64_t got = 0, tries = 0;
+    int rc = OC_OK;
+    while (got < n) {
+        if (++tries > 64 * n + 1000) {
+            rc = OC_E_ARG;
+            break;
+        }
+        const int64_t w = sm64_range(&s, wmin, wmax), h = sm64_range(&s, wmin, wmax);
+        const int64_t x0 = sm64_range(&s, 0, D - w), y0 = sm64_range(&s, 0, D - h);
+        const int64_t x1 = x0 + w, y1 = y0 + h;
+        int64_t ax = x0 / cs - 1, bx = x0 / cs + 1, ay = y0 / cs - 1, by = y0 / cs + 1;
+        if (ax < 0) ax = 0;
+        if (ay < 0) ay = 0;
+        if (bx > nc - 1) bx = nc - 1;
+        if (by > nc - 1) by = nc - 1;
+        int ok = 1;
+        for (int64_t cy = ay; cy <= by && ok; cy++)
+            for (int64_t cx = ax; cx <= bx && ok; cx++)
+                for (int32_t j = head[cy * nc + cx]; j >= 0 && ok; j = next[j]) {
+                    const double *q = out + 4 * (int64_t)j;
+                    const double gx = fmax(q[0] - (double)x1, (double)x0 - q[2]);
+                    const double gy = fmax(q[1] - (double)y1, (double)y0 - q[3]);
+                    if (fmax(gx, gy) < gap) ok = 0;
+                }
+        if (!ok) continue;
+        double *o = out + 4 * got;
+        o[0] = (double)x0;
+        o[1] = (double)y0;
+        o[2] = (double)x1;
+        o[3] = (double)y1;
+        const int64_t c = (y0 / cs) * nc + x0 / cs;
+        next[got] = head[c];
+        head[c] = (int32_t)got;
+        got++;
+    }
+    free(head);
+    free(next);
+    return rc;
+}

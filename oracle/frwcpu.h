@@ -159,6 +159,19 @@ int64_t oc_walk_stream(const oc_grid *g, const oc_rtree *t, int defect,
                        const double gauss[4], const double *intg, const double *r,
                        int64_t nr, int64_t *used, int32_t *hops);
 
+/* ---- synthetic layouts ---- */
+/* The benchmark layouts, restated from the product's generator contract
+ * (include/frw.h, frw_generate_layout) so that CPU-side legs can make the
+ * same rects without loading the product library: a splitmix64 stream from
+ * `seed`; per attempt w = U[wmin, wmax], h = U[wmin, wmax], x0 = U[0, D - w],
+ * y0 = U[0, D - h] (U[a, b] = a + next() mod (b - a + 1), D = floor(domain));
+ * accepted when the L-infinity gap to every accepted rect is >= gap.  Writes
+ * n*4 doubles (integers); returns OC_E_ARG when 64*n + 1000 attempts do not
+ * place n rects.  The reference's own generator (utils/TestGenerator.cpp:
+ * 49-105, sizes 1-24, no gap) is not used by any benchmark config. */
+int oc_generate_layout(uint64_t seed, int64_t n, double domain, int wmin, int wmax, double gap,
+                       double *out);
+
 /* ---- control-variate features ---- */
 /* For each point rec4[i] = (x, y, a0, unused): (dx, dy) from the point to the
  * nearest point of each edge (top, right, bottom, left) of rect `target`,

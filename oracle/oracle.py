@@ -18,7 +18,15 @@ import subprocess
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_SRC = "/root/reference/randomWalk"
+
+
+def reference_root() -> str:
+    """The reference checkout: $REFERENCE, else the default of oracle/Makefile."""
+    if os.environ.get("REFERENCE"):
+        return os.environ["REFERENCE"]
+    out = subprocess.run(["make", "-s", "--no-print-directory", "-C", HERE, "print-reference"],
+                         capture_output=True, text=True)
+    return out.stdout.strip()
 
 NSAMPLE = 200
 END_ESCAPED = -1
@@ -40,8 +48,8 @@ def _p(a, t=_D):
 def build(ref: bool = True) -> None:
     """Compile liboracle.so, and the reference library when its sources exist."""
     subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
-    if ref and os.path.isdir(REF_SRC):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    if ref:
+        subprocess.run(["make", "-s", "-C", HERE, "ref-if-present"], check=True)
 
 
 class WalkCfg(C.Structure):
@@ -121,6 +129,7 @@ def lib():
                                      _I64, _I32]
         L.oc_walk_stream.restype = C.c_int64
         L.oc_cv_features.argtypes = [_D, C.c_int64, C.c_int64, _D, C.c_int64, C.POINTER(C.c_float)]
+        L.oc_generate_layout.argtypes = [C.c_uint64, C.c_int64, C.c_double, C.c_int, C.c_int, C.c_double, _D]
         L.oc3_cube_green_table.argtypes = [C.c_int, _D, _D, _D, _D, _D]
         L.oc3_green_cube.argtypes = [C.c_double, C.c_double, C.c_double]
         L.oc3_green_cube.restype = C.c_double
@@ -190,6 +199,17 @@ def point_from_index(sq, index: int, exact_perimeter: bool = False):
     o = np.zeros(2)
     lib().oc_point_from_index(_p(s), int(index), NSAMPLE, int(exact_perimeter), _p(o))
     return o
+
+
+def generate_layout(seed: int, n: int, domain: float, wmin: int = 5, wmax: int = 50,
+                    gap: float = 2.0) -> np.ndarray:
+    """The benchmark layout generator restated in C (n x 4 float64, integer
+    corners); equal to the product's frw_generate_layout rect for rect."""
+    out = np.zeros((int(n), 4))
+    rc = lib().oc_generate_layout(int(seed), int(n), float(domain), int(wmin), int(wmax), float(gap), _p(out))
+    if rc != 0:
+        raise ValueError(f"oc_generate_layout -> {rc}")
+    return out
 
 
 class Grid:

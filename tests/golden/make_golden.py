@@ -18,10 +18,16 @@ reference sources), then records:
   up to 16 targets;
 * a few hundred reference walks (RandomWalk's body, JKISS seeded once) with
   the uniform stream they consumed, their end rect and hop count.
+
+The fixture layout files themselves are copied, unchanged, to
+tests/golden/layouts/ so that the product's own reader can be checked against
+the rects and bounds above on machines without the reference checkout.  The
+checkout is $REFERENCE, else the default of oracle/Makefile.
 """
 from __future__ import annotations
 
 import os
+import shutil
 import sys
 
 import numpy as np
@@ -31,7 +37,8 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 import oracle as O  # noqa: E402
 
-REF_ROOT = "/root/reference"
+REF_ROOT = O.reference_root()
+LAYOUTS = os.path.join(HERE, "layouts")
 FIXTURES = [
     ("test", "tests/test", 10, 300),
     ("test1", "tests/test1", 5, 300),
@@ -56,8 +63,15 @@ def query_points(rects, b, rng, n=2000):
     return pts
 
 
+def copy_layouts():
+    os.makedirs(LAYOUTS, exist_ok=True)
+    for name, rel, _, _ in FIXTURES:
+        shutil.copyfile(os.path.join(REF_ROOT, rel), os.path.join(LAYOUTS, name))
+
+
 def main():
     O.build(ref=True)
+    copy_layouts()
     for name, rel, target, nwalks in FIXTURES:
         path = os.path.join(REF_ROOT, rel)
         R = O.Ref(path=path)

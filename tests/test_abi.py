@@ -92,3 +92,14 @@ def test_bad_layout_arguments_rejected_before_device():
     with pytest.raises(frw.FrwError) as e:
         frw.Layout.from_file("/nonexistent/layout")
     assert e.value.status == frw.E_IO
+
+
+@pytest.mark.parametrize("seed,n,domain", [(0xF4A7 + 1, 100, 1000.0), (0xF4A7 + 2, 10_000, 1e4),
+                                           (0xF4A7 + 3, 1_000_000, 1e5), (5, 70_000, 2e4)])
+def test_oracle_generator_equals_product_generator(seed, n, domain):
+    # the CPU legs of the benchmark make their layouts with the oracle's
+    # generator (no product library in those processes): it must give the
+    # product's rects exactly, including the 10^6-rect layout
+    a = O.generate_layout(seed, n, domain)
+    b = frw.generate_layout(seed, n, domain)
+    assert a.shape == (n, 4) and np.array_equal(a, b.astype(np.float64))

@@ -107,3 +107,54 @@ def test_failed_rank_ends_peer_collective_with_error(tmp_path):
     assert os.path.exists(out + ".err1")
     # rank 0's all-reduce either raised (peer gone / timeout) or never produced rows
     assert os.path.exists(out + ".err0") or not os.path.exists(out)
+
+
+def _sparse_worker(rank, world, port, n_walks, out_path):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=10))
+    sys.path.insert(0, os.path.join(ROOT, "engineer-thesis_b200"))
+    from frw import shard
+
+    try:
+        n = len(_layout())
+        v = _oracle_rows(rank, n_walks)  # [hits | sum_w | sum_w2 | walks, escaped, hops, 0]
+        rows_i = torch.zeros(n + 4, dtype=torch.int64)
+        rows_f = torch.zeros(2 * n, dtype=torch.float64)
+        rows_i[:n] = torch.as_tensor(v[:n]).to(torch.int64)
+        rows_f[:n] = torch.as_tensor(v[n:2 * n])
+        rows_f[n:] = torch.as_tensor(v[2 * n:3 * n])
+        rows_i[n:] = torch.as_tensor([int(v[3 * n + 2]), 0, 0, int(v[3 * n])])  # escaped-ish, aborted, hops, done
+        out = {}
+        for cap in (4, 64):  # 4: fewer slots than conductors reached, reported as overflow
+            buf = shard.sparse_buffer(cap)
+            shard.compact_torch(rows_i, rows_f, n, buf, cap)
+            g = shard.gather_sparse(buf, world)
+            mi = torch.zeros_like(rows_i)
+            mf = torch.zeros_like(rows_f)
+            ovf = shard.merge_sparse(g, n, cap, mi, mf)
+            out[cap] = (mi.numpy(), mf.numpy(), bool(ovf))
+        dense_i, dense_f = rows_i.clone(), rows_f.clone()
+        dist.all_reduce(dense_i)
+        dist.all_reduce(dense_f)
+        if rank == 0:
+            np.savez(out_path, mi=out[64][0], mf=out[64][1], ovf64=out[64][2], ovf4=out[4][2],
+                     di=dense_i.numpy(), df=dense_f.numpy())
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sparse_exchange_equals_dense_all_reduce(tmp_path):
+    import torch.multiprocessing as tmp
+
+    out = str(tmp_path / "sparse.npz")
+    tmp.start_processes(_sparse_worker, args=(2, _free_port(), 3000, out), nprocs=2, join=True,
+                        start_method="spawn")
+    r = np.load(out)
+    assert not r["ovf64"] and r["ovf4"]
+    assert np.array_equal(r["mi"], r["di"])
+    np.testing.assert_allclose(r["mf"], r["df"], rtol=1e-14, atol=0)

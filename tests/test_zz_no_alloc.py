@@ -27,6 +27,20 @@ def _fn():
     return f
 
 
+def _device_memory():
+    """(bytes used and reserved by the device's default stream-ordered pool,
+    free device bytes): what an allocating call would change."""
+    import torch
+
+    cu = C.CDLL("libcuda.so.1")
+    pool = C.c_void_p()
+    assert cu.cuDeviceGetDefaultMemPool(C.byref(pool), torch.cuda.current_device()) == 0
+    used, reserved = C.c_uint64(), C.c_uint64()
+    assert cu.cuMemPoolGetAttribute(pool, 7, C.byref(used)) == 0  # CU_MEMPOOL_ATTR_USED_MEM_CURRENT
+    assert cu.cuMemPoolGetAttribute(pool, 5, C.byref(reserved)) == 0  # CU_MEMPOOL_ATTR_RESERVED_MEM_CURRENT
+    return used.value, reserved.value, torch.cuda.mem_get_info()[0]
+
+
 def test_static_walk_trace_matches_allocating_trace_twice():
     import torch
 
@@ -42,9 +56,16 @@ def test_static_walk_trace_matches_allocating_trace_twice():
             b1 = torch.zeros(n, dtype=torch.int32, device="cuda")
             w = torch.zeros(n, dtype=torch.float64, device="cuda")
             torch.cuda.synchronize()
+            before = _device_memory()
             st = fn(L._h, 0, first, n, seed, C.byref(o), end.data_ptr(), hops.data_ptr(), b1.data_ptr(),
                     w.data_ptr(), None)
+            after = _device_memory()
             assert st == 0, frw.lib().frw_last_error().decode()
+            # nothing taken from the stream-ordered pool; and once the first call
+            # has loaded the array with its module, no device memory at all
+            assert after[:2] == before[:2], (call, before, after)
+            if call == 1:
+                assert after[2] == before[2], (before, after)
             got = (end.cpu().numpy(), hops.cpu().numpy(), b1.cpu().numpy(), w.cpu().numpy())
             for g, x in zip(got, want):
                 assert np.array_equal(g, x), f"call {call}"
