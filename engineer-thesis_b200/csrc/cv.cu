@@ -22,7 +22,10 @@
 // 64-row chunks, Adam, and FP64 reductions.
 #include <cuda_bf16.h>
 
+#include <atomic>
+
 #include "cv.cuh"
+#include "cv_feat.cuh"
 #include "query.cuh"
 
 namespace frw {
@@ -30,128 +33,6 @@ namespace cv {
 namespace {
 
 constexpr unsigned kFull = 0xFFFFFFFFu;
-
-// ---------------------------------------------------------------- features
-// d / a0 as d * (1 / a0) (one division per point), clamped to [-16, 16]
-__device__ __forceinline__ float feat(double d, double inv) {
-    double v = __dmul_rn(d, inv);
-    v = fmin(fmax(v, -16.0), 16.0);
-    return (float)v;
-}
-
-// (dx, dy) from p to the nearest point of each edge of rect r: top, right,
-// bottom, left (layout axes, y down).
-__device__ __forceinline__ void edge_feats(double px, double py, double x0, double y0, double x1, double y1,
-                                           double a0, float *f) {
-    const double cx = fmin(fmax(px, x0), x1), cy = fmin(fmax(py, y0), y1);
-    const double dcx = __dsub_rn(cx, px), dcy = __dsub_rn(cy, py);
-    const double inv = __ddiv_rn(1.0, a0);
-    f[0] = feat(dcx, inv);
-    f[1] = feat(__dsub_rn(y0, py), inv);
-    f[2] = feat(__dsub_rn(x1, px), inv);
-    f[3] = feat(dcy, inv);
-    f[4] = f[0];
-    f[5] = feat(__dsub_rn(y1, py), inv);
-    f[6] = feat(__dsub_rn(x0, px), inv);
-    f[7] = f[3];
-}
-
-// Nearest rect other than layer index `exclude` (smallest L-inf gap, then
-// smallest layer index) from the tree; Morton position or -1.
-__device__ int nearest_other_tree(const DevLayout &L, double px, double py, int exclude) {
-    const float pxf = (float)px, pyf = (float)py, slack = L.slack;
-    double best = 1e300;
-    int best_id = 0x7FFFFFFF, best_k = -1;
-    float limf = 3.0e38f;
-    int stk[kStackMax];
-    int sp = 0, nd = 0;
-    for (;;) {
-        const float4 *bp = L.nbox + 4 * nd;
-        const int4 rf = __ldg(L.nref + nd);
-        const int ref[4] = {rf.x, rf.y, rf.z, rf.w};
-        float lb[4];
-#pragma unroll
-        for (int c = 0; c < 4; c++) lb[c] = ref[c] == kRefEmpty ? 3.0e38f : lb_box_f(__ldg(bp + c), pxf, pyf);
-#pragma unroll
-        for (int c = 0; c < 4; c++) {
-            if (ref[c] >= kRefEmpty || lb[c] > limf) continue;
-            const int f0 = leaf_first(ref[c]), m = leaf_count(ref[c]);
-            for (int k = f0; k < f0 + m; k++) {
-                const float4 r = __ldg(L.rects + k);
-                const float gf = fmaxf(fmaxf(r.x - pxf, pxf - r.z), fmaxf(r.y - pyf, pyf - r.w));
-                if (gf > limf) continue;
-                const int id = __ldg(L.ids + k);
-                if (id == exclude) continue;
-                const double g = fmax(fmax((double)r.x - px, px - (double)r.z), fmax((double)r.y - py, py - (double)r.w));
-                if (g < best || (g == best && id < best_id)) {
-                    best = g;
-                    best_id = id;
-                    best_k = k;
-                    limf = (float)best + slack;
-                }
-            }
-        }
-        int next = -1;
-        float nlb = 0.f;
-#pragma unroll
-        for (int c = 0; c < 4; c++) {
-            if (ref[c] < 0 || lb[c] > limf) continue;
-            int push = ref[c];
-            if (next < 0 || lb[c] < nlb) {
-                push = next;
-                next = ref[c];
-                nlb = lb[c];
-            }
-            if (push >= 0 && sp < kStackMax) stk[sp++] = push;
-        }
-        if (next >= 0) {
-            nd = next;
-            continue;
-        }
-        if (sp == 0) break;
-        nd = stk[--sp];
-    }
-    return best_k;
-}
-
-// The same from p's cell list when it settles the answer: every rect within
-// crad of p is listed, so a listed nearest other within crad is the nearest
-// (ties included); otherwise the tree.  Writes the rect, false when none.
-__device__ __forceinline__ bool nearest_other(const DevLayout &L, double px, double py, int exclude, float4 &o) {
-    if (L.cells && px >= L.bx0 && py >= L.by0 && px <= L.bx1 && py <= L.by1) {
-        int ix = (int)__dmul_rn(__dsub_rn(px, L.gx0), L.ginv);
-        int iy = (int)__dmul_rn(__dsub_rn(py, L.gy0), L.ginv);
-        ix = ix < 0 ? 0 : (ix >= L.gnx ? L.gnx - 1 : ix);
-        iy = iy < 0 ? 0 : (iy >= L.gny ? L.gny - 1 : iy);
-        const int64_t cell = (int64_t)iy * L.gnx + ix;
-        const int2 ce = __ldg(L.cells + cell);
-        if (ce.y >= 0) {
-            double best = 1e300;
-            int best_id = 0x7FFFFFFF;
-            float4 bo = make_float4(0.f, 0.f, 0.f, 0.f);
-            for (int k = ce.x; k < ce.x + ce.y; k++) {
-                const int id = __ldg(L.cids + k);
-                if (id == exclude) continue;
-                const float4 r = __ldg(L.crects + k);
-                const double g =
-                    fmax(fmax((double)r.x - px, px - (double)r.z), fmax((double)r.y - py, py - (double)r.w));
-                if (g < best || (g == best && id < best_id)) {
-                    best = g;
-                    best_id = id;
-                    bo = r;
-                }
-            }
-            if (best <= (double)__ldg(L.crad + cell)) {
-                o = bo;
-                return true;
-            }
-        }
-    }
-    const int k = nearest_other_tree(L, px, py, exclude);
-    if (k < 0) return false;
-    o = __ldg(L.rects + k);
-    return true;
-}
 
 __global__ void k_features(DevLayout L, double4 trect, int tid, const double4 *__restrict__ rec, int64_t n,
                            __nv_bfloat16 *__restrict__ xb, float *__restrict__ xf) {
@@ -783,8 +664,32 @@ frw_status launch_features(const DevLayout &L, double4 trect, int tid, const dou
     return FRW_OK;
 }
 
-frw_status launch_forward(const Net &n, const __nv_bfloat16 *x, int64_t rows, float *out, cudaStream_t st) {
+namespace {
+std::atomic<int> g_mlp_kernels{FRW_MLP_TCGEN05};
+
+int device_sms() {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms > 0 ? sms : 1;
+}
+}  // namespace
+
+int mlp_kernels() { return g_mlp_kernels.load(std::memory_order_relaxed); }
+
+frw_status set_mlp_kernels(int which) {
+    if (which != FRW_MLP_TCGEN05 && which != FRW_MLP_MMA_SYNC) {
+        set_error("frw_mlp_set_kernels: FRW_MLP_TCGEN05 or FRW_MLP_MMA_SYNC");
+        return FRW_E_ARG;
+    }
+    g_mlp_kernels.store(which, std::memory_order_relaxed);
+    return FRW_OK;
+}
+
+frw_status launch_forward(const Net &n, const __nv_bfloat16 *x, int64_t rows, float *out, uint32_t *status,
+                          cudaStream_t st) {
     if (rows <= 0) return FRW_OK;
+    if (mlp_kernels() == FRW_MLP_TCGEN05) return launch_forward_tc(n, x, rows, out, status, device_sms(), st);
     const int64_t tiles = (rows + 15) / 16;
     const int blocks = (int)std::min<int64_t>((tiles + 3) / 4, 148 * 8);
     k_forward<<<blocks, 128, 0, st>>>(n.p, n.w1, n.w2, x, rows, out);
@@ -793,8 +698,10 @@ frw_status launch_forward(const Net &n, const __nv_bfloat16 *x, int64_t rows, fl
 }
 
 frw_status launch_train_grad(const Net &n, const __nv_bfloat16 *x, const float *y, const float *wt, int64_t rows,
-                             float inv_wsum, float *grad, double *loss, cudaStream_t st) {
+                             float inv_wsum, float *grad, double *loss, uint32_t *status, cudaStream_t st) {
     if (rows <= 0) return FRW_OK;
+    if (mlp_kernels() == FRW_MLP_TCGEN05)
+        return launch_train_grad_tc(n, x, y, wt, rows, inv_wsum, grad, loss, status, device_sms(), st);
     const int64_t chunks = (rows + kRowsPerBlock - 1) / kRowsPerBlock;
     const int blocks = (int)std::min<int64_t>(chunks, 148 * 2);
     k_train_grad<<<blocks, 128, 0, st>>>(n.p, n.w1, n.w2, n.w2t, x, y, wt, rows, inv_wsum, grad, loss);
@@ -830,19 +737,26 @@ frw_status launch_targets(const int64_t *end, const double4 *rec, int64_t n, int
 
 frw_status launch_quad_mean(const DevLayout &L, double4 trect, int tid, const double4 *gauss, uint32_t Q,
                             const double *pi_exact, const double *wx, const double *wy, double eps, bool exact,
-                            const Net &net, double *sum, float *phi_out, cudaStream_t st) {
+                            const Net &net, double *sum, float *phi_out, uint32_t *status, cudaStream_t st) {
     double4 *sqs;
     int *sides;
     FRW_CK(cudaMallocAsync((void **)&sqs, (size_t)Q * sizeof(double4), st));
     FRW_CK(cudaMallocAsync((void **)&sides, (size_t)Q * sizeof(int), st));
     k_quad_starts<<<(Q + 127) / 128, 128, 0, st>>>(L, gauss, Q, sqs, sides);
     const int64_t n = (int64_t)Q * FRW_NSAMPLE;
-    const int blocks = (int)std::min<int64_t>((n + 127) / 128, 148 * 8);
-    k_quad_mean<<<blocks, 128, 0, st>>>(L, trect, tid, gauss, sqs, sides, Q, pi_exact, wx, wy, eps, exact, net.p,
-                                        net.w1, net.w2, sum, phi_out);
-    cudaError_t e = cudaGetLastError();
+    frw_status rc = FRW_OK;
+    if (mlp_kernels() == FRW_MLP_TCGEN05) {
+        rc = launch_quad_mean_tc(L, trect, tid, gauss, sqs, sides, Q, pi_exact, wx, wy, eps, exact, net, sum, phi_out,
+                                 status, device_sms(), st);
+    } else {
+        const int blocks = (int)std::min<int64_t>((n + 127) / 128, 148 * 8);
+        k_quad_mean<<<blocks, 128, 0, st>>>(L, trect, tid, gauss, sqs, sides, Q, pi_exact, wx, wy, eps, exact,
+                                            net.p, net.w1, net.w2, sum, phi_out);
+    }
+    cudaError_t e = rc ? cudaSuccess : cudaGetLastError();
     cudaFreeAsync(sqs, st);
     cudaFreeAsync(sides, st);
+    if (rc) return rc;
     FRW_CK(e);
     return FRW_OK;
 }

@@ -38,16 +38,33 @@ frw_status net_refresh_bf16(const Net &n, cudaStream_t st);
 // the nearest other conductor, divided by a0 and clamped to [-16, 16].
 frw_status launch_features(const DevLayout &L, double4 target_rect, int target_id, const double4 *rec,
                            int64_t n, __nv_bfloat16 *xb, float *xf, cudaStream_t st);
-frw_status launch_forward(const Net &n, const __nv_bfloat16 *x, int64_t rows, float *out, cudaStream_t st);
+// The MLP kernels: tcgen05 / TMEM tiles of 128 rows (cv_umma.cu, the
+// default) or mma.sync tiles of 16 rows (cv.cu); frw_mlp_set_kernels picks.
+// status: device word, kStDeviceWait set when a tcgen05 completion wait
+// passed its bound.
+int mlp_kernels();
+frw_status set_mlp_kernels(int which);
+frw_status launch_forward(const Net &n, const __nv_bfloat16 *x, int64_t rows, float *out, uint32_t *status,
+                          cudaStream_t st);
 // grad += d/dparams sum_r wt_r (f(x_r) - y_r)^2 * inv_wsum ; loss += same sum
 frw_status launch_train_grad(const Net &n, const __nv_bfloat16 *x, const float *y, const float *wt, int64_t rows,
-                             float inv_wsum, float *grad, double *loss, cudaStream_t st);
+                             float inv_wsum, float *grad, double *loss, uint32_t *status, cudaStream_t st);
+frw_status launch_forward_tc(const Net &n, const __nv_bfloat16 *x, int64_t rows, float *out, uint32_t *status,
+                             int sms, cudaStream_t st);
+frw_status launch_train_grad_tc(const Net &n, const __nv_bfloat16 *x, const float *y, const float *wt, int64_t rows,
+                                float inv_wsum, float *grad, double *loss, uint32_t *status, int sms,
+                                cudaStream_t st);
 frw_status launch_adam(const Net &n, float *grad, float *m, float *v, int *step, float lr, cudaStream_t st);
 // exact mean E[f] over every (grid start, first-hop bin) pair, accumulated into *sum
 frw_status launch_quad_mean(const DevLayout &L, double4 target_rect, int target_id, const double4 *gauss, uint32_t Q,
                             const double *pi_exact, const double *wx, const double *wy, double eps,
                             bool exact_perimeter, const Net &net, double *sum,
-                            float *phi_out /*nullable: Q*200 phi values, item q*200+i*/, cudaStream_t st);
+                            float *phi_out /*nullable: Q*200 phi values, item q*200+i*/, uint32_t *status,
+                            cudaStream_t st);
+frw_status launch_quad_mean_tc(const DevLayout &L, double4 trect, int tid, const double4 *gauss, const double4 *sqs,
+                               const int *sides, uint32_t Q, const double *pi_exact, const double *wx,
+                               const double *wy, double eps, bool exact, const Net &net, double *sum, float *phi_out,
+                               uint32_t *status, int sms, cudaStream_t st);
 // per walk record (end, weight factor c, q*200+i1 or -1): the sums of
 // z = c (1{end==target} - phi), z^2, w = c 1{end==target}, w^2 with phi looked
 // up in the quadrature's table

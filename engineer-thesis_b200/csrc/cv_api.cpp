@@ -170,6 +170,7 @@ frw_status frw_cv_train(const frw_layout *layout, int64_t target, const frw_opts
         float *d_y, *d_wt, *d_grad, *d_m, *d_v;
         double *d_wsum, *d_loss;
         int *d_step;
+        uint32_t *d_tstatus;
         const int steps_per_epoch = (int)((N + co.batch - 1) / co.batch);
         const int steps = steps_per_epoch * co.epochs;
         cudaError_t e = cudaSuccess;
@@ -184,6 +185,7 @@ frw_status frw_cv_train(const frw_layout *layout, int64_t target, const frw_opts
         if (e == cudaSuccess) e = B.get(&d_wsum, 8);
         if (e == cudaSuccess) e = B.get(&d_loss, (size_t)steps * 8);
         if (e == cudaSuccess) e = B.get(&d_step, 4);
+        if (e == cudaSuccess) e = B.get(&d_tstatus, 4);
         if (e != cudaSuccess) return fail(cuda_fail(e, "frw_cv_train: allocation"));
         cudaEventRecord(e0, st);
         // training walks start anywhere on the surface: a stratified start
@@ -217,6 +219,7 @@ frw_status frw_cv_train(const frw_layout *layout, int64_t target, const frw_opts
         cudaMemsetAsync(d_v, 0, cv::kParams * 4, st);
         cudaMemsetAsync(d_loss, 0, (size_t)steps * 8, st);
         cudaMemsetAsync(d_step, 0, 4, st);
+        cudaMemsetAsync(d_tstatus, 0, 4, st);
         // the training loop: a few hundred launches, enqueued directly (the
         // host stays ahead of the device; instantiating a graph of them would
         // cost more host time than it saves)
@@ -226,13 +229,16 @@ frw_status frw_cv_train(const frw_layout *layout, int64_t target, const frw_opts
             const int64_t rows = std::min<int64_t>(co.batch, N - start);
             const float inv = (float)(scale / (double)rows);
             rc = cv::launch_train_grad(M->net, d_x + 16 * start, d_y + start, d_wt + start, rows, inv, d_grad,
-                                       d_loss + s, st);
+                                       d_loss + s, d_tstatus, st);
             if (!rc) rc = cv::launch_adam(M->net, d_grad, d_m, d_v, d_step, co.lr, st);
         }
         if (rc) return fail(rc);
         cudaEventRecord(e1, st);
         std::vector<double> losses(steps);
         rc = read_back(losses.data(), d_loss, (size_t)steps * 8, st, "frw_cv_train: training");
+        uint32_t ts = 0;
+        if (!rc) rc = read_back(&ts, d_tstatus, 4, st, "frw_cv_train: training status");
+        if (!rc) rc = status_word_error(ts);
         if (rc) return fail(rc);
         double l = 0;
         for (int s = steps - steps_per_epoch; s < steps; s++) l += losses[s];
@@ -270,7 +276,7 @@ frw_status frw_cv_train(const frw_layout *layout, int64_t target, const frw_opts
         if (!rc)
             rc = cv::launch_quad_mean(v.dl, trect, (int)target, d_gauss, Q, d_pi, tables + FRW_NSAMPLE + 1,
                                       tables + 2 * FRW_NSAMPLE + 1, walk_opts->permittivity,
-                                      walk_opts->exact_perimeter != 0, M->net, d_mu, M->phi, st);
+                                      walk_opts->exact_perimeter != 0, M->net, d_mu, M->phi, d_status, st);
         if (rc) return fail(rc);
         uint32_t hs = 0;
         e = cudaEventRecord(e2, st);
@@ -394,9 +400,12 @@ frw_status frw_mlp_forward(const float *params, const float *x, int64_t n, float
     Buf B(st);
     float *d_xf, *d_out;
     __nv_bfloat16 *d_x;
+    uint32_t *d_status;
     FRW_CK(B.get(&d_xf, n * 64));
     FRW_CK(B.get(&d_x, n * 32));
     FRW_CK(B.get(&d_out, n * 4));
+    FRW_CK(B.get(&d_status, 4));
+    FRW_CK(cudaMemsetAsync(d_status, 0, 4, st));
     cv::Net net;
     rc = cv::net_alloc(&net, st);
     if (!rc) rc = cv::net_upload(&net, params, st);
@@ -405,7 +414,10 @@ frw_status frw_mlp_forward(const float *params, const float *x, int64_t n, float
         std::vector<__nv_bfloat16> hb((size_t)n * 16);
         for (int64_t i = 0; i < n * 16; i++) hb[i] = __float2bfloat16_rn(x[i]);
         FRW_CK(cudaMemcpyAsync(d_x, hb.data(), n * 32, cudaMemcpyHostToDevice, st));
-        rc = cv::launch_forward(net, d_x, n, d_out, st);
+        rc = cv::launch_forward(net, d_x, n, d_out, d_status, st);
+        uint32_t hs = 0;
+        if (!rc) rc = read_back(&hs, d_status, 4, st, "frw_mlp_forward");
+        if (!rc) rc = status_word_error(hs);
         if (!rc) rc = read_back(out, d_out, n * 4, st, "frw_mlp_forward");
     }
     cv::net_free(&net, st);
@@ -428,6 +440,9 @@ frw_status frw_mlp_grad(const float *params, const float *x, const float *y, con
     __nv_bfloat16 *d_x;
     float *d_y, *d_wt, *d_g;
     double *d_l;
+    uint32_t *d_status;
+    FRW_CK(B.get(&d_status, 4));
+    FRW_CK(cudaMemsetAsync(d_status, 0, 4, st));
     FRW_CK(B.get(&d_x, n * 32));
     FRW_CK(B.get(&d_y, n * 4));
     FRW_CK(B.get(&d_wt, n * 4));
@@ -444,13 +459,20 @@ frw_status frw_mlp_grad(const float *params, const float *x, const float *y, con
         FRW_CK(cudaMemcpyAsync(d_wt, wt, n * 4, cudaMemcpyHostToDevice, st));
         FRW_CK(cudaMemsetAsync(d_g, 0, cv::kParams * 4, st));
         FRW_CK(cudaMemsetAsync(d_l, 0, 8, st));
-        rc = cv::launch_train_grad(net, d_x, d_y, d_wt, n, (float)inv_wsum, d_g, d_l, st);
+        rc = cv::launch_train_grad(net, d_x, d_y, d_wt, n, (float)inv_wsum, d_g, d_l, d_status, st);
+        uint32_t hs = 0;
+        if (!rc) rc = read_back(&hs, d_status, 4, st, "frw_mlp_grad");
+        if (!rc) rc = status_word_error(hs);
         if (!rc) rc = read_back(grad, d_g, cv::kParams * 4, st, "frw_mlp_grad");
         if (!rc && loss) rc = read_back(loss, d_l, 8, st, "frw_mlp_grad");
     }
     cv::net_free(&net, st);
     return rc;
 }
+
+frw_status frw_mlp_set_kernels(int which) { return cv::set_mlp_kernels(which); }
+
+int frw_mlp_get_kernels(void) { return cv::mlp_kernels(); }
 
 frw_status frw_cv_features(const frw_layout *layout, int64_t target, const double *rec4, int64_t n, float *out) {
     LayoutView v;

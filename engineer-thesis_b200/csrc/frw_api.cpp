@@ -137,6 +137,7 @@ frw_status status_error(uint32_t h) {
         if (h & kStStackOverflow) m += " traversal stack overflow;";
         if (h & kStReplayCap) m += " bisection replay iteration bound exceeded;";
         if (h & kStBadInput) m += " invalid input;";
+        if (h & kStDeviceWait) m += " a device-side wait passed its bound;";
         set_error(m);
         return FRW_E_KERNEL;
     }
@@ -350,6 +351,8 @@ frw_status run_walks(const frw_layout *lay, int64_t target, uint64_t first_walk,
 }  // namespace
 
 void set_error(const std::string &msg) { g_err = msg; }
+
+frw_status status_word_error(uint32_t status) { return status_error(status); }
 
 double wait_limit_ms() {
     return t_wait_ms >= 0 ? t_wait_ms : (double)g_wait_default_us.load(std::memory_order_relaxed) * 1e-3;

@@ -59,6 +59,7 @@ enum : uint32_t {
     kStStackOverflow = 2u,  // traversal stack overflow
     kStReplayCap = 4u,      // bisection replay exceeded its iteration bound
     kStBadInput = 8u,       // a kernel met an input outside its contract
+    kStDeviceWait = 16u,    // a device-side wait (mbarrier) passed its bound
 };
 
 // ---- walk jobs ----------------------------------------------------------------
@@ -113,6 +114,9 @@ struct WalkParams {
 // ---- host helpers ----------------------------------------------------------
 void set_error(const std::string &msg);
 frw_status cuda_fail(cudaError_t e, const char *what);
+
+// FRW_E_KERNEL with a message naming the bits of a nonzero kernel status word.
+frw_status status_word_error(uint32_t status);
 
 // Bounded host waits.  The limit in force on the calling thread (ms; <= 0:
 // none) is the process-wide default (frw_set_wait_limit) unless a WaitScope

@@ -233,6 +233,8 @@ _SIGS = {
     "frw_layout_from_file": ([C.c_char_p, C.c_int, C.c_int, C.POINTER(_VP)], C.c_int),
     "frw_rows_compact": ([_VP, _VP, _VP, _VP, C.c_int64, _VP, _VP, _VP, _VP, _VP, _VP], C.c_int),
     "frw_set_wait_limit": ([C.c_double], C.c_int),
+    "frw_mlp_set_kernels": ([C.c_int], C.c_int),
+    "frw_mlp_get_kernels": ([], C.c_int),
     "frw_get_wait_limit": ([], C.c_double),
     "frw_parse_layout": ([C.c_char_p, C.c_int, _D, C.c_int64, _I64, _D, _I32], C.c_int),
     "frw_layout_create": ([_F, C.c_int64, _D, C.c_int, _VP, C.POINTER(_VP)], C.c_int),
@@ -325,6 +327,18 @@ def version() -> str:
 
 def device_check(device: int = 0) -> None:
     _check(lib().frw_device_check(device))
+
+
+MLP_TCGEN05, MLP_MMA_SYNC = 0, 1
+
+
+def set_mlp_kernels(which: int) -> None:
+    """MLP_TCGEN05 (128-row tcgen05 / TMEM tiles, the default) or MLP_MMA_SYNC."""
+    _check(lib().frw_mlp_set_kernels(int(which)))
+
+
+def mlp_kernels() -> int:
+    return int(lib().frw_mlp_get_kernels())
 
 
 def set_wait_limit(ms: float) -> None:

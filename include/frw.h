@@ -381,6 +381,16 @@ frw_status frw_cv_walk(const frw_cv *cv, uint64_t walks, uint64_t seed, frw_cv_r
 frw_status frw_cv_destroy(frw_cv *cv);
 #define FRW_CV_PARAMS 5313 /* W1[64][16] b1[64] W2[64][64] b2[64] w3[64] b3 */
 frw_status frw_cv_params(const frw_cv *cv, float *out);
+/* Which tensor-core kernels run the MLP (process-wide): FRW_MLP_TCGEN05, the
+ * default -- 128-row tiles on the fifth-generation tensor cores (tcgen05.mma,
+ * accumulators in tensor memory), every weight and bias gradient a tensor-core
+ * product accumulated over the tiles -- or FRW_MLP_MMA_SYNC, 16-row warp
+ * tiles of mma.sync.  Both compute the same function (BF16 operands, FP32
+ * accumulation) up to the order of the FP32 sums. */
+#define FRW_MLP_TCGEN05 0
+#define FRW_MLP_MMA_SYNC 1
+frw_status frw_mlp_set_kernels(int which);
+int frw_mlp_get_kernels(void);
 /* The MLP and feature kernels on host arrays (FP32 in, BF16 operands on the
  * device): forward outputs, and the gradient of
  * sum_r wt_r (f(x_r) - y_r)^2 * inv_wsum with the summed loss. */

@@ -39,7 +39,18 @@ def _random_params(seed):
     return p
 
 
-def test_mlp_forward_matches_fp64():
+KERNELS = [pytest.param(frw.MLP_TCGEN05, id="tcgen05"), pytest.param(frw.MLP_MMA_SYNC, id="mma_sync")]
+
+
+@pytest.fixture
+def mlp_kernels(request):
+    frw.set_mlp_kernels(request.param)
+    yield request.param
+    frw.set_mlp_kernels(frw.MLP_TCGEN05)
+
+
+@pytest.mark.parametrize("mlp_kernels", KERNELS, indirect=True)
+def test_mlp_forward_matches_fp64(mlp_kernels):
     p = _random_params(1)
     x = np.random.default_rng(3).uniform(-3, 3, (5000, 16)).astype(np.float32)
     got = frw.mlp_forward(p, x)
@@ -49,7 +60,8 @@ def test_mlp_forward_matches_fp64():
     assert np.corrcoef(got, want)[0, 1] > 0.9999
 
 
-def test_mlp_gradients_match_fp64():
+@pytest.mark.parametrize("mlp_kernels", KERNELS, indirect=True)
+def test_mlp_gradients_match_fp64(mlp_kernels):
     p = _random_params(4)
     rng = np.random.default_rng(5)
     n = 4096 + 37  # a ragged last chunk
@@ -69,6 +81,30 @@ def test_mlp_gradients_match_fp64():
         ga, gb = g[a:b], g_r[a:b]
         assert np.linalg.norm(ga - gb) <= 5e-2 * np.linalg.norm(gb) + 1e-7
     assert g[M.O_B3] == pytest.approx(g_r[M.O_B3], rel=1e-2)
+
+
+def test_tcgen05_and_mma_sync_kernels_agree():
+    # same BF16 operands and FP32 accumulation: only the order of the FP32
+    # sums (and so an occasional BF16 rounding of an activation) differs
+    p = _random_params(7)
+    rng = np.random.default_rng(8)
+    n = 3 * 128 + 5
+    x = rng.uniform(-3, 3, (n, 16)).astype(np.float32)
+    y = (rng.random(n) < 0.4).astype(np.float32)
+    wt = rng.exponential(1.0, n).astype(np.float32)
+    inv = 1.0 / float(wt.sum())
+    out = {}
+    try:
+        for k in (frw.MLP_TCGEN05, frw.MLP_MMA_SYNC):
+            frw.set_mlp_kernels(k)
+            assert frw.mlp_kernels() == k
+            out[k] = (frw.mlp_forward(p, x), *frw.mlp_grad(p, x, y, wt, inv))
+    finally:
+        frw.set_mlp_kernels(frw.MLP_TCGEN05)
+    (f_a, l_a, g_a), (f_b, l_b, g_b) = out[frw.MLP_TCGEN05], out[frw.MLP_MMA_SYNC]
+    assert np.abs(f_a - f_b).max() <= 1e-2 * (1 + np.abs(f_b).max())
+    assert l_a == pytest.approx(l_b, rel=1e-3)
+    assert np.linalg.norm(g_a - g_b) <= 2e-2 * np.linalg.norm(g_b)
 
 
 def test_cv_unbiased_and_reduces_variance():
