@@ -788,7 +788,6 @@ def opts3(gauss_offset=1.0, shell=0.0, hop_cap=100000, permittivity=PERMITTIVITY
     o.blocks_per_sm = blocks_per_sm
     o.refill_min = refill_min
     o.start_strata = start_strata
-    o.timeout_ms = timeout_ms
     return o
 
 

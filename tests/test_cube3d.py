@@ -2,6 +2,7 @@
 and the library's host table, both pinned bit-for-bit against the
 reference's precompute_unit_cube_green, green/green.cpp:392-431), the
 physics the table must satisfy, and the 3-D oracle's own consistency."""
+import ctypes as C
 import hashlib
 
 import numpy as np
@@ -191,3 +192,9 @@ def test_cube_api_argument_errors_without_device():
     with pytest.raises(frw.FrwError) as e:
         frw.Layout3.from_file("/nonexistent/layout", [0.0], [1.0])
     assert e.value.status == frw.E_IO
+
+
+def test_opts3_builds_without_a_device():
+    # frw3_opts_default is host-only; the Python mirror must fill every field
+    o = frw.opts3(gauss_offset=2.0, nsample=8, start_strata=4)
+    assert o.struct_size == C.sizeof(frw.Opts3) and o.gauss_offset == 2.0 and o.nsample == 8
