@@ -689,8 +689,10 @@ def main():
         frw._check(frw.lib().frw_layout_create(ctypes.cast(ptr, frw._F), W["rects"], None, local,
                                                ctypes.c_void_p(stream.cuda_stream), ctypes.byref(h)))
         Le = frw.Layout(h, W["rects"])
-        r = Le.walk(W["target"], W["walks"], seed, o, stream=stream.cuda_stream)
+        # room for 65,536 result rows (a step reaches a few hundred conductors; checked below)
+        r = Le.walk(W["target"], W["walks"], seed, o, capacity=1 << 16, stream=stream.cuda_stream)
         Le.close()
+        assert r.extra["n_entries"] == len(r.conductor), "result rows truncated"
         return r
 
     e2e_ms, nrows = float("nan"), 0

@@ -16,7 +16,9 @@
 #include <atomic>
 #include <chrono>
 #include <map>
+#include <memory>
 #include <mutex>
+#include <new>
 #include <thread>
 #include <string>
 #include <vector>
@@ -27,7 +29,7 @@
 struct frw_layout {
     int device = 0;
     int64_t n = 0;
-    std::vector<double> rects;  // layer order, as given
+    std::unique_ptr<double[]> rects;  // [4 n] layer order, as given
     double bounds[4] = {0, 0, 0, 0};
     frw::TreeBuffers T;
     frw::CellBuffers cells;
@@ -242,7 +244,7 @@ frw_status run_walks(const frw_layout *lay, int64_t target, uint64_t first_walk,
     double4 *d_tgt = &h->tgt, *d_gauss = &h->gauss;
     uint32_t *d_status = &h->status;
     unsigned long long *d_counter = &h->counter, *d_stats = h->stats;
-    const double *r = lay->rects.data() + 4 * target;
+    const double *r = lay->rects.get() + 4 * target;
     const double tg[4] = {r[0], r[1], r[2], r[3]};
     FRW_CK(cudaMemsetAsync(blk, 0, offsetof(Hdr, tgt), st));
     if (rows) FRW_CK(cudaMemsetAsync(d_acc_n, 0, R * 24, st));
@@ -387,6 +389,84 @@ frw_status read_back(void *host, const void *dev, size_t bytes, cudaStream_t st,
     return e == cudaSuccess ? FRW_OK : cuda_fail(e, what);
 }
 
+// Checks the caller's rects (finite, |c| < 2^24, not inverted), converts
+// them to the layout's FP64 host copy and settles the bounds (the given ones,
+// which must contain every rect, or the reference rule from the bounding
+// box), in one pass split over host threads for large layouts.  Errors name
+// the first offending rect.
+frw_status ingest_rects(const float *in, int64_t n, const double *given, double *out, double bounds[4]) {
+    struct Part {
+        int64_t bad = INT64_MAX;
+        int why = 0;  // 1 coordinate, 2 inverted, 3 outside the given bounds
+        double lx = INFINITY, ty = INFINITY, rx = -INFINITY, by = -INFINITY;
+    };
+    if (given && (!(given[0] <= given[2] && given[1] <= given[3]) || !std::isfinite(given[0]) ||
+                  !std::isfinite(given[1]) || !std::isfinite(given[2]) || !std::isfinite(given[3]))) {
+        set_error("bounds invalid");
+        return FRW_E_ARG;
+    }
+    const int64_t kChunk = 1 << 17;
+    const int nt = (int)std::min<int64_t>((n + kChunk - 1) / kChunk,
+                                          std::max<unsigned>(1, std::min(8u, std::thread::hardware_concurrency())));
+    std::vector<Part> parts(nt);
+    auto work = [&](int t) {
+        Part &P = parts[t];
+        const int64_t a = n * t / nt, b = n * (t + 1) / nt;
+        for (int64_t i = a; i < b; i++) {
+            const float *q = in + 4 * i;
+            double *o = out + 4 * i;
+            bool ok = true;
+            for (int k = 0; k < 4; k++) {
+                ok = ok && std::isfinite(q[k]) && fabsf(q[k]) < 16777216.0f;
+                o[k] = q[k];
+            }
+            int why = !ok ? 1 : (!(q[0] <= q[2] && q[1] <= q[3]) ? 2 : 0);
+            if (!why && given && !(o[1] >= given[1] && o[0] >= given[0] && o[3] <= given[3] && o[2] <= given[2]))
+                why = 3;
+            if (why) {
+                P.bad = i;
+                P.why = why;
+                return;
+            }
+            P.lx = std::min(P.lx, o[0]);
+            P.ty = std::min(P.ty, o[1]);
+            P.rx = std::max(P.rx, o[2]);
+            P.by = std::max(P.by, o[3]);
+        }
+    };
+    if (nt == 1) work(0);
+    else {
+        std::vector<std::thread> th;
+        for (int t = 1; t < nt; t++) th.emplace_back(work, t);
+        work(0);
+        for (auto &x : th) x.join();
+    }
+    Part all;
+    for (const Part &P : parts) {
+        if (P.bad < all.bad) {
+            all.bad = P.bad;
+            all.why = P.why;
+        }
+        all.lx = std::min(all.lx, P.lx);
+        all.ty = std::min(all.ty, P.ty);
+        all.rx = std::max(all.rx, P.rx);
+        all.by = std::max(all.by, P.by);
+    }
+    if (all.why) {
+        const std::string r = "rect " + std::to_string(all.bad);
+        set_error(all.why == 1 ? r + ": coordinate not finite or |c| >= 2^24"
+                               : all.why == 2 ? r + ": inverted (need x0 <= x1 and y0 <= y1)"
+                                              : r + " lies outside the bounds");
+        return FRW_E_ARG;
+    }
+    if (given) {
+        memcpy(bounds, given, 4 * sizeof(double));
+    } else {
+        bounds_from_extent(all.lx, all.ty, all.rx, all.by, bounds);
+    }
+    return FRW_OK;
+}
+
 frw_status layout_view(const frw_layout *L, LayoutView *out) {
     if (!L) {
         set_error("null layout");
@@ -395,7 +475,7 @@ frw_status layout_view(const frw_layout *L, LayoutView *out) {
     out->dl = L->dl;
     out->device = L->device;
     out->n = L->n;
-    out->rects = L->rects.data();
+    out->rects = L->rects.get();
     return FRW_OK;
 }
 
@@ -485,42 +565,21 @@ frw_status frw_layout_create(const float *rects, int64_t n, const double *bounds
     DeviceCtx *ctx;
     frw_status rc = device_ctx(device, &ctx);
     if (rc) return rc;
-    std::vector<double> h((size_t)n * 4);
-    for (int64_t i = 0; i < n; i++) {
-        const float *q = rects + 4 * i;
-        for (int k = 0; k < 4; k++) {
-            if (!std::isfinite(q[k]) || fabsf(q[k]) >= 16777216.0f) {
-                set_error("rect " + std::to_string(i) + ": coordinate not finite or |c| >= 2^24");
-                return FRW_E_ARG;
-            }
-            h[4 * i + k] = q[k];
-        }
-        if (!(q[0] <= q[2] && q[1] <= q[3])) {
-            set_error("rect " + std::to_string(i) + ": inverted (need x0 <= x1 and y0 <= y1)");
-            return FRW_E_ARG;
-        }
-    }
     frw_layout *L = new frw_layout();
     L->device = device;
     L->n = n;
-    L->rects.swap(h);
-    if (bounds) memcpy(L->bounds, bounds, sizeof(L->bounds));
-    else reference_bounds(L->rects.data(), n, L->bounds);
-    const double *b = L->bounds;
-    if (!(b[0] <= b[2] && b[1] <= b[3]) || !std::isfinite(b[0]) || !std::isfinite(b[1]) ||
-        !std::isfinite(b[2]) || !std::isfinite(b[3])) {
-        set_error("bounds invalid");
+    L->rects.reset(new (std::nothrow) double[(size_t)n * 4]);
+    if (!L->rects) {
         delete L;
-        return FRW_E_ARG;
+        set_error("frw_layout_create: host memory for the rect copy");
+        return FRW_E_OOM;
     }
-    for (int64_t i = 0; i < n; i++) {
-        const double *q = L->rects.data() + 4 * i;
-        if (!(q[1] >= b[1] && q[0] >= b[0] && q[3] <= b[3] && q[2] <= b[2])) {
-            set_error("rect " + std::to_string(i) + " lies outside the bounds");
-            delete L;
-            return FRW_E_ARG;
-        }
+    rc = ingest_rects(rects, n, bounds, L->rects.get(), L->bounds);
+    if (rc) {
+        delete L;
+        return rc;
     }
+    const double *b = L->bounds;
     DeviceGuard g(device);
     cudaStream_t st = (cudaStream_t)stream;
     float4 *d_in = nullptr;
@@ -712,7 +771,7 @@ frw_status frw_layout_rects(const frw_layout *L, double *out) {
         set_error("null argument");
         return FRW_E_ARG;
     }
-    memcpy(out, L->rects.data(), L->rects.size() * sizeof(double));
+    memcpy(out, L->rects.get(), (size_t)L->n * 4 * sizeof(double));
     return FRW_OK;
 }
 
@@ -819,7 +878,7 @@ frw_status frw_gauss_surface(const frw_layout *L, int64_t target, const frw_opts
     FRW_CK(S.get(&d_o, 32));
     FRW_CK(S.get(&d_status, 4));
     FRW_CK(cudaMemsetAsync(d_status, 0, 4, st));
-    FRW_CK(cudaMemcpyAsync(d_t, L->rects.data() + 4 * target, 32, cudaMemcpyHostToDevice, st));
+    FRW_CK(cudaMemcpyAsync(d_t, L->rects.get() + 4 * target, 32, cudaMemcpyHostToDevice, st));
     rc = launch_gauss(L->dl, d_t, 1, o.gauss_mode, o.gauss_param, d_o, d_status, st);
     if (rc) return rc;
     rc = check_status(d_status, st);
@@ -900,7 +959,7 @@ frw_status frw_walk_device(const frw_layout *L, int64_t target, uint64_t walks, 
     unsigned long long *d_counter = reinterpret_cast<unsigned long long *>(blk);
     double4 *d_tgt = reinterpret_cast<double4 *>(blk + 32);
     double4 *d_gauss = reinterpret_cast<double4 *>(blk + 64);
-    const double *r = L->rects.data() + 4 * target;
+    const double *r = L->rects.get() + 4 * target;
     const double tg[4] = {r[0], r[1], r[2], r[3]};
     FRW_CK(cudaMemsetAsync(d_counter, 0, 8, st));
     FRW_CK(cudaMemcpyAsync(d_tgt, tg, sizeof(tg), cudaMemcpyHostToDevice, st));
@@ -1031,7 +1090,7 @@ frw_status frw_avg_path_len(const char *path, int64_t iter_num, int64_t rect_id,
                     fprintf(f, "Ile scie\xc5\xbc" "ek wysz\xc5\x82o poza granice warstwy: %g%%\n",
                             (float)r.escaped / (float)iter_num * 100);
                 for (int64_t k = 0; k < std::min(r.n_entries, r.capacity); k++) {
-                    const double *q = L->rects.data() + 4 * cond[k];
+                    const double *q = L->rects.get() + 4 * cond[k];
                     fprintf(f, "%g %g %g %g: %g%%\n", q[0], q[1], q[2], q[3],
                             ((float)hits[k] / (float)iter_num) * 100);
                 }

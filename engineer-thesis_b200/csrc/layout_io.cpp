@@ -83,6 +83,13 @@ void reference_bounds(const double *r, int64_t n, double out[4]) {
         if (q[2] > rx) rx = q[2];
         if (q[3] > by) by = q[3];
     }
+    bounds_from_extent(lx, ty, rx, by, out);
+}
+
+// The margin rule of Parser::getLayerSize (CPU/Parser.cpp:79-84): the
+// bounding box grown on every side by int(0.01 * width) -- the width's
+// margin on the y axis too, as the reference does.
+void bounds_from_extent(double lx, double ty, double rx, double by, double out[4]) {
     const int add_w = (int)((rx - lx) * 0.01);
     out[0] = lx - add_w;
     out[1] = ty - add_w;

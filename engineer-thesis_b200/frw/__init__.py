@@ -553,7 +553,8 @@ class Layout:
         _check(lib().frw_walk(self._h, target, walks, seed, C.byref(o) if o else None, C.byref(r), stream or None))
         m = min(r.n_entries, cap)
         return WalkResult(r.walks, r.escaped, r.aborted, r.hops_total, np.array(r.gauss[:]), r.fraction_other,
-                          r.kernel_ms, cond[:m], hits[:m], c[:m], se[:m], s1[:m], s2[:m])
+                          r.kernel_ms, cond[:m], hits[:m], c[:m], se[:m], s1[:m], s2[:m],
+                          extra={"n_entries": int(r.n_entries)})
 
     def walk_device(self, target: int, walks: int, seed: int, o: Opts | None, hits, sum_w, sum_w2, stats, status,
                     stream: int = 0):
