@@ -223,14 +223,16 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
     const uint64_t seed = P.seed_dev ? *P.seed_dev : P.seed;
     const uint64_t kChunk = P.chunk ? (uint64_t)P.chunk : kChunkDefault;
 
-    bool active = false, exhausted = false;
+    bool active = false, exhausted = false, starting = false;
     int job = 0;
     uint64_t pw = 0;
-    uint32_t hop = 0, stream = 0;
-    uint4 rnd = make_uint4(0, 0, 0, 0);  // uniforms of hops (hop & ~3) .. +3
+    uint32_t hop = 0, stream = 0;  // hop: the Philox word of the lane's next point
+    uint4 rnd = make_uint4(0, 0, 0, 0);  // uniforms of words (hop & ~3) .. +3
     int32_t hops = 0, bin1 = -1;
     int side = 0;
-    double px = 0, py = 0, a0 = 0, perim = 0;
+    double a0 = 0, perim = 0;
+    // The rect the lane's next point is mapped on: the Gaussian surface of a
+    // walk about to start, else the last square of its walk.
     double sq[4] = {0, 0, 0, 0};
     uint32_t st = 0;
     // Walks of this lane that end on its job's target (most walks: 92% on the
@@ -293,30 +295,17 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
                     }
                     const WalkJob &J = job_of<kMulti>(P, job);
                     const double4 g4 = P.gauss[job];
-                    const double G[4] = {g4.x, g4.y, g4.z, g4.w};
-                    perim = __dadd_rn(__dmul_rn(2.0, __dsub_rn(G[2], G[0])), __dmul_rn(2.0, __dsub_rn(G[3], G[1])));
+                    sq[0] = g4.x;
+                    sq[1] = g4.y;
+                    sq[2] = g4.z;
+                    sq[3] = g4.w;
                     pw = J.first_walk + (gw - J.walk_begin);
                     stream = J.stream_id;
                     hop = 0;
                     hops = 0;
                     bin1 = -1;
                     a0 = 0.0;
-                    rnd = draw_block(seed, stream, pw, 0);
-                    double u = word_u(rnd, 0);
-                    if (P.start_strata) {  // stratum pw mod S of the start distribution
-                        const double s = (double)(uint32_t)(pw % P.start_strata);
-                        u = __ddiv_rn(__dadd_rn(s, u), (double)P.start_strata);
-                    }
-                    if (P.start_grid) {  // midpoint of arc floor(u*Q) of Q equal arcs
-                        const uint32_t q = (uint32_t)__dmul_rn(u, (double)P.start_grid);
-                        u = __ddiv_rn(__dadd_rn((double)q, 0.5), (double)P.start_grid);
-                        if (P.rec_q) bin1 = -2 - (int)q;  // the arc rides in bin1 until the first hop
-                    }
-                    if (uniform_start) {
-                        side = perimeter_point(G, u, px, py);
-                    } else {
-                        point_from_index(G, bin_of(s_intg, s_guide, u), exact, px, py);
-                    }
+                    starting = true;
                     active = true;
                 }
             }
@@ -338,7 +327,42 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
             continue;
         }
 
-        // ---- one hop of every active walk ----
+        // ---- the point of every active walk: its start point on the Gaussian
+        // surface (word 0), or the next hop's point on its last square (word
+        // `hop`); starts and hops share the Philox draw, the bin search and the
+        // perimeter mapping, so a warp runs each once per iteration ----
+        double px = 0, py = 0;
+        if (active) {
+            if ((hop & 3) == 0) rnd = draw_block(seed, stream, pw, hop);
+            double u = word_u(rnd, hop);
+            if (starting) {
+                perim = __dadd_rn(__dmul_rn(2.0, __dsub_rn(sq[2], sq[0])), __dmul_rn(2.0, __dsub_rn(sq[3], sq[1])));
+                if (P.start_strata) {  // stratum pw mod S of the start distribution
+                    const double s = (double)(uint32_t)(pw % P.start_strata);
+                    u = __ddiv_rn(__dadd_rn(s, u), (double)P.start_strata);
+                }
+                if (P.start_grid) {  // midpoint of arc floor(u*Q) of Q equal arcs
+                    const uint32_t q = (uint32_t)__dmul_rn(u, (double)P.start_grid);
+                    u = __ddiv_rn(__dadd_rn((double)q, 0.5), (double)P.start_grid);
+                    if (P.rec_q) bin1 = -2 - (int)q;  // the arc rides in bin1 until the first hop
+                }
+            }
+            if (starting && uniform_start) {
+                side = perimeter_point(sq, u, px, py);
+            } else {
+                const int bin = bin_of(s_intg, s_guide, u);
+                point_from_index(sq, bin, exact, px, py);
+                if (hop == 1) {
+                    if (P.rec_q) P.rec_q[walk_index()] = (-2 - bin1) * FRW_NSAMPLE + bin;
+                    bin1 = bin;
+                    a0 = __dsub_rn(sq[2], sq[0]);
+                    if (P.rec_cv) *reinterpret_cast<double2 *>(&P.rec_cv[walk_index()]) = make_double2(px, py);
+                }
+            }
+            starting = false;
+        }
+
+        // ---- one query of every active walk ----
         int code = 0x7FFFFFFF;  // != ended
         if (active) {
             const WalkJob &J = job_of<kMulti>(P, job);
@@ -351,18 +375,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
                 hops++;
                 if (hit != kNoHit) code = hit;
                 else if (hops >= P.hop_cap) code = -2;
-                else {
-                    hop++;
-                    if ((hop & 3) == 0) rnd = draw_block(seed, stream, pw, hop);
-                    const int bin = bin_of(s_intg, s_guide, word_u(rnd, hop));
-                    point_from_index(sq, bin, exact, px, py);
-                    if (hop == 1) {
-                        if (P.rec_q) P.rec_q[walk_index()] = (-2 - bin1) * FRW_NSAMPLE + bin;
-                        bin1 = bin;
-                        a0 = __dsub_rn(sq[2], sq[0]);
-                        if (P.rec_cv) *reinterpret_cast<double2 *>(&P.rec_cv[walk_index()]) = make_double2(px, py);
-                    }
-                }
+                else hop++;  // the next point, on the square just found, uses word `hop`
             }
         }
         const bool ended = active && code != 0x7FFFFFFF;
