@@ -677,6 +677,8 @@ int device_sms() {
 
 int mlp_kernels() { return g_mlp_kernels.load(std::memory_order_relaxed); }
 
+int device_sm_count() { return device_sms(); }
+
 frw_status set_mlp_kernels(int which) {
     if (which != FRW_MLP_TCGEN05 && which != FRW_MLP_MMA_SYNC) {
         set_error("frw_mlp_set_kernels: FRW_MLP_TCGEN05 or FRW_MLP_MMA_SYNC");
@@ -700,8 +702,15 @@ frw_status launch_forward(const Net &n, const __nv_bfloat16 *x, int64_t rows, fl
 frw_status launch_train_grad(const Net &n, const __nv_bfloat16 *x, const float *y, const float *wt, int64_t rows,
                              float inv_wsum, float *grad, double *loss, uint32_t *status, cudaStream_t st) {
     if (rows <= 0) return FRW_OK;
-    if (mlp_kernels() == FRW_MLP_TCGEN05)
-        return launch_train_grad_tc(n, x, y, wt, rows, inv_wsum, grad, loss, status, device_sms(), st);
+    if (mlp_kernels() == FRW_MLP_TCGEN05) {  // partial sums per CTA, then added to grad
+        const int sms = device_sms(), nb = train_blocks_tc(rows, sms);
+        float *part = nullptr;
+        FRW_CK(cudaMallocAsync(&part, (size_t)nb * kPartStride * sizeof(float), st));
+        frw_status rc = launch_train_grad_tc(n, x, y, wt, rows, inv_wsum, part, loss, status, sms, st);
+        if (!rc) rc = launch_reduce_sum_tc(part, nb, grad, st);
+        cudaFreeAsync(part, st);
+        return rc;
+    }
     const int64_t chunks = (rows + kRowsPerBlock - 1) / kRowsPerBlock;
     const int blocks = (int)std::min<int64_t>(chunks, 148 * 2);
     k_train_grad<<<blocks, 128, 0, st>>>(n.p, n.w1, n.w2, n.w2t, x, y, wt, rows, inv_wsum, grad, loss);

@@ -51,9 +51,19 @@ frw_status launch_train_grad(const Net &n, const __nv_bfloat16 *x, const float *
                              float inv_wsum, float *grad, double *loss, uint32_t *status, cudaStream_t st);
 frw_status launch_forward_tc(const Net &n, const __nv_bfloat16 *x, int64_t rows, float *out, uint32_t *status,
                              int sms, cudaStream_t st);
+// tcgen05 training step: each CTA writes its partial gradient to its slot of
+// part ([train_blocks_tc(rows, sms)][kPartStride] floats); launch_reduce_adam_tc
+// then sums the slots in CTA order and applies Adam at step t (1-based), or
+// launch_reduce_sum_tc adds them to a gradient.
+constexpr int kPartStride = (kParams + 3) & ~3;  // floats per CTA slot: 16-byte aligned slots
+int train_blocks_tc(int64_t rows, int sms);
 frw_status launch_train_grad_tc(const Net &n, const __nv_bfloat16 *x, const float *y, const float *wt, int64_t rows,
-                                float inv_wsum, float *grad, double *loss, uint32_t *status, int sms,
+                                float inv_wsum, float *part, double *loss, uint32_t *status, int sms,
                                 cudaStream_t st);
+frw_status launch_reduce_adam_tc(const Net &n, const float *part, int nb, float *m, float *v, int t, float lr,
+                                 cudaStream_t st);
+frw_status launch_reduce_sum_tc(const float *part, int nb, float *grad, cudaStream_t st);
+int device_sm_count();
 frw_status launch_adam(const Net &n, float *grad, float *m, float *v, int *step, float lr, cudaStream_t st);
 // exact mean E[f] over every (grid start, first-hop bin) pair, accumulated into *sum
 frw_status launch_quad_mean(const DevLayout &L, double4 target_rect, int target_id, const double4 *gauss, uint32_t Q,

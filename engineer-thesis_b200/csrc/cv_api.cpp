@@ -167,7 +167,7 @@ frw_status frw_cv_train(const frw_layout *layout, int64_t target, const frw_opts
         int64_t *d_end;
         double4 *d_rec;
         __nv_bfloat16 *d_x;
-        float *d_y, *d_wt, *d_grad, *d_m, *d_v;
+        float *d_y, *d_wt, *d_grad, *d_m, *d_v, *d_part = nullptr;
         double *d_wsum, *d_loss;
         int *d_step;
         uint32_t *d_tstatus;
@@ -186,6 +186,10 @@ frw_status frw_cv_train(const frw_layout *layout, int64_t target, const frw_opts
         if (e == cudaSuccess) e = B.get(&d_loss, (size_t)steps * 8);
         if (e == cudaSuccess) e = B.get(&d_step, 4);
         if (e == cudaSuccess) e = B.get(&d_tstatus, 4);
+        const bool tc = cv::mlp_kernels() == FRW_MLP_TCGEN05;
+        const int sms_tc = tc ? cv::device_sm_count() : 0;
+        const int nb_tc = tc ? cv::train_blocks_tc(co.batch, sms_tc) : 0;
+        if (e == cudaSuccess && tc) e = B.get(&d_part, (size_t)nb_tc * cv::kPartStride * sizeof(float));
         if (e != cudaSuccess) return fail(cuda_fail(e, "frw_cv_train: allocation"));
         cudaEventRecord(e0, st);
         // training walks start anywhere on the surface: a stratified start
@@ -228,9 +232,16 @@ frw_status frw_cv_train(const frw_layout *layout, int64_t target, const frw_opts
             const int64_t start = (int64_t)(s % steps_per_epoch) * co.batch;
             const int64_t rows = std::min<int64_t>(co.batch, N - start);
             const float inv = (float)(scale / (double)rows);
-            rc = cv::launch_train_grad(M->net, d_x + 16 * start, d_y + start, d_wt + start, rows, inv, d_grad,
-                                       d_loss + s, d_tstatus, st);
-            if (!rc) rc = cv::launch_adam(M->net, d_grad, d_m, d_v, d_step, co.lr, st);
+            if (tc) {  // partial gradients per CTA, summed in CTA order with the Adam step
+                const int nb = cv::train_blocks_tc(rows, sms_tc);
+                rc = cv::launch_train_grad_tc(M->net, d_x + 16 * start, d_y + start, d_wt + start, rows, inv, d_part,
+                                              d_loss + s, d_tstatus, sms_tc, st);
+                if (!rc) rc = cv::launch_reduce_adam_tc(M->net, d_part, nb, d_m, d_v, s + 1, co.lr, st);
+            } else {
+                rc = cv::launch_train_grad(M->net, d_x + 16 * start, d_y + start, d_wt + start, rows, inv, d_grad,
+                                           d_loss + s, d_tstatus, st);
+                if (!rc) rc = cv::launch_adam(M->net, d_grad, d_m, d_v, d_step, co.lr, st);
+            }
         }
         if (rc) return fail(rc);
         cudaEventRecord(e1, st);

@@ -41,18 +41,42 @@ constexpr uint32_t kXH = 0;                    // 12 groups: h1 (0-7), x (8-9), 
 constexpr uint32_t kDZ = kXH + 12 * kGrp;      // 16 groups: dz2 (0-7), dz1 (8-15)
 constexpr uint32_t kH2 = kDZ + 16 * kGrp;      // 16 groups: h2 (0-7), ones (8), zeros (9-15)
 constexpr uint32_t kB3 = kH2 + 16 * kGrp;      // 2 groups: (dz3, 1, 0 ...) (0), zeros (1)
-constexpr uint32_t kW1 = kB3 + 2 * kGrp;       // W1 as B (K = 16 inputs, N = 64 outputs)
-constexpr uint32_t kW2 = kW1 + 2048;           // W2 as B (K = 64 inputs, N = 64 outputs)
-constexpr uint32_t kW2T = kW2 + 8192;          // W2^T as B (K = 64 outputs, N = 64 inputs)
-constexpr uint32_t kPar = kW2T + 8192;         // b1[64] b2[64] w3[64] b3 (floats)
-constexpr uint32_t kBar = kPar + 1024;         // mbarrier (8 B), TMEM base (4 B)
-constexpr uint32_t kRed = kBar + 64;           // block reductions: loss (double)
-constexpr uint32_t kSmem = kRed + 64;          // both kernels (the forward pass leaves DZ, H2, B3 unused)
-constexpr uint32_t kTmemCols = 256;
-// Two CTAs per SM at most: 3 x 111 KB exceeds the SM's 228 KB of shared
-// memory, and two CTAs' TMEM (2 x 256 columns) fits the SM's 512 columns,
-// so tcgen05.alloc never waits for another CTA.
-static_assert(kSmem > 228 * 1024 / 3 && 2 * (kSmem + 1024) <= 228 * 1024, "exactly two CTAs per SM");
+// Where the weights, the FP32 vectors, the mbarrier and the reduction slot
+// sit, and how much shared memory and TMEM a CTA takes.  Training: after the
+// four operand buffers, 111 KB and 256 TMEM columns, so at most two CTAs per
+// SM (three would exceed the SM's 228 KB) and their TMEM (2 x 256) fits the
+// SM's 512 columns -- tcgen05.alloc never waits for another CTA.  Forward
+// passes: XH (groups 0-9) and the forward weights only, 31 KB used, 46 KB
+// reserved so that at most four CTAs share an SM, each with 128 columns (Z1,
+// Z2).
+struct TrainMap {
+    static constexpr uint32_t W1 = kB3 + 2 * kGrp;  // W1 as B (K = 16 inputs, N = 64 outputs)
+    static constexpr uint32_t W2 = W1 + 2048;       // W2 as B (K = 64 inputs, N = 64 outputs)
+    static constexpr uint32_t W2T = W2 + 8192;      // W2^T as B (K = 64 outputs, N = 64 inputs)
+    static constexpr uint32_t Par = W2T + 8192;     // b1[64] b2[64] w3[64] b3 (floats)
+    static constexpr uint32_t Bar = Par + 1024;     // mbarrier (8 B), TMEM base (4 B)
+    static constexpr uint32_t Red = Bar + 64;       // block reductions: loss (double)
+    static constexpr uint32_t Smem = Red + 64;
+    static constexpr uint32_t TmemCols = 256;
+    static constexpr int PerSm = 2;
+};
+struct FwdMap {
+    static constexpr uint32_t W1 = 10 * kGrp;
+    static constexpr uint32_t W2 = W1 + 2048;
+    static constexpr uint32_t W2T = W2;  // not loaded
+    static constexpr uint32_t Par = W2 + 8192;
+    static constexpr uint32_t Bar = Par + 1024;
+    static constexpr uint32_t Red = Bar + 64;
+    static constexpr uint32_t Smem = 46 * 1024;
+    static constexpr uint32_t TmemCols = 128;
+    static constexpr int PerSm = 4;
+};
+template <class M>
+constexpr bool residency_ok() {  // (PerSm + 1) CTAs exceed the SM's shared memory, PerSm fit, TMEM fits
+    return (M::PerSm + 1) * (M::Smem + 1024) > 228 * 1024 && M::PerSm * (M::Smem + 1024) <= 228 * 1024 &&
+           M::PerSm * M::TmemCols <= 512 && M::Red + 64 <= M::Smem;
+}
+static_assert(residency_ok<TrainMap>() && residency_ok<FwdMap>(), "CTA residency and TMEM budget");
 
 constexpr long long kWaitCycles = 2000000000ll;  // ~1 s at 2 GHz: bound of every mbarrier wait
 
@@ -156,6 +180,7 @@ __device__ __forceinline__ void st_group_raw(unsigned char *buf, int g, int r, u
 }
 
 // The weights as B operands (K-major core-matrix grids) and the FP32 vectors.
+template <class M>
 __device__ void load_weights(unsigned char *sm, const float *p, const __nv_bfloat16 *w1, const __nv_bfloat16 *w2,
                              const __nv_bfloat16 *w2t, bool need_w2t) {
     const uint4 *w1q = reinterpret_cast<const uint4 *>(w1);
@@ -163,15 +188,15 @@ __device__ void load_weights(unsigned char *sm, const float *p, const __nv_bfloa
     const uint4 *w2tq = reinterpret_cast<const uint4 *>(w2t);
     for (int c = threadIdx.x; c < 64 * 2; c += blockDim.x) {  // W1[n][k]: 64 rows x 2 chunks of 8
         const int n = c >> 1, kc = c & 1;
-        *reinterpret_cast<uint4 *>(sm + kW1 + (n >> 3) * 256 + kc * 128 + (n & 7) * 16) = w1q[c];
+        *reinterpret_cast<uint4 *>(sm + M::W1 + (n >> 3) * 256 + kc * 128 + (n & 7) * 16) = w1q[c];
     }
     for (int c = threadIdx.x; c < 64 * 8; c += blockDim.x) {  // W2[n][k] and W2T[n][k]: 64 rows x 8 chunks
         const int n = c >> 3, kc = c & 7;
         const uint32_t off = (n >> 3) * 1024 + kc * 128 + (n & 7) * 16;
-        *reinterpret_cast<uint4 *>(sm + kW2 + off) = w2q[c];
-        if (need_w2t) *reinterpret_cast<uint4 *>(sm + kW2T + off) = w2tq[c];
+        *reinterpret_cast<uint4 *>(sm + M::W2 + off) = w2q[c];
+        if (need_w2t) *reinterpret_cast<uint4 *>(sm + M::W2T + off) = w2tq[c];
     }
-    float *par = reinterpret_cast<float *>(sm + kPar);
+    float *par = reinterpret_cast<float *>(sm + M::Par);
     for (int i = threadIdx.x; i < kHid; i += blockDim.x) {
         par[i] = p[oB1 + i];
         par[64 + i] = p[oB2 + i];
@@ -183,19 +208,20 @@ __device__ void load_weights(unsigned char *sm, const float *p, const __nv_bfloa
 // ---------------------------------------------------------------- forward
 // CTA set-up shared by the kernels: weights into shared memory, TMEM
 // allocated (warp 0), the mbarrier initialised; returns the TMEM base.
+template <class M>
 __device__ __forceinline__ uint32_t cta_setup(unsigned char *sm, const float *p, const __nv_bfloat16 *w1,
                                               const __nv_bfloat16 *w2, const __nv_bfloat16 *w2t, bool need_w2t) {
-    load_weights(sm, p, w1, w2, w2t, need_w2t);
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + kBar + 8);
+    load_weights<M>(sm, p, w1, w2, w2t, need_w2t);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + M::Bar + 8);
     if (threadIdx.x < 32) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(tslot)),
-                     "r"(kTmemCols)
+                     "r"(M::TmemCols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (threadIdx.x == 0) {
-        mbar_init(su32(sm + kBar));
-        *reinterpret_cast<double *>(sm + kRed) = 0.0;
+        mbar_init(su32(sm + M::Bar));
+        *reinterpret_cast<double *>(sm + M::Red) = 0.0;
     }
     fence_async_smem();
     tc_before();
@@ -205,24 +231,26 @@ __device__ __forceinline__ uint32_t cta_setup(unsigned char *sm, const float *p,
 }
 
 // Releases the TMEM once every access is complete (warp 0, the allocator).
+template <class M>
 __device__ __forceinline__ void cta_teardown(uint32_t tm) {
     tc_before();
     __syncthreads();
     tc_after();
     if (threadIdx.x < 32)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tm), "r"(kTmemCols) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tm), "r"(M::TmemCols) : "memory");
 }
 
 // Forward pass of one tile whose X rows every thread has stored in XH
 // groups 8-9: Z1 = X W1^T, H1 = silu(Z1 + b1), Z2 = H1 W2^T, and this
 // thread's output silu(Z2 + b2) . w3 + b3.  `fail` is block-uniform on
 // return (true: a completion wait passed its bound; the output is void).
+template <class M>
 __device__ __forceinline__ float forward_tile(unsigned char *sm, uint32_t tm, uint32_t mbar, uint32_t &phase,
                                               bool &fail) {
     const int tid = threadIdx.x;
     const uint32_t tlane = tm + ((uint32_t)(32 * (tid >> 5)) << 16);
-    const float *par = reinterpret_cast<const float *>(sm + kPar);
-    const uint32_t sxh = su32(sm + kXH), sw1 = su32(sm + kW1), sw2 = su32(sm + kW2);
+    const float *par = reinterpret_cast<const float *>(sm + M::Par);
+    const uint32_t sxh = su32(sm + kXH), sw1 = su32(sm + M::W1), sw2 = su32(sm + M::W2);
     fence_async_smem();
     if ((fail = __syncthreads_or(fail))) return 0.f;
     if (tid == 0) {
@@ -283,8 +311,8 @@ __global__ void __launch_bounds__(kThreads) k_forward_tc(const float *__restrict
                                                          float *__restrict__ out, uint32_t *status) {
     extern __shared__ __align__(1024) unsigned char sm[];
     const int tid = threadIdx.x;
-    const uint32_t tm = cta_setup(sm, p, w1, w2, nullptr, false);
-    const uint32_t mbar = su32(sm + kBar);
+    const uint32_t tm = cta_setup<FwdMap>(sm, p, w1, w2, nullptr, false);
+    const uint32_t mbar = su32(sm + FwdMap::Bar);
     uint32_t phase = 0;
     bool fail = false;
     const int64_t tiles = (rows + kThreads - 1) / kThreads;
@@ -298,11 +326,11 @@ __global__ void __launch_bounds__(kThreads) k_forward_tc(const float *__restrict
         }
         st_group_raw(sm + kXH, 8, tid, x0);
         st_group_raw(sm + kXH, 9, tid, x1);
-        const float o = forward_tile(sm, tm, mbar, phase, fail);
+        const float o = forward_tile<FwdMap>(sm, tm, mbar, phase, fail);
         if (!fail && row < rows) out[row] = o;
     }
     if (fail && tid == 0) atomicOr(status, kStDeviceWait);
-    cta_teardown(tm);
+    cta_teardown<FwdMap>(tm);
 }
 
 // The exact mean of the control variate (cv.cu's k_quad_mean) with the MLP on
@@ -318,8 +346,8 @@ __global__ void __launch_bounds__(kThreads) k_quad_mean_tc(
     float *__restrict__ phi_out, uint32_t *status) {
     extern __shared__ __align__(1024) unsigned char sm[];
     const int tid = threadIdx.x;
-    const uint32_t tm = cta_setup(sm, p, w1, w2, nullptr, false);
-    const uint32_t mbar = su32(sm + kBar);
+    const uint32_t tm = cta_setup<FwdMap>(sm, p, w1, w2, nullptr, false);
+    const uint32_t mbar = su32(sm + FwdMap::Bar);
     uint32_t phase = 0;
     bool fail = false;
     const int64_t n = (int64_t)Q * FRW_NSAMPLE;
@@ -357,7 +385,7 @@ __global__ void __launch_bounds__(kThreads) k_quad_mean_tc(
         }
         st_group(sm + kXH, 8, tid, f);
         st_group(sm + kXH, 9, tid, f + 8);
-        const float phi = forward_tile(sm, tm, mbar, phase, fail);
+        const float phi = forward_tile<FwdMap>(sm, tm, mbar, phase, fail);
         if (!fail) {
             acc += wgt * (double)phi;
             if (phi_out && t < n) phi_out[t] = phi;
@@ -367,7 +395,7 @@ __global__ void __launch_bounds__(kThreads) k_quad_mean_tc(
     for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
     if ((tid & 31) == 0 && !fail) atomicAdd(sum, acc);
     if (fail && tid == 0) atomicOr(status, kStDeviceWait);
-    cta_teardown(tm);
+    cta_teardown<FwdMap>(tm);
 }
 
 // ---------------------------------------------------------------- training
@@ -378,7 +406,7 @@ __global__ void __launch_bounds__(kThreads) k_train_grad_tc(const float *__restr
                                                             const __nv_bfloat16 *__restrict__ w2t,
                                                             const __nv_bfloat16 *__restrict__ x,
                                                             const float *__restrict__ y, const float *__restrict__ wt,
-                                                            int64_t rows, float inv_wsum, float *__restrict__ grad,
+                                                            int64_t rows, float inv_wsum, float *__restrict__ part,
                                                             double *__restrict__ loss_out, uint32_t *status) {
     extern __shared__ __align__(1024) unsigned char sm[];
     const int tid = threadIdx.x, warp = tid >> 5;
@@ -391,13 +419,13 @@ __global__ void __launch_bounds__(kThreads) k_train_grad_tc(const float *__restr
         for (int g = 9; g < 16; g++) st_group_raw(sm + kH2, g, tid, z);
         st_group_raw(sm + kB3, 1, tid, z);
     }
-    const uint32_t tm = cta_setup(sm, p, w1, w2, w2t, true);
-    double *red = reinterpret_cast<double *>(sm + kRed);
-    const uint32_t mbar = su32(sm + kBar);
+    const uint32_t tm = cta_setup<TrainMap>(sm, p, w1, w2, w2t, true);
+    double *red = reinterpret_cast<double *>(sm + TrainMap::Red);
+    const uint32_t mbar = su32(sm + TrainMap::Bar);
     const uint32_t tlane = tm + ((uint32_t)(32 * warp) << 16);
-    const float *par = reinterpret_cast<const float *>(sm + kPar);
+    const float *par = reinterpret_cast<const float *>(sm + TrainMap::Par);
     const uint32_t sxh = su32(sm + kXH), sdz = su32(sm + kDZ), sh2 = su32(sm + kH2), sb3 = su32(sm + kB3);
-    const uint32_t sw1 = su32(sm + kW1), sw2 = su32(sm + kW2), sw2t = su32(sm + kW2T);
+    const uint32_t sw1 = su32(sm + TrainMap::W1), sw2 = su32(sm + TrainMap::W2), sw2t = su32(sm + TrainMap::W2T);
     uint32_t phase = 0;
     bool fail = false;
     double lsum = 0.0;
@@ -540,27 +568,34 @@ __global__ void __launch_bounds__(kThreads) k_train_grad_tc(const float *__restr
     if (__syncthreads_or(fail)) {
         if (tid == 0) atomicOr(status, kStDeviceWait);
     } else if (ntile > 0) {
+        // this CTA's gradient, in the packed parameter order, to its own slot
+        // of the partial sums (plain stores; k_reduce_adam / k_reduce_sum add
+        // the slots up in a fixed order)
+        float *g = part + (size_t)blockIdx.x * kPartStride;
         float v[32];
         if (warp < 2) {  // f = tid: dW2[f][0..63], db2[f], dw3[f]
             const int f = tid;
             tmem_ld32(tlane + 128, v);
 #pragma unroll
-            for (int i = 0; i < 32; i++) atomicAdd(&grad[oW2 + f * kHid + i], v[i]);
+            for (int i = 0; i < 32; i += 4)
+                *reinterpret_cast<float4 *>(g + oW2 + f * kHid + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
             tmem_ld32(tlane + 160, v);
 #pragma unroll
-            for (int i = 0; i < 32; i++) atomicAdd(&grad[oW2 + f * kHid + 32 + i], v[i]);
+            for (int i = 0; i < 32; i += 4)
+                *reinterpret_cast<float4 *>(g + oW2 + f * kHid + 32 + i) =
+                    make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
             tmem_ld32(tlane + 192, v);
-            atomicAdd(&grad[oB2 + f], v[16]);
+            g[oB2 + f] = v[16];
             tmem_ld32(tlane + 224, v);
-            atomicAdd(&grad[oW3 + f], v[0]);
+            g[oW3 + f] = v[0];
         } else {  // f = tid - 64: dW1[f][0..15], db1[f]; lane 64 also holds db3
             const int f = tid - 64;
             tmem_ld32(tlane + 192, v);
 #pragma unroll
-            for (int i = 0; i < 16; i++) atomicAdd(&grad[oW1 + f * kIn + i], v[i]);
-            atomicAdd(&grad[oB1 + f], v[16]);
+            for (int i = 0; i < 16; i++) g[oW1 + f * kIn + i] = v[i];
+            g[oB1 + f] = v[16];
             tmem_ld32(tlane + 224, v);
-            if (f == 0) atomicAdd(&grad[oB3], v[0]);
+            if (f == 0) g[oB3] = v[0];
         }
         // loss: warp sums, then one atomic per CTA
 #pragma unroll
@@ -569,31 +604,84 @@ __global__ void __launch_bounds__(kThreads) k_train_grad_tc(const float *__restr
     }
     __syncthreads();
     if (tid == 0 && !fail && ntile > 0) atomicAdd(loss_out, red[0]);
-    cta_teardown(tm);
+    cta_teardown<TrainMap>(tm);
+}
+
+// The gradient of a training step: the CTAs' partial sums added in CTA
+// order (so the step is reproducible), then Adam on the FP32 master copy and
+// the BF16 operand copies refreshed -- the same update as cv.cu's k_adam, at
+// step t (1-based).
+__global__ void k_reduce_adam(const float *__restrict__ part, int nb, float *__restrict__ p, float *__restrict__ m,
+                              float *__restrict__ v, int t, float lr, __nv_bfloat16 *__restrict__ w1,
+                              __nv_bfloat16 *__restrict__ w2, __nv_bfloat16 *__restrict__ w2t) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kParams) return;
+    float gi = 0.f;
+    for (int b = 0; b < nb; b++) gi += part[(size_t)b * kPartStride + i];
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float mh = mi / (1.f - powf(b1, (float)t)), vh = vi / (1.f - powf(b2, (float)t));
+    const float pi = p[i] - lr * mh / (sqrtf(vh) + 1e-8f);
+    p[i] = pi;
+    if (i < oB1) w1[i] = __float2bfloat16_rn(pi);
+    else if (i >= oW2 && i < oB2) {
+        const int k = i - oW2;
+        w2[k] = __float2bfloat16_rn(pi);
+        w2t[(k % kHid) * kHid + k / kHid] = __float2bfloat16_rn(pi);
+    }
+}
+
+// grad += the CTAs' partial sums, in CTA order.
+__global__ void k_reduce_sum(const float *__restrict__ part, int nb, float *__restrict__ grad) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kParams) return;
+    float gi = 0.f;
+    for (int b = 0; b < nb; b++) gi += part[(size_t)b * kPartStride + i];
+    grad[i] += gi;
 }
 
 }  // namespace
 
+int train_blocks_tc(int64_t rows, int sms) {
+    const int64_t tiles = (rows + kThreads - 1) / kThreads;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(tiles, TrainMap::PerSm * (int64_t)sms));
+}
+
 frw_status launch_forward_tc(const Net &n, const __nv_bfloat16 *x, int64_t rows, float *out, uint32_t *status,
                              int sms, cudaStream_t st) {
     if (rows <= 0) return FRW_OK;
-    FRW_CK(cudaFuncSetAttribute(k_forward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem));
+    FRW_CK(cudaFuncSetAttribute(k_forward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, FwdMap::Smem));
     const int64_t tiles = (rows + kThreads - 1) / kThreads;
-    const int blocks = (int)std::min<int64_t>(tiles, 2 * (int64_t)sms);
-    k_forward_tc<<<blocks, kThreads, kSmem, st>>>(n.p, n.w1, n.w2, x, rows, out, status);
+    const int blocks = (int)std::min<int64_t>(tiles, FwdMap::PerSm * (int64_t)sms);
+    k_forward_tc<<<blocks, kThreads, FwdMap::Smem, st>>>(n.p, n.w1, n.w2, x, rows, out, status);
     FRW_CK(cudaGetLastError());
     return FRW_OK;
 }
 
 frw_status launch_train_grad_tc(const Net &n, const __nv_bfloat16 *x, const float *y, const float *wt, int64_t rows,
-                                float inv_wsum, float *grad, double *loss, uint32_t *status, int sms,
+                                float inv_wsum, float *part, double *loss, uint32_t *status, int sms,
                                 cudaStream_t st) {
     if (rows <= 0) return FRW_OK;
-    FRW_CK(cudaFuncSetAttribute(k_train_grad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem));
-    const int64_t tiles = (rows + kThreads - 1) / kThreads;
-    const int blocks = (int)std::min<int64_t>(tiles, 2 * (int64_t)sms);
-    k_train_grad_tc<<<blocks, kThreads, kSmem, st>>>(n.p, n.w1, n.w2, n.w2t, x, y, wt, rows, inv_wsum, grad,
-                                                          loss, status);
+    FRW_CK(cudaFuncSetAttribute(k_train_grad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, TrainMap::Smem));
+    const int blocks = train_blocks_tc(rows, sms);
+    k_train_grad_tc<<<blocks, kThreads, TrainMap::Smem, st>>>(n.p, n.w1, n.w2, n.w2t, x, y, wt, rows, inv_wsum, part,
+                                                              loss, status);
+    FRW_CK(cudaGetLastError());
+    return FRW_OK;
+}
+
+frw_status launch_reduce_adam_tc(const Net &n, const float *part, int nb, float *m, float *v, int t, float lr,
+                                 cudaStream_t st) {
+    k_reduce_adam<<<(kParams + 255) / 256, 256, 0, st>>>(part, nb, n.p, m, v, t, lr, n.w1, n.w2, n.w2t);
+    FRW_CK(cudaGetLastError());
+    return FRW_OK;
+}
+
+frw_status launch_reduce_sum_tc(const float *part, int nb, float *grad, cudaStream_t st) {
+    k_reduce_sum<<<(kParams + 255) / 256, 256, 0, st>>>(part, nb, grad);
     FRW_CK(cudaGetLastError());
     return FRW_OK;
 }
@@ -602,10 +690,10 @@ frw_status launch_quad_mean_tc(const DevLayout &L, double4 trect, int tid, const
                                const int *sides, uint32_t Q, const double *pi_exact, const double *wx,
                                const double *wy, double eps, bool exact, const Net &net, double *sum, float *phi_out,
                                uint32_t *status, int sms, cudaStream_t st) {
-    FRW_CK(cudaFuncSetAttribute(k_quad_mean_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem));
+    FRW_CK(cudaFuncSetAttribute(k_quad_mean_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, FwdMap::Smem));
     const int64_t tiles = ((int64_t)Q * FRW_NSAMPLE + kThreads - 1) / kThreads;
-    const int blocks = (int)std::min<int64_t>(tiles, 2 * (int64_t)sms);
-    k_quad_mean_tc<<<blocks, kThreads, kSmem, st>>>(L, trect, tid, gauss, sqs, sides, Q, pi_exact, wx, wy, eps, exact,
+    const int blocks = (int)std::min<int64_t>(tiles, FwdMap::PerSm * (int64_t)sms);
+    k_quad_mean_tc<<<blocks, kThreads, FwdMap::Smem, st>>>(L, trect, tid, gauss, sqs, sides, Q, pi_exact, wx, wy, eps, exact,
                                                     net.p, net.w1, net.w2, sum, phi_out, status);
     FRW_CK(cudaGetLastError());
     return FRW_OK;
