@@ -240,7 +240,6 @@ __device__ __forceinline__ uint32_t replay_square(const DevLayout &L, const Cand
         return 0;
     }
     double dist = L.dist0;
-    bool maxReached = false, isc;
     uint32_t st = 0;
     // the loop's first box is p +- 1 again, already found free: its step (grow
     // by dist, no halving before the first collision) is taken directly
@@ -249,25 +248,40 @@ __device__ __forceinline__ uint32_t replay_square(const DevLayout &L, const Cand
     o[2] = __dadd_rn(o[2], dist);
     o[3] = __dadd_rn(o[3], dist);
     int it = 1;
-    while ((isc = collides_box(L, C, o, W)) || !maxReached || above_min(dist)) {
-        if (isc) {
-            if (above_min(dist)) dist = half_of(dist);
-            maxReached = true;
-            o[0] = __dadd_rn(o[0], dist);
-            o[1] = __dadd_rn(o[1], dist);
-            o[2] = __dsub_rn(o[2], dist);
-            o[3] = __dsub_rn(o[3], dist);
-        } else {
-            if (maxReached) dist = half_of(dist);
-            o[0] = __dsub_rn(o[0], dist);
-            o[1] = __dsub_rn(o[1], dist);
-            o[2] = __dadd_rn(o[2], dist);
-            o[3] = __dadd_rn(o[3], dist);
+    // Growth (the reference's maxReached still false): grow by dist, without
+    // halving, until a box collides.
+    bool isc = collides_box(L, C, o, W);
+    while (!isc) {
+        o[0] = __dsub_rn(o[0], dist);
+        o[1] = __dsub_rn(o[1], dist);
+        o[2] = __dadd_rn(o[2], dist);
+        o[3] = __dadd_rn(o[3], dist);
+        if (++it > kReplayCap) {
+            st |= kStReplayCap;
+            sq[0] = o[0]; sq[1] = o[1]; sq[2] = o[2]; sq[3] = o[3];
+            return st;
         }
+        isc = collides_box(L, C, o, W);
+    }
+    // Bisection (maxReached): the loop runs while the box collides or dist is
+    // above MIN_DIST; a colliding box shrinks by dist, halved first while above
+    // MIN_DIST, a free one grows by half of dist.  Both as one signed step --
+    // x + (-d) rounds exactly as x - d -- so a warp whose lanes disagree on the
+    // collision issues the four updates once.
+    for (;;) {
+        const bool am = above_min(dist);
+        if (!isc && !am) break;
+        if (!isc || am) dist = half_of(dist);
+        const double sd = isc ? dist : -dist;
+        o[0] = __dadd_rn(o[0], sd);
+        o[1] = __dadd_rn(o[1], sd);
+        o[2] = __dsub_rn(o[2], sd);
+        o[3] = __dsub_rn(o[3], sd);
         if (++it > kReplayCap) {
             st |= kStReplayCap;
             break;
         }
+        isc = collides_box(L, C, o, W);
     }
     sq[0] = o[0]; sq[1] = o[1]; sq[2] = o[2]; sq[3] = o[3];
     return st;
