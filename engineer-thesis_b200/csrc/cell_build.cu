@@ -11,9 +11,11 @@
 // containing p (max with 0).  The margin (M * 2^-30, M the layout's
 // coordinate scale) covers the rounding of the cell index of p and of the
 // cell's coordinates, both of order M * 2^-50.  Built from the tree: one
-// clearance query at each cell centre, then a count -> scan -> fill pair of
-// box enumerations.  Cells with more than max_per_cell rects keep count -1
-// and their points use the tree.
+// clearance query at each cell centre and one box enumeration per cell (the
+// count pass), a scan, then the fill pass, which copies the rects the count
+// pass staged (the first kStage of each cell) and enumerates again only the
+// longer cells, from the radius the count pass kept.  Cells with more than
+// max_per_cell rects keep count -1 and their points use the tree.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -28,6 +30,9 @@ namespace {
 constexpr int kScanThreads = 1024;
 constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanThreads * kScanItems;
+// rect indices staged per cell by the count pass (a cell of the configs'
+// density lists about 2 rects)
+constexpr int kStage = 4;
 
 // Visits the tree's rects touching the closed box B, in tree order, until
 // visit() returns false.  Returns false when the traversal stack overflowed
@@ -67,60 +72,83 @@ struct Grid {
     int nx, ny;
 };
 
-// The cell grown by its radius r_C (returned).
-__device__ __forceinline__ double cell_box(const DevLayout &L, const Grid &G, int64_t c, double B[4]) {
+// The box of cell c grown by r.
+__device__ __forceinline__ void grown_box(const Grid &G, int64_t c, double r, double B[4]) {
     const int ix = (int)(c % G.nx), iy = (int)(c / G.nx);
     const double x0 = G.gx0 + ix * G.side, y0 = G.gy0 + iy * G.side;
-    const double x1 = x0 + G.side, y1 = y0 + G.side;
+    B[0] = x0 - r;
+    B[1] = y0 - r;
+    B[2] = (x0 + G.side) + r;
+    B[3] = (y0 + G.side) + r;
+}
+
+// The radius r_C of cell c: the tree's clearance at the cell centre.
+__device__ __forceinline__ double cell_radius(const DevLayout &L, const Grid &G, int64_t c) {
+    const int ix = (int)(c % G.nx), iy = (int)(c / G.nx);
+    const double x0 = G.gx0 + ix * G.side, y0 = G.gy0 + iy * G.side;
     Cands C;
     int hit;
     double best;
     clearance(L, x0 + 0.5 * G.side, y0 + 0.5 * G.side, C, hit, best);  // L has no cells: the tree
-    const double r = fmax(best, 0.0) + 0.5 * G.side + 2.0 * L.delta + G.margin;
-    B[0] = x0 - r;
-    B[1] = y0 - r;
-    B[2] = x1 + r;
-    B[3] = y1 + r;
-    return r;
+    return fmax(best, 0.0) + 0.5 * G.side + 2.0 * L.delta + G.margin;
 }
 
 // Per cell: its list length, or -1 (in cells[c].y) when it exceeds cap or
-// the enumeration was incomplete; cnt[c] = entries to reserve.
+// the enumeration was incomplete; cnt[c] = entries to reserve; rad[c] its
+// radius and stage[kStage c ..] the (Morton) indices of its first kStage
+// rects, for the fill pass.
 __global__ void k_cell_count(DevLayout L, Grid G, int cap, int64_t *__restrict__ cnt, int2 *__restrict__ cells,
-                             float *__restrict__ crad, unsigned long long *overflow, int64_t ncells) {
+                             float *__restrict__ crad, double *__restrict__ rad, int32_t *__restrict__ stage,
+                             unsigned long long *overflow, int64_t ncells) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncells) return;
+    const double r = cell_radius(L, G, c);
     double B[4];
-    const double r = cell_box(L, G, c, B);
+    grown_box(G, c, r, B);
+    rad[c] = r;
     // a point of the cell lies within margin/2 of it whatever the rounding of
     // its cell index, so every rect within r - margin of the point is listed
     crad[c] = __double2float_rd(r - G.margin);
     int n = 0;
-    const bool complete = touching(L, B, [&](int, float4) { return ++n <= cap; });
+    int32_t *sg = stage + kStage * c;
+    const bool complete = touching(L, B, [&](int k, float4) {
+        if (n < kStage) sg[n] = k;
+        return ++n <= cap;
+    });
     const bool ok = complete && n <= cap;
     cnt[c] = ok ? n : 0;
     cells[c] = make_int2(0, ok ? n : -1);
     if (!ok) atomicAdd(overflow, 1ull);
 }
 
-// Writes the lists of the cells that did not overflow (the enumeration order
-// is deterministic, so it meets the same rects as the count).
-__global__ void k_cell_fill(DevLayout L, Grid G, const int64_t *__restrict__ start, int2 *__restrict__ cells,
-                            float4 *__restrict__ crects, int32_t *__restrict__ cids, int64_t ncells) {
+// Writes the lists of the cells that did not overflow: the staged rects, or
+// for longer lists the enumeration of the same grown box again (its order is
+// deterministic, so it meets the same rects as the count).
+__global__ void k_cell_fill(DevLayout L, Grid G, const int64_t *__restrict__ start, const double *__restrict__ rad,
+                            const int32_t *__restrict__ stage, int2 *__restrict__ cells, float4 *__restrict__ crects,
+                            int32_t *__restrict__ cids, int64_t ncells) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncells) return;
     const int m = cells[c].y;
     if (m < 0) return;
-    double B[4];
-    cell_box(L, G, c, B);
     const int64_t s = start[c];
-    int n = 0;
-    touching(L, B, [&](int k, float4 r) {
-        if (n >= m) return false;
-        crects[s + n] = r;
-        cids[s + n] = __ldg(L.ids + k);
-        return ++n < m;
-    });
+    if (m <= kStage) {
+        for (int i = 0; i < m; i++) {
+            const int k = stage[kStage * c + i];
+            crects[s + i] = __ldg(L.rects + k);
+            cids[s + i] = __ldg(L.ids + k);
+        }
+    } else {
+        double B[4];
+        grown_box(G, c, rad[c], B);
+        int n = 0;
+        touching(L, B, [&](int k, float4 r) {
+            if (n >= m) return false;
+            crects[s + n] = r;
+            cids[s + n] = __ldg(L.ids + k);
+            return ++n < m;
+        });
+    }
     cells[c] = make_int2((int)s, m);
 }
 
@@ -256,6 +284,8 @@ frw_status build_cells(const DevLayout &Lin, double cells_per_rect, int cap, cud
     C.side = side;
     C.ginv = 1.0 / side;
     int64_t *cnt = nullptr, *start = nullptr, *sums = nullptr, *grand = nullptr;
+    double *rad = nullptr;
+    int32_t *stage = nullptr;
     unsigned long long *ovf = nullptr;
     const int64_t tiles = (ncells + kScanTile - 1) / kScanTile;
     frw_status rc = FRW_OK;
@@ -269,12 +299,14 @@ frw_status build_cells(const DevLayout &Lin, double cells_per_rect, int cap, cud
         if (!ck(cudaMallocAsync(&C.crad, (size_t)ncells * sizeof(float), st), "malloc cell radii")) break;
         if (!ck(cudaMallocAsync(&cnt, (size_t)ncells * 8, st), "malloc cell counts")) break;
         if (!ck(cudaMallocAsync(&start, (size_t)ncells * 8, st), "malloc cell starts")) break;
+        if (!ck(cudaMallocAsync(&rad, (size_t)ncells * 8, st), "malloc cell radii (build)")) break;
+        if (!ck(cudaMallocAsync(&stage, (size_t)ncells * kStage * 4, st), "malloc staged rects")) break;
         if (!ck(cudaMallocAsync(&sums, (size_t)tiles * 8, st), "malloc tile sums")) break;
         if (!ck(cudaMallocAsync(&grand, 8, st), "malloc total")) break;
         if (!ck(cudaMallocAsync(&ovf, 8, st), "malloc overflow count")) break;
         if (!ck(cudaMemsetAsync(ovf, 0, 8, st), "memset")) break;
         const unsigned blocks = (unsigned)((ncells + 127) / 128);
-        k_cell_count<<<blocks, 128, 0, st>>>(L, G, cap, cnt, C.cells, C.crad, ovf, ncells);
+        k_cell_count<<<blocks, 128, 0, st>>>(L, G, cap, cnt, C.cells, C.crad, rad, stage, ovf, ncells);
         k_tile_sums<<<(unsigned)tiles, kScanThreads, 0, st>>>(cnt, ncells, sums);
         k_scan_sums<<<1, kScanThreads, 0, st>>>(sums, tiles, grand);
         k_tile_scan<<<(unsigned)tiles, kScanThreads, 0, st>>>(cnt, ncells, sums, start);
@@ -292,13 +324,13 @@ frw_status build_cells(const DevLayout &Lin, double cells_per_rect, int cap, cud
         C.overflow = (int64_t)novf;
         if (!ck(cudaMallocAsync(&C.crects, (size_t)std::max<int64_t>(total, 1) * 16, st), "malloc cell rects")) break;
         if (!ck(cudaMallocAsync(&C.cids, (size_t)std::max<int64_t>(total, 1) * 4, st), "malloc cell ids")) break;
-        if (total > 0) k_cell_fill<<<blocks, 128, 0, st>>>(L, G, start, C.cells, C.crects, C.cids, ncells);
+        if (total > 0) k_cell_fill<<<blocks, 128, 0, st>>>(L, G, start, rad, stage, C.cells, C.crects, C.cids, ncells);
         if (!ck(cudaGetLastError(), "cell fill")) break;
         if (!ck(cudaEventRecord(e1, st), "event")) break;
         if ((rc = wait_event(e1, "build_cells"))) break;
         cudaEventElapsedTime(&C.build_ms, e0, e1);
     } while (0);
-    for (void *p : {(void *)cnt, (void *)start, (void *)sums, (void *)grand, (void *)ovf})
+    for (void *p : {(void *)cnt, (void *)start, (void *)sums, (void *)grand, (void *)ovf, (void *)rad, (void *)stage})
         if (p) cudaFreeAsync(p, st);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

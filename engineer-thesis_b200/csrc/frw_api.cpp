@@ -389,83 +389,27 @@ frw_status read_back(void *host, const void *dev, size_t bytes, cudaStream_t st,
     return e == cudaSuccess ? FRW_OK : cuda_fail(e, what);
 }
 
-// Checks the caller's rects (finite, |c| < 2^24, not inverted), converts
-// them to the layout's FP64 host copy and settles the bounds (the given ones,
-// which must contain every rect, or the reference rule from the bounding
-// box), in one pass split over host threads for large layouts.  Errors name
-// the first offending rect.
-frw_status ingest_rects(const float *in, int64_t n, const double *given, double *out, double bounds[4]) {
-    struct Part {
-        int64_t bad = INT64_MAX;
-        int why = 0;  // 1 coordinate, 2 inverted, 3 outside the given bounds
-        double lx = INFINITY, ty = INFINITY, rx = -INFINITY, by = -INFINITY;
-    };
-    if (given && (!(given[0] <= given[2] && given[1] <= given[3]) || !std::isfinite(given[0]) ||
-                  !std::isfinite(given[1]) || !std::isfinite(given[2]) || !std::isfinite(given[3]))) {
-        set_error("bounds invalid");
-        return FRW_E_ARG;
+// The FP64 host copy of a layout's rects (layer order), converted by host
+// threads that run while the device checks the rects and builds the layout;
+// join() before the copy is read or freed.
+struct HostCopy {
+    std::vector<std::thread> th;
+    void start(const float *in, int64_t n, double *out) {
+        const int64_t kChunk = 1 << 17;
+        const int nt = (int)std::min<int64_t>((n + kChunk - 1) / kChunk,
+                                              std::max<unsigned>(1, std::min(8u, std::thread::hardware_concurrency())));
+        for (int t = 0; t < nt; t++)
+            th.emplace_back([=] {
+                const int64_t a = 4 * (n * t / nt), b = 4 * (n * (t + 1) / nt);
+                for (int64_t i = a; i < b; i++) out[i] = in[i];
+            });
     }
-    const int64_t kChunk = 1 << 17;
-    const int nt = (int)std::min<int64_t>((n + kChunk - 1) / kChunk,
-                                          std::max<unsigned>(1, std::min(8u, std::thread::hardware_concurrency())));
-    std::vector<Part> parts(nt);
-    auto work = [&](int t) {
-        Part &P = parts[t];
-        const int64_t a = n * t / nt, b = n * (t + 1) / nt;
-        for (int64_t i = a; i < b; i++) {
-            const float *q = in + 4 * i;
-            double *o = out + 4 * i;
-            bool ok = true;
-            for (int k = 0; k < 4; k++) {
-                ok = ok && std::isfinite(q[k]) && fabsf(q[k]) < 16777216.0f;
-                o[k] = q[k];
-            }
-            int why = !ok ? 1 : (!(q[0] <= q[2] && q[1] <= q[3]) ? 2 : 0);
-            if (!why && given && !(o[1] >= given[1] && o[0] >= given[0] && o[3] <= given[3] && o[2] <= given[2]))
-                why = 3;
-            if (why) {
-                P.bad = i;
-                P.why = why;
-                return;
-            }
-            P.lx = std::min(P.lx, o[0]);
-            P.ty = std::min(P.ty, o[1]);
-            P.rx = std::max(P.rx, o[2]);
-            P.by = std::max(P.by, o[3]);
-        }
-    };
-    if (nt == 1) work(0);
-    else {
-        std::vector<std::thread> th;
-        for (int t = 1; t < nt; t++) th.emplace_back(work, t);
-        work(0);
+    void join() {
         for (auto &x : th) x.join();
+        th.clear();
     }
-    Part all;
-    for (const Part &P : parts) {
-        if (P.bad < all.bad) {
-            all.bad = P.bad;
-            all.why = P.why;
-        }
-        all.lx = std::min(all.lx, P.lx);
-        all.ty = std::min(all.ty, P.ty);
-        all.rx = std::max(all.rx, P.rx);
-        all.by = std::max(all.by, P.by);
-    }
-    if (all.why) {
-        const std::string r = "rect " + std::to_string(all.bad);
-        set_error(all.why == 1 ? r + ": coordinate not finite or |c| >= 2^24"
-                               : all.why == 2 ? r + ": inverted (need x0 <= x1 and y0 <= y1)"
-                                              : r + " lies outside the bounds");
-        return FRW_E_ARG;
-    }
-    if (given) {
-        memcpy(bounds, given, 4 * sizeof(double));
-    } else {
-        bounds_from_extent(all.lx, all.ty, all.rx, all.by, bounds);
-    }
-    return FRW_OK;
-}
+    ~HostCopy() { join(); }
+};
 
 frw_status layout_view(const frw_layout *L, LayoutView *out) {
     if (!L) {
@@ -562,6 +506,11 @@ frw_status frw_layout_create(const float *rects, int64_t n, const double *bounds
         set_error("frw_layout_create: at most 2^26-1 rects per layout");
         return FRW_E_ARG;
     }
+    if (bounds && (!(bounds[0] <= bounds[2] && bounds[1] <= bounds[3]) || !std::isfinite(bounds[0]) ||
+                   !std::isfinite(bounds[1]) || !std::isfinite(bounds[2]) || !std::isfinite(bounds[3]))) {
+        set_error("bounds invalid");
+        return FRW_E_ARG;
+    }
     DeviceCtx *ctx;
     frw_status rc = device_ctx(device, &ctx);
     if (rc) return rc;
@@ -574,16 +523,13 @@ frw_status frw_layout_create(const float *rects, int64_t n, const double *bounds
         set_error("frw_layout_create: host memory for the rect copy");
         return FRW_E_OOM;
     }
-    rc = ingest_rects(rects, n, bounds, L->rects.get(), L->bounds);
-    if (rc) {
-        delete L;
-        return rc;
-    }
     const double *b = L->bounds;
     DeviceGuard g(device);
     cudaStream_t st = (cudaStream_t)stream;
     float4 *d_in = nullptr;
+    HostCopy copy;
     auto fail = [&](frw_status r) {
+        copy.join();
         if (d_in) cudaFreeAsync(d_in, st);
         free_tree(&L->T, st);
         free_cells(&L->cells, st);
@@ -594,6 +540,23 @@ frw_status frw_layout_create(const float *rects, int64_t n, const double *bounds
     if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMallocAsync rects"));
     e = cudaMemcpyAsync(d_in, rects, (size_t)n * 16, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return fail(cuda_fail(e, "upload rects"));
+    copy.start(rects, n, L->rects.get());
+    {
+        // the rects are checked on the device; errors name the first offending rect
+        int64_t bad = -1;
+        int why = 0;
+        double ext[4];
+        rc = check_rects(d_in, n, bounds, ctx->sms, st, &bad, &why, ext);
+        if (rc) return fail(rc);
+        if (bad >= 0) {
+            const std::string r = "rect " + std::to_string(bad);
+            set_error(why == 1 ? r + ": coordinate not finite or |c| >= 2^24"
+                               : why == 2 ? r + ": inverted (need x0 <= x1 and y0 <= y1)" : r + " lies outside the bounds");
+            return fail(FRW_E_ARG);
+        }
+        if (bounds) memcpy(L->bounds, bounds, 4 * sizeof(double));
+        else bounds_from_extent(ext[0], ext[1], ext[2], ext[3], L->bounds);
+    }
     rc = build_tree(d_in, (int32_t)n, L->bounds, L->leaf_max, st, &L->T, &L->build_ms);
     if (rc) return fail(rc);
     cudaFreeAsync(d_in, st);
@@ -633,6 +596,7 @@ frw_status frw_layout_create(const float *rects, int64_t n, const double *bounds
     rc = build_cells(dl, kDefaultCellsPerRect, kDefaultCellMax, st, &L->cells);
     if (rc) return fail(rc);
     attach_cells(dl, L->cells);
+    copy.join();
     *out = L;
     return FRW_OK;
 }

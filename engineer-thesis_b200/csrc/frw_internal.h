@@ -174,6 +174,17 @@ struct TreeBuffers {
     int32_t nodes = 0, depth = 0;
     int64_t bytes = 0;
 };
+// Device check of a layout's rects (finite, |c| < 2^24, x0 <= x1 and
+// y0 <= y1, inside `given` when not null) and the extent of the rects:
+// bad = index of the first offending rect (-1: none) and why its reason
+// (1 coordinate, 2 inverted, 3 outside the given bounds); ext = min x0,
+// min y0, max x1, max y1.  Waits for the stream (bounded).
+struct RectCheck {
+    unsigned long long bad;
+    unsigned key[4];
+};
+frw_status check_rects(const float4 *d_rects, int64_t n, const double *given, int sms, cudaStream_t stream,
+                       int64_t *bad, int *why, double ext[4]);
 frw_status build_tree(const float4 *d_rects_in, int32_t n, const double bounds[4], int leaf_max,
                       cudaStream_t stream, TreeBuffers *out, float *build_ms);
 // Layout buffers come from the device's stream-ordered pool; the free calls

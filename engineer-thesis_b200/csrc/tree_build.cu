@@ -20,6 +20,9 @@
 // the structure (the boxes are exact FP32 unions of FP32-exact rects).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cstddef>
+#include <cstring>
 #include <initializer_list>
 #include <vector>
 
@@ -389,7 +392,116 @@ __global__ void __launch_bounds__(1024) k_build_small(const uint32_t *__restrict
     }
 }
 
+// Order-preserving unsigned key of a float (+0 for -0): unsigned order of
+// the keys is the order of the values.
+__device__ __forceinline__ unsigned f_key(float f) {
+    const unsigned u = __float_as_uint(f + 0.0f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+// Checks every rect (finite, |c| < 2^24, not inverted, inside the given
+// bounds when there are any) and reduces the extent of the valid ones:
+// out->bad = min over bad rects of (index << 2 | reason), out->key = keys of
+// min x0, min y0 (atomicMin) and max x1, max y1 (atomicMax).
+__global__ void __launch_bounds__(256) k_check_rects(const float4 *__restrict__ rects, int64_t n, int has_given,
+                                                     double g0, double g1, double g2, double g3,
+                                                     RectCheck *__restrict__ out) {
+    unsigned k0 = 0xFFFFFFFFu, k1 = 0xFFFFFFFFu, k2 = 0u, k3 = 0u;
+    unsigned long long bad = ~0ull;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float4 q = __ldg(rects + i);
+        const float c[4] = {q.x, q.y, q.z, q.w};
+        bool ok = true;
+#pragma unroll
+        for (int k = 0; k < 4; k++) ok = ok && isfinite(c[k]) && fabsf(c[k]) < 16777216.0f;
+        int why = !ok ? 1 : (!(q.x <= q.z && q.y <= q.w) ? 2 : 0);
+        if (!why && has_given &&
+            !((double)q.y >= g1 && (double)q.x >= g0 && (double)q.w <= g3 && (double)q.z <= g2))
+            why = 3;
+        if (why) {
+            bad = min(bad, ((unsigned long long)i << 2) | (unsigned)why);
+            continue;
+        }
+        k0 = min(k0, f_key(q.x));
+        k1 = min(k1, f_key(q.y));
+        k2 = max(k2, f_key(q.z));
+        k3 = max(k3, f_key(q.w));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        k0 = min(k0, __shfl_xor_sync(0xFFFFFFFFu, k0, o));
+        k1 = min(k1, __shfl_xor_sync(0xFFFFFFFFu, k1, o));
+        k2 = max(k2, __shfl_xor_sync(0xFFFFFFFFu, k2, o));
+        k3 = max(k3, __shfl_xor_sync(0xFFFFFFFFu, k3, o));
+        bad = min(bad, __shfl_xor_sync(0xFFFFFFFFu, bad, o));
+    }
+    __shared__ unsigned sk[4][8];
+    __shared__ unsigned long long sb[8];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        sk[0][w] = k0;
+        sk[1][w] = k1;
+        sk[2][w] = k2;
+        sk[3][w] = k3;
+        sb[w] = bad;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nw = blockDim.x >> 5;
+        for (int j = 1; j < nw; j++) {
+            k0 = min(k0, sk[0][j]);
+            k1 = min(k1, sk[1][j]);
+            k2 = max(k2, sk[2][j]);
+            k3 = max(k3, sk[3][j]);
+            bad = min(bad, sb[j]);
+        }
+        atomicMin(&out->key[0], k0);
+        atomicMin(&out->key[1], k1);
+        atomicMax(&out->key[2], k2);
+        atomicMax(&out->key[3], k3);
+        if (bad != ~0ull) atomicMin(&out->bad, bad);
+    }
+}
+
+float key_value(unsigned k) {
+    const unsigned u = (k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k;
+    float f;
+    memcpy(&f, &u, 4);
+    return f;
+}
+
 }  // namespace
+
+frw_status check_rects(const float4 *d_rects, int64_t n, const double *given, int sms, cudaStream_t st,
+                       int64_t *bad, int *why, double ext[4]) {
+    RectCheck *d = nullptr;
+    FRW_CK(cudaMallocAsync(&d, sizeof(RectCheck), st));
+    frw_status rc = FRW_OK;
+    do {
+        cudaError_t e = cudaMemsetAsync(d, 0xFF, offsetof(RectCheck, key) + 2 * sizeof(unsigned), st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(&d->key[2], 0, 2 * sizeof(unsigned), st);
+        if (e != cudaSuccess) {
+            rc = cuda_fail(e, "check_rects: memset");
+            break;
+        }
+        const int64_t want = (n + 255) / 256;
+        const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)std::max(sms, 1) * 8));
+        k_check_rects<<<blocks, 256, 0, st>>>(d_rects, n, given != nullptr, given ? given[0] : 0.0,
+                                               given ? given[1] : 0.0, given ? given[2] : 0.0,
+                                               given ? given[3] : 0.0, d);
+        if ((e = cudaGetLastError()) != cudaSuccess) {
+            rc = cuda_fail(e, "check_rects: launch");
+            break;
+        }
+        RectCheck h;
+        if ((rc = read_back(&h, d, sizeof(h), st, "check_rects"))) break;
+        *bad = h.bad == ~0ull ? -1 : (int64_t)(h.bad >> 2);
+        *why = h.bad == ~0ull ? 0 : (int)(h.bad & 3);
+        for (int k = 0; k < 4; k++) ext[k] = (double)key_value(h.key[k]);
+    } while (0);
+    cudaFreeAsync(d, st);
+    return rc;
+}
 
 void free_tree(TreeBuffers *t, cudaStream_t st) {
     for (void *p : {(void *)t->rects, (void *)t->ids, (void *)t->nbox, (void *)t->nref})
