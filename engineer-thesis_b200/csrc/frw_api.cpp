@@ -26,10 +26,79 @@
 #include "frw_internal.h"
 #include "layout_io.h"
 
+namespace frw {
+// Host copies of layout rects are kept for reuse when their layout is
+// destroyed (a few buffers, 1 GiB at most), so that a layout created again at
+// the same or a smaller size is written into memory already mapped instead of
+// faulting in fresh pages.
+class HostRectPool {
+    std::mutex mu_;
+    std::vector<std::pair<size_t, double *>> free_;  // (capacity in doubles, buffer)
+    size_t held_ = 0;                                // doubles held in free_
+    static constexpr size_t kMaxHeld = (1ull << 30) / sizeof(double);
+    static constexpr size_t kMaxBuffers = 4;
+
+  public:
+    double *get(size_t n, size_t *cap) {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            size_t best = free_.size();
+            for (size_t i = 0; i < free_.size(); i++)
+                if (free_[i].first >= n && (best == free_.size() || free_[i].first < free_[best].first)) best = i;
+            if (best < free_.size() && free_[best].first <= 2 * n + 4096) {  // not a much larger buffer
+                double *p = free_[best].second;
+                *cap = free_[best].first;
+                held_ -= *cap;
+                free_.erase(free_.begin() + (std::ptrdiff_t)best);
+                return p;
+            }
+        }
+        *cap = n;
+        return new (std::nothrow) double[n];
+    }
+    void put(double *p, size_t cap) {
+        std::lock_guard<std::mutex> g(mu_);
+        if (cap > kMaxHeld) {
+            delete[] p;
+            return;
+        }
+        free_.emplace_back(cap, p);
+        held_ += cap;
+        while (held_ > kMaxHeld || free_.size() > kMaxBuffers) {  // drop the oldest
+            held_ -= free_.front().first;
+            delete[] free_.front().second;
+            free_.erase(free_.begin());
+        }
+    }
+};
+// never destroyed: layouts released during process exit may still return
+// their buffers
+HostRectPool &host_rects() {
+    static HostRectPool *pool = new HostRectPool();
+    return *pool;
+}
+
+struct HostRects {
+    double *p = nullptr;
+    size_t cap = 0;
+    HostRects() = default;
+    HostRects(const HostRects &) = delete;
+    HostRects &operator=(const HostRects &) = delete;
+    ~HostRects() {
+        if (p) host_rects().put(p, cap);
+    }
+    bool acquire(size_t n) {
+        p = host_rects().get(n, &cap);
+        return p != nullptr;
+    }
+    double *get() const { return p; }
+};
+}  // namespace frw
+
 struct frw_layout {
     int device = 0;
     int64_t n = 0;
-    std::unique_ptr<double[]> rects;  // [4 n] layer order, as given
+    frw::HostRects rects;  // [4 n] layer order, as given
     double bounds[4] = {0, 0, 0, 0};
     frw::TreeBuffers T;
     frw::CellBuffers cells;
@@ -517,8 +586,7 @@ frw_status frw_layout_create(const float *rects, int64_t n, const double *bounds
     frw_layout *L = new frw_layout();
     L->device = device;
     L->n = n;
-    L->rects.reset(new (std::nothrow) double[(size_t)n * 4]);
-    if (!L->rects) {
+    if (!L->rects.acquire((size_t)n * 4)) {
         delete L;
         set_error("frw_layout_create: host memory for the rect copy");
         return FRW_E_OOM;
@@ -576,6 +644,11 @@ frw_status frw_layout_create(const float *rects, int64_t n, const double *bounds
         double dist = (bh > bw) ? bh : bw;
         dist *= 0.05;
         dl.dist0 = dist;
+        // the replay's bisection halves dist while it is above MIN_DIST
+        // ((double)0.095f; halving a positive normal double is exact)
+        int halvings = 0;
+        for (double d = dist; d > (double)0.095f && halvings < 64; d *= 0.5) halvings++;
+        dl.halvings = halvings;
         // tie window: every box of a replay has coordinates below
         // M = 4 * max(|bounds|, W, H) + 16 after <= 256 roundings of at most
         // M * 2^-53 each, i.e. within M * 2^-45; delta = M * 2^-40 leaves 32x.

@@ -42,6 +42,7 @@ struct DevLayout {
     double delta;               // tie window of the clearance replay (see query.cuh)
     float slack;                // FP32 pre-filter margin: 4 ulp_f32(max |bound|)
     int32_t n, nodes;
+    int32_t halvings;  // bisection steps of the replay with dist above MIN_DIST: dist0 halved that often
     // cell lists (optional, cells == nullptr: tree only): a gnx x gny grid of
     // side 1/ginv from (gx0, gy0); cell (start, count) into crects / cids,
     // count < 0 when the cell overflowed and its points use the tree

@@ -265,19 +265,33 @@ __device__ __forceinline__ uint32_t replay_square(const DevLayout &L, const Cand
     }
     // Bisection (maxReached): the loop runs while the box collides or dist is
     // above MIN_DIST; a colliding box shrinks by dist, halved first while above
-    // MIN_DIST, a free one grows by half of dist.  Both as one signed step --
-    // x + (-d) rounds exactly as x - d -- so a warp whose lanes disagree on the
-    // collision issues the four updates once.
-    for (;;) {
-        const bool am = above_min(dist);
-        if (!isc && !am) break;
-        if (!isc || am) dist = half_of(dist);
+    // MIN_DIST, a free one grows by half of dist.  While dist is above MIN_DIST
+    // every step halves it whatever the collision, so those steps are the
+    // first L.halvings of the loop, a count fixed by the layout (dist starts at
+    // dist0 every query); each is one signed step -- x + (-d) rounds exactly as
+    // x - d -- so a warp whose lanes disagree on the collision issues the four
+    // updates once.  After them the loop shrinks by dist while the box
+    // collides.
+    if (it + L.halvings > kReplayCap) {  // the iteration bound falls inside the halvings
+        st |= kStReplayCap;
+        sq[0] = o[0]; sq[1] = o[1]; sq[2] = o[2]; sq[3] = o[3];
+        return st;
+    }
+    for (int k = 0; k < L.halvings; k++) {
+        dist = half_of(dist);
         const double sd = isc ? dist : -dist;
         o[0] = __dadd_rn(o[0], sd);
         o[1] = __dadd_rn(o[1], sd);
         o[2] = __dsub_rn(o[2], sd);
         o[3] = __dsub_rn(o[3], sd);
-        if (++it > kReplayCap) {
+        isc = collides_box(L, C, o, W);
+    }
+    while (isc) {
+        o[0] = __dadd_rn(o[0], dist);
+        o[1] = __dadd_rn(o[1], dist);
+        o[2] = __dsub_rn(o[2], dist);
+        o[3] = __dsub_rn(o[3], dist);
+        if (++it > kReplayCap - L.halvings) {
             st |= kStReplayCap;
             break;
         }
