@@ -221,6 +221,12 @@ __device__ __forceinline__ double half_of(double d) {
 __device__ __forceinline__ bool above_min(double d) {
     return __double_as_longlong(d) > __double_as_longlong(kMinDist);
 }
+// d when shrinking (the box collides), -d when growing: the sign bit set by
+// an integer operation on the high word.
+__device__ __forceinline__ double signed_step(double d, bool shrink) {
+    const int hi = __double2hiint(d) ^ (shrink ? 0 : (int)0x80000000);
+    return __hiloint2double(hi, __double2loint(d));
+}
 
 // drawBiggestSquareAtPoint replayed on scalars: same operations, same order,
 // explicit round-to-nearest intrinsics (no contraction); the halvings as
@@ -277,9 +283,10 @@ __device__ __forceinline__ uint32_t replay_square(const DevLayout &L, const Cand
         sq[0] = o[0]; sq[1] = o[1]; sq[2] = o[2]; sq[3] = o[3];
         return st;
     }
+#pragma unroll 4
     for (int k = 0; k < L.halvings; k++) {
         dist = half_of(dist);
-        const double sd = isc ? dist : -dist;
+        const double sd = signed_step(dist, isc);
         o[0] = __dadd_rn(o[0], sd);
         o[1] = __dadd_rn(o[1], sd);
         o[2] = __dsub_rn(o[2], sd);
