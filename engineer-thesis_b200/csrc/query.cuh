@@ -30,11 +30,18 @@ constexpr int kReplayCap = 256;
 constexpr int kNoHit = 0x7FFFFFFF;
 constexpr double kMinDist = (double).095f;  // drawBiggestSquareAtPoint MIN_DIST
 
+// The rects the replay tests for boxes within delta of the clearance: a
+// point answered by a cell list keeps its cell's whole list (first >= 0:
+// base[first .. first + n)), a superset of the near ties; a point answered
+// by the tree keeps the near-tie list idx[0 .. n) (first < 0).  Testing more
+// rects than the ties is as exact: every listed rect is a real rect of the
+// layout.
 struct Cands {
-    const float4 *base;  // the array idx[] points into: the tree's rects or a cell list
-    int idx[kCandMax];   // positions of the near-tied rects in base
+    const float4 *base;  // the tree's rects or the cell lists
+    int idx[kCandMax];   // tree: positions of the near-tied rects in base
     float g[kCandMax];   // their gaps, rounded down (keeping extra entries is harmless)
     int n;
+    int first;
 };
 
 // L-infinity distance from a point (in FP32) to a box, 0 inside.
@@ -83,9 +90,11 @@ __device__ __forceinline__ void scan_rect(const float4 r, int k, const int32_t *
 // any point of the cell (the cell's radius is bounded by the clearance of
 // its centre plus half a side, with a margin far above the rounding of the
 // cell index), so scanning it gives the same d*, the same containing rect and
-// a superset of the same ties as the whole tree.  Otherwise (no cell lists,
-// or an overflowed cell): one depth-first, nearest-child-first traversal.
-// Node boxes and rect gaps are screened in FP32 (errors below L.slack); only
+// a superset of the same ties as the whole tree; a list holds about two
+// rects, so every one gets the exact FP64 gap without an FP32 screen, and
+// the list itself stands for the ties.  Otherwise (no cell lists, or an
+// overflowed cell): one depth-first, nearest-child-first traversal.  Node
+// boxes and rect gaps are screened in FP32 (errors below L.slack); only
 // rects that can matter -- inside the current tie window or containing p --
 // get the exact FP64 gap.  Returns status bits.
 __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, double py, Cands &C,
@@ -95,12 +104,11 @@ __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, dou
     best = fmin(fmin(px - L.bx0, L.bx1 - px), fmin(py - L.by0, L.by1 - py));
     hit = kNoHit;
     C.n = 0;
+    C.first = -1;
     C.base = L.rects;
     // outside the closed bounds no rect can contain p and p+-1 already
     // leaves the bounds: nothing to look up
     if (!(px >= L.bx0 && py >= L.by0 && px <= L.bx1 && py <= L.by1)) return 0;
-    const float pxf = (float)px, pyf = (float)py, slack = L.slack;
-    float limf = (float)(fmax(best, 0.0) + r2) + slack;  // screen: FP32 value > limf => exact > limit
     if (L.cells) {
         int ix = (int)__dmul_rn(__dsub_rn(px, L.gx0), L.ginv);
         int iy = (int)__dmul_rn(__dsub_rn(py, L.gy0), L.ginv);
@@ -109,11 +117,23 @@ __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, dou
         const int2 ce = __ldg(L.cells + (int64_t)iy * L.gnx + ix);
         if (ce.y >= 0) {
             C.base = L.crects;
-            for (int k = ce.x; k < ce.x + ce.y; k++)
-                scan_rect(__ldg(L.crects + k), k, L.cids, px, py, pxf, pyf, r2, slack, limf, best, hit, C, st);
+            C.first = ce.x;
+            C.n = ce.y;
+            for (int k = ce.x; k < ce.x + ce.y; k++) {
+                const float4 r = __ldg(L.crects + k);
+                const double x0 = r.x, y0 = r.y, x1 = r.z, y1 = r.w;
+                const double g = fmax(fmax(x0 - px, px - x1), fmax(y0 - py, py - y1));
+                if (g <= 0.0 && px >= x0 && py >= y0 && px <= x1 && py <= y1) {
+                    const int id = __ldg(L.cids + k);
+                    hit = id < hit ? id : hit;
+                }
+                best = fmin(best, g);
+            }
             return st;
         }
     }
+    const float pxf = (float)px, pyf = (float)py, slack = L.slack;
+    float limf = (float)(fmax(best, 0.0) + r2) + slack;  // screen: FP32 value > limf => exact > limit
     int stk_node[kStackMax];
     float stk_lb[kStackMax];
     int sp = 0;
@@ -181,7 +201,7 @@ __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, dou
 __device__ __forceinline__ bool collides_listed(const DevLayout &L, const Cands &C, const double o[4]) {
     if (!(o[1] >= L.by0 && o[0] >= L.bx0 && o[3] <= L.by1 && o[2] <= L.bx1)) return true;
     for (int q = 0; q < C.n; q++) {
-        const float4 r = __ldg(C.base + C.idx[q]);
+        const float4 r = __ldg(C.base + (C.first >= 0 ? C.first + q : C.idx[q]));
         if ((double)r.z >= o[0] && o[2] >= (double)r.x && (double)r.w >= o[1] && o[3] >= (double)r.y)
             return true;
     }
