@@ -32,14 +32,13 @@ constexpr double kMinDist = (double).095f;  // drawBiggestSquareAtPoint MIN_DIST
 
 // The rects the replay tests for boxes within delta of the clearance: a
 // point answered by a cell list keeps its cell's whole list (first >= 0:
-// base[first .. first + n)), a superset of the near ties; a point answered
-// by the tree keeps the near-tie list idx[0 .. n) (first < 0).  Testing more
-// rects than the ties is as exact: every listed rect is a real rect of the
-// layout.
+// the cell-list entries first .. first + n - 1), a superset of the near
+// ties; a point answered by the tree keeps the near-tie list idx[0 .. n) of
+// tree rects (first < 0).  Testing more rects than the ties is as exact:
+// every listed rect is a real rect of the layout.
 struct Cands {
-    const float4 *base;  // the tree's rects or the cell lists
-    int idx[kCandMax];   // tree: positions of the near-tied rects in base
-    float g[kCandMax];   // their gaps, rounded down (keeping extra entries is harmless)
+    int idx[kCandMax];  // tree: positions of the near-tied rects among the tree's rects
+    float g[kCandMax];  // their gaps, rounded down (keeping extra entries is harmless)
     int n;
     int first;
 };
@@ -97,6 +96,8 @@ __device__ __forceinline__ void scan_rect(const float4 r, int k, const int32_t *
 // boxes and rect gaps are screened in FP32 (errors below L.slack); only
 // rects that can matter -- inside the current tie window or containing p --
 // get the exact FP64 gap.  Returns status bits.
+// kInside: the caller has checked that p lies inside the bounds.
+template <bool kInside = false>
 __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, double py, Cands &C,
                                               int &hit, double &best) {
     uint32_t st = 0;
@@ -105,10 +106,9 @@ __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, dou
     hit = kNoHit;
     C.n = 0;
     C.first = -1;
-    C.base = L.rects;
     // outside the closed bounds no rect can contain p and p+-1 already
     // leaves the bounds: nothing to look up
-    if (!(px >= L.bx0 && py >= L.by0 && px <= L.bx1 && py <= L.by1)) return 0;
+    if (!kInside && !(px >= L.bx0 && py >= L.by0 && px <= L.bx1 && py <= L.by1)) return 0;
     if (L.cells) {
         int ix = (int)__dmul_rn(__dsub_rn(px, L.gx0), L.ginv);
         int iy = (int)__dmul_rn(__dsub_rn(py, L.gy0), L.ginv);
@@ -116,7 +116,6 @@ __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, dou
         iy = iy < 0 ? 0 : (iy >= L.gny ? L.gny - 1 : iy);
         const int2 ce = __ldg(L.cells + (int64_t)iy * L.gnx + ix);
         if (ce.y >= 0) {
-            C.base = L.crects;
             C.first = ce.x;
             C.n = ce.y;
             for (int k = ce.x; k < ce.x + ce.y; k++) {
@@ -201,7 +200,7 @@ __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, dou
 __device__ __forceinline__ bool collides_listed(const DevLayout &L, const Cands &C, const double o[4]) {
     if (!(o[1] >= L.by0 && o[0] >= L.bx0 && o[3] <= L.by1 && o[2] <= L.bx1)) return true;
     for (int q = 0; q < C.n; q++) {
-        const float4 r = __ldg(C.base + (C.first >= 0 ? C.first + q : C.idx[q]));
+        const float4 r = __ldg(C.first >= 0 ? L.crects + C.first + q : L.rects + C.idx[q]);
         if ((double)r.z >= o[0] && o[2] >= (double)r.x && (double)r.w >= o[1] && o[3] >= (double)r.y)
             return true;
     }
@@ -329,11 +328,12 @@ __device__ __forceinline__ uint32_t replay_square(const DevLayout &L, const Cand
 }
 
 // drawBiggestSquareAtPoint + checkCollisons(point) for one point.
+template <bool kInside = false>
 __device__ __forceinline__ uint32_t query_point(const DevLayout &L, double px, double py, double sq[4],
                                                 int &hit) {
     Cands C;
     double best;
-    uint32_t st = clearance(L, px, py, C, hit, best);
+    uint32_t st = clearance<kInside>(L, px, py, C, hit, best);
     st |= replay_square(L, C, px, py, best, sq);
     return st;
 }

@@ -192,7 +192,9 @@ __device__ __forceinline__ void tab_round(const WalkParams &P, Slot *tab, int la
     }
 }
 
-template <bool kMulti>
+// kRec: per-walk records requested (some P.rec_* set); without them the
+// record stores and their tests are compiled out.
+template <bool kMulti, bool kRec>
 __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const WalkParams P) {
     __shared__ double s_intg[FRW_NSAMPLE + 1];
     __shared__ double s_wx[FRW_NSAMPLE], s_wy[FRW_NSAMPLE];
@@ -344,7 +346,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
                 if (P.start_grid) {  // midpoint of arc floor(u*Q) of Q equal arcs
                     const uint32_t q = (uint32_t)__dmul_rn(u, (double)P.start_grid);
                     u = __ddiv_rn(__dadd_rn((double)q, 0.5), (double)P.start_grid);
-                    if (P.rec_q) bin1 = -2 - (int)q;  // the arc rides in bin1 until the first hop
+                    if (kRec && P.rec_q) bin1 = -2 - (int)q;  // the arc rides in bin1 until the first hop
                 }
             }
             if (starting && uniform_start) {
@@ -353,10 +355,11 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
                 const int bin = bin_of(s_intg, s_guide, u);
                 point_from_index(sq, bin, exact, px, py);
                 if (hop == 1) {
-                    if (P.rec_q) P.rec_q[walk_index()] = (-2 - bin1) * FRW_NSAMPLE + bin;
+                    if (kRec && P.rec_q) P.rec_q[walk_index()] = (-2 - bin1) * FRW_NSAMPLE + bin;
                     bin1 = bin;
                     a0 = __dsub_rn(sq[2], sq[0]);
-                    if (P.rec_cv) *reinterpret_cast<double2 *>(&P.rec_cv[walk_index()]) = make_double2(px, py);
+                    if (kRec && P.rec_cv)
+                        *reinterpret_cast<double2 *>(&P.rec_cv[walk_index()]) = make_double2(px, py);
                 }
             }
             starting = false;
@@ -371,7 +374,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
                 code = -1;  // escaped: left the layer bounds
             } else {
                 int hit;
-                st |= query_point(L, px, py, sq, hit);
+                st |= query_point<true>(L, px, py, sq, hit);
                 hops++;
                 if (hit != kNoHit) code = hit;
                 else if (hops >= P.hop_cap) code = -2;
@@ -393,15 +396,17 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
                 c = __ddiv_rn(__dmul_rn(__dmul_rn(-P.permittivity, perim), dot), a0);
             }
             if (code >= 0) wgt = c;
-            const uint64_t gw = walk_index();
-            if (P.rec_end) P.rec_end[gw] = code;
-            if (P.rec_hops) P.rec_hops[gw] = hops;
-            if (P.rec_bin) P.rec_bin[gw] = bin1 < 0 ? -1 : bin1;
-            if (P.rec_w) P.rec_w[gw] = c;
-            if (P.rec_q && bin1 < 0) P.rec_q[gw] = -1;
-            if (P.rec_cv) {  // first-hop point written at hop 1 (zero when there was none)
-                if (bin1 < 0) *reinterpret_cast<double2 *>(&P.rec_cv[gw]) = make_double2(0.0, 0.0);
-                reinterpret_cast<double2 *>(&P.rec_cv[gw])[1] = make_double2(a0, c);
+            if (kRec) {
+                const uint64_t gw = walk_index();
+                if (P.rec_end) P.rec_end[gw] = code;
+                if (P.rec_hops) P.rec_hops[gw] = hops;
+                if (P.rec_bin) P.rec_bin[gw] = bin1 < 0 ? -1 : bin1;
+                if (P.rec_w) P.rec_w[gw] = c;
+                if (P.rec_q && bin1 < 0) P.rec_q[gw] = -1;
+                if (P.rec_cv) {  // first-hop point written at hop 1 (zero when there was none)
+                    if (bin1 < 0) *reinterpret_cast<double2 *>(&P.rec_cv[gw]) = make_double2(0.0, 0.0);
+                    reinterpret_cast<double2 *>(&P.rec_cv[gw])[1] = make_double2(a0, c);
+                }
             }
             active = false;
             s_lhops[threadIdx.x] += (unsigned long long)hops;
@@ -450,8 +455,8 @@ __global__ void k_compact(const unsigned long long *__restrict__ acc_n, const do
 
 int walk_max_blocks_per_sm(int threads, bool multi) {
     int b = 0;
-    if (multi) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<true>, threads, 0);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<false>, threads, 0);
+    if (multi) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<true, false>, threads, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<false, false>, threads, 0);
     return b;
 }
 
@@ -460,8 +465,14 @@ frw_status launch_walk(const WalkParams &P, int threads, int blocks, cudaStream_
         set_error("launch_walk: threads per block must be 256");
         return FRW_E_ARG;
     }
-    if (P.njobs > 1) k_walk<true><<<blocks, threads, 0, stream>>>(P);
-    else k_walk<false><<<blocks, threads, 0, stream>>>(P);
+    const bool rec = P.rec_end || P.rec_hops || P.rec_bin || P.rec_w || P.rec_q || P.rec_cv;
+    if (P.njobs > 1) {
+        if (rec) k_walk<true, true><<<blocks, threads, 0, stream>>>(P);
+        else k_walk<true, false><<<blocks, threads, 0, stream>>>(P);
+    } else {
+        if (rec) k_walk<false, true><<<blocks, threads, 0, stream>>>(P);
+        else k_walk<false, false><<<blocks, threads, 0, stream>>>(P);
+    }
     FRW_CK(cudaGetLastError());
     return FRW_OK;
 }
