@@ -107,6 +107,9 @@ __device__ __forceinline__ int slot_hash(unsigned long long key) {
 // once with DISTINCT keys (so distinct slots): empty slots are claimed with a
 // shared-memory CAS, the rest of the update has a single writer.  False when
 // the warp table is full.
+// kW: weighted walks (uniform start); without weights every weight is 0 and
+// only the counts are kept.
+template <bool kW>
 __device__ __forceinline__ bool tab_insert(Slot *tab, unsigned long long key, unsigned long long n, double s,
                                            double s2) {
     const int h = slot_hash(key);
@@ -117,14 +120,16 @@ __device__ __forceinline__ bool tab_insert(Slot *tab, unsigned long long key, un
             k = atomicCAS(&sl.key, kEmptyKey, key);
             if (k == kEmptyKey) {
                 sl.n = 0;
-                sl.s = sl.cs = sl.s2 = sl.cs2 = 0.0;
+                if (kW) sl.s = sl.cs = sl.s2 = sl.cs2 = 0.0;
                 k = key;
             }
         }
         if (k == key) {
             sl.n += n;
-            kahan_add(sl.s, sl.cs, s);
-            kahan_add(sl.s2, sl.cs2, s2);
+            if (kW) {
+                kahan_add(sl.s, sl.cs, s);
+                kahan_add(sl.s2, sl.cs2, s2);
+            }
             return true;
         }
     }
@@ -137,7 +142,7 @@ __device__ __forceinline__ const WalkJob &job_of(const WalkParams &P, int j) {
 }
 
 // Whole warp: push every used slot to the global rows, then clear.
-template <bool kMulti>
+template <bool kMulti, bool kW>
 __device__ void tab_flush(const WalkParams &P, Slot *tab, int lane) {
     for (int q = lane; q < kTabSlots; q += 32) {
         Slot &sl = tab[q];
@@ -148,8 +153,10 @@ __device__ void tab_flush(const WalkParams &P, Slot *tab, int lane) {
         if (code >= 0) {
             const int64_t row = job_of<kMulti>(P, job).acc_base + code;
             atomicAdd(P.acc_n + row, sl.n);
-            atomicAdd(P.acc_s + row, __dsub_rn(sl.s, sl.cs));
-            atomicAdd(P.acc_s2 + row, __dsub_rn(sl.s2, sl.cs2));
+            if (kW) {
+                atomicAdd(P.acc_s + row, __dsub_rn(sl.s, sl.cs));
+                atomicAdd(P.acc_s2 + row, __dsub_rn(sl.s2, sl.cs2));
+            }
         } else {
             atomicAdd(js + (code == -1 ? 0 : 1), sl.n);
         }
@@ -164,7 +171,7 @@ __device__ void tab_flush(const WalkParams &P, Slot *tab, int lane) {
 // group's lowest lane gathers the group's sums (in lane order) and adds them
 // to the table, all groups in parallel; a full table is flushed and the rest
 // retried.
-template <bool kMulti>
+template <bool kMulti, bool kW>
 __device__ __forceinline__ void tab_round(const WalkParams &P, Slot *tab, int lane, unsigned lt, bool ins,
                                           unsigned long long key, unsigned long long cnt, double s1, double s2) {
     const unsigned em = __ballot_sync(kFull, ins);
@@ -174,27 +181,36 @@ __device__ __forceinline__ void tab_round(const WalkParams &P, Slot *tab, int la
     const unsigned leaders = __ballot_sync(kFull, lead);
     for (unsigned rest = em & ~leaders; rest; rest &= rest - 1) {
         const int l = __ffs(rest) - 1;
-        const double a = __shfl_sync(kFull, s1, l), b = __shfl_sync(kFull, s2, l);
         const unsigned long long kl = __shfl_sync(kFull, key, l), cl = __shfl_sync(kFull, cnt, l);
+        double a = 0.0, b = 0.0;
+        if (kW) {
+            a = __shfl_sync(kFull, s1, l);
+            b = __shfl_sync(kFull, s2, l);
+        }
         if (lead && kl == key) {
-            s1 = __dadd_rn(s1, a);
-            s2 = __dadd_rn(s2, b);
+            if (kW) {
+                s1 = __dadd_rn(s1, a);
+                s2 = __dadd_rn(s2, b);
+            }
             cnt += cl;
         }
     }
     bool pending = lead;
     for (;;) {
-        const bool failed = pending && !tab_insert(tab, key, cnt, s1, s2);
+        const bool failed = pending && !tab_insert<kW>(tab, key, cnt, s1, s2);
         pending = failed;
         __syncwarp();
         if (!__any_sync(kFull, failed)) break;
-        tab_flush<kMulti>(P, tab, lane);  // table full: empty it, retry the rest
+        tab_flush<kMulti, kW>(P, tab, lane);  // table full: empty it, retry the rest
     }
 }
 
 // kRec: per-walk records requested (some P.rec_* set); without them the
-// record stores and their tests are compiled out.
-template <bool kMulti, bool kRec>
+// record stores and their tests are compiled out.  kUniform: uniform start
+// on the Gaussian perimeter, whose walks carry the first-hop weight; with
+// the Green-CDF start every weight is 0, so the weight, its inputs and the
+// weight sums are compiled out.
+template <bool kMulti, bool kRec, bool kUniform>
 __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const WalkParams P) {
     __shared__ double s_intg[FRW_NSAMPLE + 1];
     __shared__ double s_wx[FRW_NSAMPLE], s_wy[FRW_NSAMPLE];
@@ -220,7 +236,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
 
     const uint32_t lt = (1u << lane) - 1u;
     const int refill_min = P.refill_min < 1 ? 1 : (P.refill_min > 32 ? 32 : P.refill_min);
-    const bool uniform_start = P.start_mode == FRW_START_UNIFORM;
+    constexpr bool uniform_start = kUniform;
     const bool exact = P.exact_perimeter != 0;
     const uint64_t seed = P.seed_dev ? *P.seed_dev : P.seed;
     const uint64_t kChunk = P.chunk ? (uint64_t)P.chunk : kChunkDefault;
@@ -313,7 +329,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
             }
             if (kMulti && __any_sync(kFull, job != pjob)) {  // leave the old job's sums behind
                 const bool moved = job != pjob;
-                tab_round<kMulti>(P, tab, lane, lt, moved && pn > 0, target_key(pjob), pn, ps, ps2);
+                tab_round<kMulti, kUniform>(P, tab, lane, lt, moved && pn > 0, target_key(pjob), pn, ps, ps2);
                 if (moved) {
                     const unsigned long long lh = s_lhops[threadIdx.x];
                     if (lh) atomicAdd(P.job_stats + 4 * pjob + 2, lh);
@@ -338,7 +354,8 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
             if ((hop & 3) == 0) rnd = draw_block(seed, stream, pw, hop);
             double u = word_u(rnd, hop);
             if (starting) {
-                perim = __dadd_rn(__dmul_rn(2.0, __dsub_rn(sq[2], sq[0])), __dmul_rn(2.0, __dsub_rn(sq[3], sq[1])));
+                if (kUniform)
+                    perim = __dadd_rn(__dmul_rn(2.0, __dsub_rn(sq[2], sq[0])), __dmul_rn(2.0, __dsub_rn(sq[3], sq[1])));
                 if (P.start_strata) {  // stratum pw mod S of the start distribution
                     const double s = (double)(uint32_t)(pw % P.start_strata);
                     u = __ddiv_rn(__dadd_rn(s, u), (double)P.start_strata);
@@ -357,7 +374,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
                 if (hop == 1) {
                     if (kRec && P.rec_q) P.rec_q[walk_index()] = (-2 - bin1) * FRW_NSAMPLE + bin;
                     bin1 = bin;
-                    a0 = __dsub_rn(sq[2], sq[0]);
+                    if (kUniform || kRec) a0 = __dsub_rn(sq[2], sq[0]);
                     if (kRec && P.rec_cv)
                         *reinterpret_cast<double2 *>(&P.rec_cv[walk_index()]) = make_double2(px, py);
                 }
@@ -412,19 +429,21 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
             s_lhops[threadIdx.x] += (unsigned long long)hops;
             if ((int64_t)code == job_of<kMulti>(P, job).target) {
                 pn++;
-                ps = __dadd_rn(ps, wgt);
-                ps2 = __dadd_rn(ps2, __dmul_rn(wgt, wgt));
+                if (kUniform) {
+                    ps = __dadd_rn(ps, wgt);
+                    ps2 = __dadd_rn(ps2, __dmul_rn(wgt, wgt));
+                }
             } else {
                 ins = true;
                 key = ((unsigned long long)job << 32) | (uint32_t)(code + 2);
             }
         }
-        tab_round<kMulti>(P, tab, lane, lt, ins, key, 1ull, wgt, __dmul_rn(wgt, wgt));
+        tab_round<kMulti, kUniform>(P, tab, lane, lt, ins, key, 1ull, wgt, __dmul_rn(wgt, wgt));
     }
     __syncwarp();
-    tab_round<kMulti>(P, tab, lane, lt, pn > 0, target_key(pjob), pn, ps, ps2);
+    tab_round<kMulti, kUniform>(P, tab, lane, lt, pn > 0, target_key(pjob), pn, ps, ps2);
     if (s_lhops[threadIdx.x]) atomicAdd(P.job_stats + 4 * pjob + 2, s_lhops[threadIdx.x]);
-    tab_flush<kMulti>(P, tab, lane);
+    tab_flush<kMulti, kUniform>(P, tab, lane);
     if (st) atomicOr(P.status, st);
 }
 
@@ -455,8 +474,8 @@ __global__ void k_compact(const unsigned long long *__restrict__ acc_n, const do
 
 int walk_max_blocks_per_sm(int threads, bool multi) {
     int b = 0;
-    if (multi) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<true, false>, threads, 0);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<false, false>, threads, 0);
+    if (multi) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<true, false, true>, threads, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<false, false, true>, threads, 0);
     return b;
 }
 
@@ -466,12 +485,14 @@ frw_status launch_walk(const WalkParams &P, int threads, int blocks, cudaStream_
         return FRW_E_ARG;
     }
     const bool rec = P.rec_end || P.rec_hops || P.rec_bin || P.rec_w || P.rec_q || P.rec_cv;
+    const bool uni = P.start_mode == FRW_START_UNIFORM;
+    const dim3 g(blocks), b(threads);
     if (P.njobs > 1) {
-        if (rec) k_walk<true, true><<<blocks, threads, 0, stream>>>(P);
-        else k_walk<true, false><<<blocks, threads, 0, stream>>>(P);
+        if (rec) uni ? k_walk<true, true, true><<<g, b, 0, stream>>>(P) : k_walk<true, true, false><<<g, b, 0, stream>>>(P);
+        else uni ? k_walk<true, false, true><<<g, b, 0, stream>>>(P) : k_walk<true, false, false><<<g, b, 0, stream>>>(P);
     } else {
-        if (rec) k_walk<false, true><<<blocks, threads, 0, stream>>>(P);
-        else k_walk<false, false><<<blocks, threads, 0, stream>>>(P);
+        if (rec) uni ? k_walk<false, true, true><<<g, b, 0, stream>>>(P) : k_walk<false, true, false><<<g, b, 0, stream>>>(P);
+        else uni ? k_walk<false, false, true><<<g, b, 0, stream>>>(P) : k_walk<false, false, false><<<g, b, 0, stream>>>(P);
     }
     FRW_CK(cudaGetLastError());
     return FRW_OK;
