@@ -225,9 +225,9 @@ __device__ __forceinline__ Window replay_window(const DevLayout &L, double px, d
 
 __device__ __forceinline__ bool collides_box(const DevLayout &L, const Cands &C, const double o[4],
                                              const Window &W) {
-    if (o[2] > W.hi) return true;
-    if (o[2] < W.lo) return false;
-    return collides_listed(L, C, o);
+    bool c = o[2] > W.hi;
+    if (!c && !(o[2] < W.lo)) c = collides_listed(L, C, o);  // rare: within delta of the clearance
+    return c;
 }
 
 // dist / 2 for the replay's step sizes (normal, positive, above MIN_DIST/2):

@@ -141,6 +141,27 @@ __device__ __forceinline__ const WalkJob &job_of(const WalkParams &P, int j) {
     return kMulti ? P.jobs[j] : P.job0;
 }
 
+// Counts only (no weights): one walk end of `key` added to its slot with a
+// shared-memory atomic (slots are claimed by CAS and hold n = 0 while
+// empty), so lanes with equal keys need no grouping.  False when the table
+// is full.
+__device__ __forceinline__ bool tab_count(Slot *tab, unsigned long long key, unsigned long long n) {
+    const int h = slot_hash(key);
+    for (int probe = 0; probe < kTabSlots; probe++) {
+        Slot &sl = tab[(h + probe) & (kTabSlots - 1)];
+        unsigned long long k = *(volatile unsigned long long *)&sl.key;
+        if (k == kEmptyKey) {
+            k = atomicCAS(&sl.key, kEmptyKey, key);
+            if (k == kEmptyKey) k = key;
+        }
+        if (k == key) {
+            atomicAdd(&sl.n, n);
+            return true;
+        }
+    }
+    return false;
+}
+
 // Whole warp: push every used slot to the global rows, then clear.
 template <bool kMulti, bool kW>
 __device__ void tab_flush(const WalkParams &P, Slot *tab, int lane) {
@@ -161,6 +182,7 @@ __device__ void tab_flush(const WalkParams &P, Slot *tab, int lane) {
             atomicAdd(js + (code == -1 ? 0 : 1), sl.n);
         }
         atomicAdd(js + 3, sl.n);
+        sl.n = 0;
         sl.key = kEmptyKey;
     }
     __syncwarp();
@@ -176,6 +198,17 @@ __device__ __forceinline__ void tab_round(const WalkParams &P, Slot *tab, int la
                                           unsigned long long key, unsigned long long cnt, double s1, double s2) {
     const unsigned em = __ballot_sync(kFull, ins);
     if (!em) return;
+    if (!kW) {
+        bool pending = ins;
+        for (;;) {
+            const bool failed = pending && !tab_count(tab, key, cnt);
+            pending = failed;
+            __syncwarp();
+            if (!__any_sync(kFull, failed)) break;
+            tab_flush<kMulti, kW>(P, tab, lane);  // table full: empty it, retry the rest
+        }
+        return;
+    }
     bool lead = false;
     if (ins) lead = (__match_any_sync(em, key) & lt) == 0;
     const unsigned leaders = __ballot_sync(kFull, lead);
@@ -226,7 +259,10 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
         s_wy[i] = P.wy[i];
     }
     Slot *tab = s_tab[wib];
-    for (int q = lane; q < kTabSlots; q += 32) tab[q].key = kEmptyKey;
+    for (int q = lane; q < kTabSlots; q += 32) {
+        tab[q].key = kEmptyKey;
+        tab[q].n = 0;
+    }
     if (lane == 0) s_chunk[wib][0] = s_chunk[wib][1] = 0;
     s_lhops[threadIdx.x] = 0;
     __syncthreads();
@@ -241,11 +277,13 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
     const uint64_t seed = P.seed_dev ? *P.seed_dev : P.seed;
     const uint64_t kChunk = P.chunk ? (uint64_t)P.chunk : kChunkDefault;
 
-    bool active = false, exhausted = false, starting = false;
+    bool active = false, exhausted = false;
     int job = 0;
     uint64_t pw = 0;
-    uint32_t hop = 0, stream = 0;  // hop: the Philox word of the lane's next point
-    uint4 rnd = make_uint4(0, 0, 0, 0);  // uniforms of words (hop & ~3) .. +3
+    uint32_t stream = 0;
+    uint4 rnd = make_uint4(0, 0, 0, 0);  // uniforms of Philox words (hops & ~3) .. +3
+    // queries so far of the lane's walk, also the Philox word of its next
+    // point (word 0 places the start, word h the point after query h)
     int32_t hops = 0, bin1 = -1;
     int side = 0;
     double a0 = 0, perim = 0;
@@ -319,11 +357,9 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
                     sq[3] = g4.w;
                     pw = J.first_walk + (gw - J.walk_begin);
                     stream = J.stream_id;
-                    hop = 0;
                     hops = 0;
                     bin1 = -1;
                     a0 = 0.0;
-                    starting = true;
                     active = true;
                 }
             }
@@ -347,10 +383,12 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
 
         // ---- the point of every active walk: its start point on the Gaussian
         // surface (word 0), or the next hop's point on its last square (word
-        // `hop`); starts and hops share the Philox draw, the bin search and the
-        // perimeter mapping, so a warp runs each once per iteration ----
+        // `hops`); starts and hops share the Philox draw, the bin search and
+        // the perimeter mapping, so a warp runs each once per iteration ----
         double px = 0, py = 0;
         if (active) {
+            const uint32_t hop = (uint32_t)hops;
+            const bool starting = hops == 0;
             if ((hop & 3) == 0) rnd = draw_block(seed, stream, pw, hop);
             double u = word_u(rnd, hop);
             if (starting) {
@@ -379,7 +417,6 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
                         *reinterpret_cast<double2 *>(&P.rec_cv[walk_index()]) = make_double2(px, py);
                 }
             }
-            starting = false;
         }
 
         // ---- one query of every active walk ----
@@ -395,7 +432,6 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const Wal
                 hops++;
                 if (hit != kNoHit) code = hit;
                 else if (hops >= P.hop_cap) code = -2;
-                else hop++;  // the next point, on the square just found, uses word `hop`
             }
         }
         const bool ended = active && code != 0x7FFFFFFF;

@@ -273,6 +273,26 @@ def test_walk_argument_errors_and_empty_runs():
         assert r.walks == 0 and len(r.conductor) == 0
 
 
+@pytest.mark.parametrize("mode", ["reference", "capacitance", "capacitance-grid"])
+def test_walks_with_and_without_records_agree(mode):
+    """The walk kernel is compiled per launch configuration (per-walk records
+    or none, start mode): the same walks traced with records and run without
+    them give the same ends, hop totals and weight sums."""
+    o = {"reference": frw.opts(), "capacitance": frw.capacitance_opts(1.0),
+         "capacitance-grid": frw.capacitance_opts(1.0, start_grid=512)}[mode]
+    n = 200_000
+    with frw.Layout.from_rects(config1_layout()) as L:
+        r = L.walk(0, n, seed=77, o=o, capacity=4096)
+        end, hops, _, w = L.walk_trace(0, 0, n, 77, o)
+    cond, cnt = np.unique(end[end >= 0], return_counts=True)
+    assert np.array_equal(cond, r.conductor) and np.array_equal(cnt, r.hits)
+    assert hops.sum() == r.hops_total and (end == -1).sum() == r.escaped and (end == -2).sum() == r.aborted
+    sw = np.array([w[end == k].sum() for k in cond])
+    np.testing.assert_allclose(r.sum_w, sw, rtol=1e-12, atol=1e-12 * max(np.abs(sw).max(), 1e-300))
+    if mode == "reference":  # the Green-CDF start carries no weight
+        assert not np.any(w) and not np.any(r.sum_w)
+
+
 def test_walk_device_rows_match_frw_walk():
     """frw_walk_device accumulates the same rows into device arrays without a
     host sync: two runs over disjoint walk ranges equal one frw_walk run over
