@@ -90,8 +90,9 @@ WalkParams params_for(const frw_batch *B, const WalkJob *jobs, const WalkJob &jo
 }
 
 int grid_for(const frw_batch *B, const frw_tuning &t, uint64_t total) {
-    int bps = t.blocks_per_sm > 0 ? t.blocks_per_sm : walk_max_blocks_per_sm(256, true);
-    bps = std::max(1, std::min(bps, walk_max_blocks_per_sm(256, true)));
+    const int maxb = walk_max_blocks_per_sm(256, B->njobs > 1, B->opts.start_mode == FRW_START_UNIFORM);
+    int bps = t.blocks_per_sm > 0 ? t.blocks_per_sm : maxb;
+    bps = std::max(1, std::min(bps, maxb));
     uint64_t blocks = (uint64_t)B->sms * bps, need = (total + 255) / 256;
     return (int)std::max<uint64_t>(1, std::min(blocks, need));
 }
@@ -299,7 +300,8 @@ frw_status frw_batch_tune(frw_batch *B, uint64_t trial_walks, frw_tuning *chosen
         return FRW_E_CUDA;
     }
     cudaEvent_t k0 = ev[0], k1 = ev[1];
-    const int maxb = std::max(1, walk_max_blocks_per_sm(256, true));
+    const int maxb =
+        std::max(1, walk_max_blocks_per_sm(256, B->njobs > 1, B->opts.start_mode == FRW_START_UNIFORM));
     const int refills[] = {1, 4, 16};
     const int chunks[] = {32, 128, 512};
     frw_tuning best = B->tuning;

@@ -72,6 +72,22 @@ struct Grid {
     int nx, ny;
 };
 
+// The count pass visits the cells in tiles of 8 x 4, one tile per warp, so
+// that a warp's tree traversals start from neighbouring points and take
+// similar paths: thread t gets cell (tile_x * 8 + t % 8, tile_y * 4 + t % 32
+// / 8) of tile t / 32, or -1 past the grid's edge.
+constexpr int kTileW = 8, kTileH = 4;
+__device__ __forceinline__ int64_t tiled_cell(const Grid &G, int64_t t) {
+    const int64_t tile = t >> 5;
+    const int lane = (int)(t & 31);
+    const int64_t tiles_x = (G.nx + kTileW - 1) / kTileW;
+    const int64_t ix = (tile % tiles_x) * kTileW + (lane % kTileW), iy = (tile / tiles_x) * kTileH + lane / kTileW;
+    return ix < G.nx && iy < G.ny ? iy * G.nx + ix : -1;
+}
+int64_t tiled_threads(int64_t nx, int64_t ny) {
+    return ((nx + kTileW - 1) / kTileW) * ((ny + kTileH - 1) / kTileH) * 32;
+}
+
 // The box of cell c grown by r.
 __device__ __forceinline__ void grown_box(const Grid &G, int64_t c, double r, double B[4]) {
     const int ix = (int)(c % G.nx), iy = (int)(c / G.nx);
@@ -99,9 +115,11 @@ __device__ __forceinline__ double cell_radius(const DevLayout &L, const Grid &G,
 // rects, for the fill pass.
 __global__ void k_cell_count(DevLayout L, Grid G, int cap, int64_t *__restrict__ cnt, int2 *__restrict__ cells,
                              float *__restrict__ crad, double *__restrict__ rad, int32_t *__restrict__ stage,
-                             unsigned long long *overflow, int64_t ncells) {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= ncells) return;
+                             unsigned long long *overflow, int64_t nthreads) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nthreads) return;
+    const int64_t c = tiled_cell(G, t);
+    if (c < 0) return;
     const double r = cell_radius(L, G, c);
     double B[4];
     grown_box(G, c, r, B);
@@ -306,7 +324,9 @@ frw_status build_cells(const DevLayout &Lin, double cells_per_rect, int cap, cud
         if (!ck(cudaMallocAsync(&ovf, 8, st), "malloc overflow count")) break;
         if (!ck(cudaMemsetAsync(ovf, 0, 8, st), "memset")) break;
         const unsigned blocks = (unsigned)((ncells + 127) / 128);
-        k_cell_count<<<blocks, 128, 0, st>>>(L, G, cap, cnt, C.cells, C.crad, rad, stage, ovf, ncells);
+        const int64_t nt = tiled_threads(nx, ny);
+        k_cell_count<<<(unsigned)((nt + 127) / 128), 128, 0, st>>>(L, G, cap, cnt, C.cells, C.crad, rad, stage, ovf,
+                                                                  nt);
         k_tile_sums<<<(unsigned)tiles, kScanThreads, 0, st>>>(cnt, ncells, sums);
         k_scan_sums<<<1, kScanThreads, 0, st>>>(sums, tiles, grand);
         k_tile_scan<<<(unsigned)tiles, kScanThreads, 0, st>>>(cnt, ncells, sums, start);

@@ -117,7 +117,7 @@ struct DeviceCtx {
     int sms = 0;
     int cc_major = 0, cc_minor = 0;
     double *tables = nullptr;  // intg[201] | wx[200] | wy[200]
-    int walk_bps = 0;          // resident walk blocks per SM (occupancy query, cached)
+    int walk_bps[2] = {0, 0};  // resident walk blocks per SM by uniform start (occupancy query, cached)
 };
 std::mutex g_mu;
 std::map<int, DeviceCtx> g_ctx;
@@ -184,7 +184,7 @@ frw_status poll_event(cudaEvent_t ev, const char *what) {
         return e == cudaSuccess ? FRW_OK : cuda_fail(e, what);
     }
     const auto t0 = std::chrono::steady_clock::now();
-    for (int k = 0;; k++) {
+    for (;;) {
         cudaError_t e = cudaEventQuery(ev);
         if (e == cudaSuccess) return FRW_OK;
         if (e != cudaErrorNotReady) return cuda_fail(e, what);
@@ -195,8 +195,11 @@ frw_status poll_event(cudaEvent_t ev, const char *what) {
                       "released in stream order)");
             return FRW_E_TIMEOUT;
         }
-        if (k < 64) std::this_thread::yield();
-        else std::this_thread::sleep_for(std::chrono::microseconds(k < 1024 ? 20 : 200));
+        // short device steps (a layout build waits on several of tens of us)
+        // are polled without sleeping, whose wake-up can take far longer than
+        // the step on a loaded host; long waits sleep between polls
+        if (ms < 2.0) std::this_thread::yield();
+        else std::this_thread::sleep_for(std::chrono::microseconds(ms < 50.0 ? 20 : 200));
     }
 }
 
@@ -358,8 +361,9 @@ frw_status run_walks(const frw_layout *lay, int64_t target, uint64_t first_walk,
     P.wx = ctx->tables + FRW_NSAMPLE + 1;
     P.wy = ctx->tables + 2 * FRW_NSAMPLE + 1;
     const int threads = 256;
-    if (!ctx->walk_bps) ctx->walk_bps = walk_max_blocks_per_sm(threads, false);
-    int bps = o.blocks_per_sm > 0 ? o.blocks_per_sm : ctx->walk_bps;
+    const int uni = o.start_mode == FRW_START_UNIFORM;
+    if (!ctx->walk_bps[uni]) ctx->walk_bps[uni] = walk_max_blocks_per_sm(threads, false, uni);
+    int bps = o.blocks_per_sm > 0 ? o.blocks_per_sm : ctx->walk_bps[uni];
     if (bps < 1) bps = 1;
     int blocks = ctx->sms * bps;
     const uint64_t need = (walks + threads - 1) / threads;
@@ -450,7 +454,30 @@ frw_status wait_stream(cudaStream_t st, const char *what) {
     return rc;
 }
 
-frw_status read_back(void *host, const void *dev, size_t bytes, cudaStream_t st, const char *what) {
+frw_status read_back(void *host, const void *dev, size_t bytes, cudaStream_t st, const char *what, bool staged) {
+    // small reads (sizes, counts, status words) go through a pinned buffer of
+    // the calling thread: one copy behind the stream's work and one bounded
+    // wait; a copy whose wait gave up may still land, so its buffer is left
+    // to it
+    constexpr size_t kStage = 4096;
+    static thread_local void *stage = nullptr;
+    if (staged && bytes <= kStage) {
+        if (!stage && cudaMallocHost(&stage, kStage) != cudaSuccess) {
+            stage = nullptr;
+            cudaGetLastError();
+        }
+        if (stage) {
+            cudaError_t e = cudaMemcpyAsync(stage, dev, bytes, cudaMemcpyDeviceToHost, st);
+            if (e != cudaSuccess) return cuda_fail(e, what);
+            frw_status rc = wait_stream(st, what);
+            if (rc) {
+                stage = nullptr;
+                return rc;
+            }
+            memcpy(host, stage, bytes);
+            return FRW_OK;
+        }
+    }
     frw_status rc = wait_stream(st, what);
     if (rc) return rc;
     cudaError_t e = cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, st);
@@ -1028,8 +1055,9 @@ frw_status frw_walk_device(const frw_layout *L, int64_t target, uint64_t walks, 
     P.intg = ctx->tables;
     P.wx = ctx->tables + FRW_NSAMPLE + 1;
     P.wy = ctx->tables + 2 * FRW_NSAMPLE + 1;
-    if (!ctx->walk_bps) ctx->walk_bps = walk_max_blocks_per_sm(256, false);
-    int bps = o.blocks_per_sm > 0 ? o.blocks_per_sm : std::max(ctx->walk_bps, 1);
+    const int uni = o.start_mode == FRW_START_UNIFORM;
+    if (!ctx->walk_bps[uni]) ctx->walk_bps[uni] = walk_max_blocks_per_sm(256, false, uni);
+    int bps = o.blocks_per_sm > 0 ? o.blocks_per_sm : std::max(ctx->walk_bps[uni], 1);
     int blocks = ctx->sms * bps;
     const uint64_t need = (walks + 255) / 256;
     if ((uint64_t)blocks > need) blocks = (int)std::max<uint64_t>(need, 1);

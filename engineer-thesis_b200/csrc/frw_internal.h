@@ -136,8 +136,12 @@ struct WaitScope {
 frw_status wait_stream(cudaStream_t st, const char *what);
 // Waits for a recorded event.
 frw_status wait_event(cudaEvent_t e, const char *what);
-// Bounded wait for `st`, then a synchronous copy of a small device result.
-frw_status read_back(void *host, const void *dev, size_t bytes, cudaStream_t st, const char *what);
+// A small device result after everything enqueued on `st` so far, with a
+// bounded wait.  staged: through a pinned buffer of the calling thread (made
+// on its first use), one copy queued behind the work and one wait; else a
+// wait, then a synchronous copy (no allocation).
+frw_status read_back(void *host, const void *dev, size_t bytes, cudaStream_t st, const char *what,
+                     bool staged = true);
 
 // CUDA events destroyed at scope exit, error paths included.
 struct Events {
@@ -232,7 +236,8 @@ frw_status launch_gauss_jobs(const WalkJob *d_jobs, const double *d_targets, int
 
 // walk.cu
 frw_status launch_walk(const WalkParams &P, int threads, int blocks, cudaStream_t stream);
-int walk_max_blocks_per_sm(int threads, bool multi);
+// Resident k_walk blocks per SM for one job or many, uniform start or not.
+int walk_max_blocks_per_sm(int threads, bool multi, bool uniform);
 // Compacts the nonzero accumulator rows (at most cap of them written; cap < 0:
 // rows): their count, written or not, goes to *d_count.
 frw_status launch_compact(const unsigned long long *acc_n, const double *acc_s, const double *acc_s2,

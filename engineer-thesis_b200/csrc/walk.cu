@@ -29,7 +29,11 @@ namespace frw {
 namespace {
 
 constexpr int kWalkThreads = 256;
-constexpr int kWalkMinBlocks = 4;  // 64 registers per thread: 4 blocks (32 warps) per SM
+// Resident blocks per SM: weighted walks (uniform start) keep more state, so
+// they run at 64 registers per thread (4 blocks of 256, 32 warps); walks
+// without weights fit 48 registers and run 5 blocks (40 warps).
+constexpr int kWalkMinBlocksW = 4;
+constexpr int kWalkMinBlocks = 5;
 constexpr int kWarpsPerBlock = kWalkThreads / 32;
 constexpr int kTabSlots = 32;  // per warp
 constexpr unsigned long long kEmptyKey = ~0ull;
@@ -244,7 +248,7 @@ __device__ __forceinline__ void tab_round(const WalkParams &P, Slot *tab, int la
 // the Green-CDF start every weight is 0, so the weight, its inputs and the
 // weight sums are compiled out.
 template <bool kMulti, bool kRec, bool kUniform>
-__global__ void __launch_bounds__(kWalkThreads, kWalkMinBlocks) k_walk(const WalkParams P) {
+__global__ void __launch_bounds__(kWalkThreads, kUniform ? kWalkMinBlocksW : kWalkMinBlocks) k_walk(const WalkParams P) {
     __shared__ double s_intg[FRW_NSAMPLE + 1];
     __shared__ double s_wx[FRW_NSAMPLE], s_wy[FRW_NSAMPLE];
     __shared__ Slot s_tab[kWarpsPerBlock][kTabSlots];
@@ -508,10 +512,15 @@ __global__ void k_compact(const unsigned long long *__restrict__ acc_n, const do
 
 }  // namespace
 
-int walk_max_blocks_per_sm(int threads, bool multi) {
+int walk_max_blocks_per_sm(int threads, bool multi, bool uniform) {
     int b = 0;
-    if (multi) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<true, false, true>, threads, 0);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<false, false, true>, threads, 0);
+    if (multi) {
+        if (uniform) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<true, false, true>, threads, 0);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<true, false, false>, threads, 0);
+    } else {
+        if (uniform) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<false, false, true>, threads, 0);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<false, false, false>, threads, 0);
+    }
     return b;
 }
 

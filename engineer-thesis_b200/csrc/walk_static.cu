@@ -132,7 +132,8 @@ extern "C" frw_status frw_walk_trace_static(const frw_layout *layout, int64_t ta
         P.intg = tables;
         P.wx = tables + FRW_NSAMPLE + 1;
         P.wy = tables + 2 * FRW_NSAMPLE + 1;
-        int bps = o.blocks_per_sm > 0 ? o.blocks_per_sm : walk_max_blocks_per_sm(256, false);
+        int bps = o.blocks_per_sm > 0 ? o.blocks_per_sm
+                                      : walk_max_blocks_per_sm(256, false, o.start_mode == FRW_START_UNIFORM);
         if (bps < 1) bps = 1;
         uint64_t blocks = (uint64_t)sms * bps, need = (walks + 255) / 256;
         if (blocks > need) blocks = need;
@@ -144,8 +145,8 @@ extern "C" frw_status frw_walk_trace_static(const frw_layout *layout, int64_t ta
         WaitScope ws(o.timeout_ms);
         uint32_t h_status = 0;
         unsigned long long h_stats[4] = {0, 0, 0, 0};
-        rc = read_back(&h_status, status, 4, st, "frw_walk_trace_static");
-        if (!rc) rc = read_back(h_stats, stats, 32, st, "frw_walk_trace_static");
+        rc = read_back(&h_status, status, 4, st, "frw_walk_trace_static", false);
+        if (!rc) rc = read_back(h_stats, stats, 32, st, "frw_walk_trace_static", false);
         if (!rc && h_status) {
             set_error("frw_walk_trace_static: kernel reported an internal limit");
             rc = FRW_E_KERNEL;
