@@ -12,7 +12,9 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "cv.cuh"
@@ -32,6 +34,8 @@ struct frw_cv {
 
 namespace frw {
 namespace {
+
+std::atomic<int> g_cv_walk_mode{FRW_CV_WALK_FUSED};
 
 struct Buf {
     std::vector<void *> p;
@@ -95,6 +99,59 @@ frw_status check_cv_walk_opts(const frw_opts &o) {
         set_error("control variate: needs FRW_START_UNIFORM, start_grid a power of two <= 2^23 and hop_cap >= 2");
         return FRW_E_ARG;
     }
+    return FRW_OK;
+}
+
+// frw_cv_walk with the control variate's sums kept by the walk kernel: one
+// launch into dense rows; the estimates come from the target's row (plain:
+// sums of c over walks ending on the target) and the kernel's sums of z.
+frw_status cv_walk_fused(const frw_cv *M, uint64_t walks, uint64_t seed, frw_cv_result *res, cudaStream_t st) {
+    const int64_t n = M->view.n;
+    Buf B(st);
+    unsigned long long *d_hits, *d_stats;
+    double *d_s1, *d_s2, *d_pack;  // pack: sum z, sum z^2, sum w, sum w^2, status word
+    uint32_t *d_status;
+    cudaError_t e = B.get(&d_hits, (size_t)n * 8);
+    if (e == cudaSuccess) e = B.get(&d_s1, (size_t)n * 8);
+    if (e == cudaSuccess) e = B.get(&d_s2, (size_t)n * 8);
+    if (e == cudaSuccess) e = B.get(&d_stats, 32);
+    if (e == cudaSuccess) e = B.get(&d_pack, 48);
+    if (e == cudaSuccess) e = B.get(&d_status, 4);
+    if (e != cudaSuccess) return cuda_fail(e, "frw_cv_walk: allocation");
+    for (auto z : {std::make_pair((void *)d_hits, (size_t)n * 8), std::make_pair((void *)d_s1, (size_t)n * 8),
+                   std::make_pair((void *)d_s2, (size_t)n * 8), std::make_pair((void *)d_stats, (size_t)32),
+                   std::make_pair((void *)d_pack, (size_t)48), std::make_pair((void *)d_status, (size_t)4)})
+        if ((e = cudaMemsetAsync(z.first, 0, z.second, st)) != cudaSuccess) return cuda_fail(e, "frw_cv_walk: clear");
+    Events ev(2);
+    if (!ev.ok(2)) return cuda_fail(cudaErrorUnknown, "frw_cv_walk: cudaEventCreate");
+    frw_opts o = M->opts;
+    o.first_walk = 0;
+    cudaEventRecord(ev[0], st);
+    frw_status rc = walk_device_rows(M->layout, M->target, walks, seed, o, reinterpret_cast<uint64_t *>(d_hits), d_s1,
+                                     d_s2, reinterpret_cast<uint64_t *>(d_stats), d_status, M->phi, d_pack, st);
+    cudaEventRecord(ev[1], st);
+    if (rc) return rc;
+    e = cudaMemcpyAsync(d_pack + 2, d_s1 + M->target, 8, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_pack + 3, d_s2 + M->target, 8, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_pack + 4, d_status, 4, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return cuda_fail(e, "frw_cv_walk: gather");
+    double h[5] = {0, 0, 0, 0, 0};
+    if ((rc = read_back(h, d_pack, 40, st, "frw_cv_walk"))) return rc;
+    uint32_t status_word;
+    memcpy(&status_word, &h[4], 4);
+    if (status_word) return status_word_error(status_word);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev[0], ev[1]);
+    const double N = (double)walks;
+    const double mz = h[0] / N, vz = std::max(h[1] / N - mz * mz, 0.0) * N / (N - 1);
+    const double mw = h[2] / N, vw = std::max(h[3] / N - mw * mw, 0.0) * N / (N - 1);
+    res->walks = walks;
+    res->plain = mw;
+    res->plain_se = sqrt(vw / N);
+    res->cv = mz + M->mean_term;
+    res->cv_se = sqrt(vz / N);
+    res->variance_ratio = vz > 0 ? vw / vz : 0.0;
+    res->kernel_ms = ms;
     return FRW_OK;
 }
 
@@ -325,6 +382,17 @@ frw_status frw_cv_info_get(const frw_cv *M, frw_cv_info *info) {
     return FRW_OK;
 }
 
+frw_status frw_cv_set_walk_mode(int mode) {
+    if (mode != FRW_CV_WALK_FUSED && mode != FRW_CV_WALK_RECORDS) {
+        set_error("frw_cv_set_walk_mode: FRW_CV_WALK_FUSED or FRW_CV_WALK_RECORDS");
+        return FRW_E_ARG;
+    }
+    g_cv_walk_mode.store(mode, std::memory_order_relaxed);
+    return FRW_OK;
+}
+
+int frw_cv_get_walk_mode(void) { return g_cv_walk_mode.load(std::memory_order_relaxed); }
+
 frw_status frw_cv_walk(const frw_cv *M, uint64_t walks, uint64_t seed, frw_cv_result *res, void *stream) {
     if (!M || !res || walks < 2) {
         set_error("frw_cv_walk: bad arguments");
@@ -333,6 +401,7 @@ frw_status frw_cv_walk(const frw_cv *M, uint64_t walks, uint64_t seed, frw_cv_re
     SetDevice sd(M->view.device);
     WaitScope ws(M->opts.timeout_ms);
     cudaStream_t st = (cudaStream_t)stream;
+    if (g_cv_walk_mode.load(std::memory_order_relaxed) == FRW_CV_WALK_FUSED) return cv_walk_fused(M, walks, seed, res, st);
     const uint64_t chunk = std::min<uint64_t>(walks, 1ull << 23);
     Buf B(st);
     int64_t *d_end;

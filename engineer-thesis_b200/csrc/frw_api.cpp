@@ -1008,6 +1008,18 @@ frw_status frw_walk_device(const frw_layout *L, int64_t target, uint64_t walks, 
         set_error("frw_walk_device: null argument");
         return FRW_E_ARG;
     }
+    return walk_device_rows(L, target, walks, seed, o, hits, sum_w, sum_w2, stats, status, nullptr, nullptr,
+                            (cudaStream_t)stream);
+}
+
+}  // extern "C"
+
+// The walks of frw_walk_device into device rows, optionally with the control
+// variate's sums; no host wait.
+frw_status frw::walk_device_rows(const frw_layout *L, int64_t target, uint64_t walks, uint64_t seed,
+                                 const frw_opts &o, uint64_t *hits, double *sum_w, double *sum_w2, uint64_t *stats,
+                                 uint32_t *status, const float *cv_phi, double *cv_sums, cudaStream_t st) {
+    frw_status rc = FRW_OK;
     if (target < 0 || target >= L->n) {
         set_error("target conductor index out of range");
         return FRW_E_ARG;
@@ -1016,7 +1028,6 @@ frw_status frw_walk_device(const frw_layout *L, int64_t target, uint64_t walks, 
     DeviceCtx *ctx;
     rc = device_ctx(L->device, &ctx);
     if (rc) return rc;
-    cudaStream_t st = (cudaStream_t)stream;
     Scratch S(st);
     char *blk;
     FRW_CK(S.get(&blk, 64 + 32));  // counter, then the target rect (32 B) and its Gaussian surface
@@ -1055,6 +1066,8 @@ frw_status frw_walk_device(const frw_layout *L, int64_t target, uint64_t walks, 
     P.intg = ctx->tables;
     P.wx = ctx->tables + FRW_NSAMPLE + 1;
     P.wy = ctx->tables + 2 * FRW_NSAMPLE + 1;
+    P.cv_phi = cv_phi;
+    P.cv_sums = cv_sums;
     const int uni = o.start_mode == FRW_START_UNIFORM;
     if (!ctx->walk_bps[uni]) ctx->walk_bps[uni] = walk_max_blocks_per_sm(256, false, uni);
     int bps = o.blocks_per_sm > 0 ? o.blocks_per_sm : std::max(ctx->walk_bps[uni], 1);
@@ -1063,6 +1076,8 @@ frw_status frw_walk_device(const frw_layout *L, int64_t target, uint64_t walks, 
     if ((uint64_t)blocks > need) blocks = (int)std::max<uint64_t>(need, 1);
     return launch_walk(P, 256, blocks, st);
 }
+
+extern "C" {
 
 frw_status frw_rows_compact(const frw_layout *L, const uint64_t *hits, const double *sum_w, const double *sum_w2,
                             int64_t capacity, int64_t *idx, uint64_t *out_hits, double *out_sum_w, double *out_sum_w2,

@@ -106,6 +106,11 @@ struct WalkParams {
     double *rec_w;
     int32_t *rec_q;   // optional: first-hop cell q * 200 + bin of the grid start (-1: no first hop)
     double4 *rec_cv;  // optional: (first-hop point x, y, first square side a0, weight factor c)
+    // optional control variate (single job, uniform grid start, no records):
+    // phi per (grid arc q, first-hop bin) at q * 200 + bin, and the sums of
+    // z = c (y - phi) and z^2 over all walks (y = 1 on the target), added here
+    const float *cv_phi;
+    double *cv_sums;
     // tables
     const double *intg;  // [201]
     const double *wx;    // [200]
@@ -262,5 +267,11 @@ frw_status check_opts(const frw_opts *opts);
 frw_status walk_records(const frw_layout *layout, int64_t target, uint64_t first_walk, uint64_t walks,
                         uint64_t seed, const frw_opts &o, cudaStream_t st, int64_t *rec_end, double4 *rec_cv,
                         double *rec_w = nullptr, int32_t *rec_q = nullptr);
+// The walks of frw_walk_device into device rows (hits, sum_w, sum_w2 per
+// conductor; stats; status), optionally with the control variate's sums
+// (cv_phi / cv_sums of WalkParams); no host wait.
+frw_status walk_device_rows(const frw_layout *layout, int64_t target, uint64_t walks, uint64_t seed,
+                            const frw_opts &o, uint64_t *hits, double *sum_w, double *sum_w2, uint64_t *stats,
+                            uint32_t *status, const float *cv_phi, double *cv_sums, cudaStream_t st);
 
 }  // namespace frw

@@ -246,8 +246,9 @@ __device__ __forceinline__ void tab_round(const WalkParams &P, Slot *tab, int la
 // record stores and their tests are compiled out.  kUniform: uniform start
 // on the Gaussian perimeter, whose walks carry the first-hop weight; with
 // the Green-CDF start every weight is 0, so the weight, its inputs and the
-// weight sums are compiled out.
-template <bool kMulti, bool kRec, bool kUniform>
+// weight sums are compiled out.  kCV: the control variate's sums (P.cv_phi,
+// P.cv_sums) are kept beside the rows.
+template <bool kMulti, bool kRec, bool kUniform, bool kCV = false>
 __global__ void __launch_bounds__(kWalkThreads, kUniform ? kWalkMinBlocksW : kWalkMinBlocks) k_walk(const WalkParams P) {
     __shared__ double s_intg[FRW_NSAMPLE + 1];
     __shared__ double s_wx[FRW_NSAMPLE], s_wy[FRW_NSAMPLE];
@@ -255,6 +256,7 @@ __global__ void __launch_bounds__(kWalkThreads, kUniform ? kWalkMinBlocksW : kWa
     __shared__ uint8_t s_guide[kGuide];
     __shared__ unsigned long long s_chunk[kWarpsPerBlock][2];  // per warp: unclaimed part of its walk chunk
     __shared__ unsigned long long s_lhops[kWalkThreads];       // per lane: hops of its walks (current job)
+    __shared__ double s_cvz[kCV ? 2 : 1][kCV ? kWalkThreads : 1];  // per lane: sums of z and z^2
 
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     for (int i = threadIdx.x; i <= FRW_NSAMPLE; i += blockDim.x) s_intg[i] = P.intg[i];
@@ -269,6 +271,7 @@ __global__ void __launch_bounds__(kWalkThreads, kUniform ? kWalkMinBlocksW : kWa
     }
     if (lane == 0) s_chunk[wib][0] = s_chunk[wib][1] = 0;
     s_lhops[threadIdx.x] = 0;
+    if (kCV) s_cvz[0][threadIdx.x] = s_cvz[1][threadIdx.x] = 0.0;
     __syncthreads();
     for (int k = threadIdx.x; k < kGuide; k += blockDim.x)
         s_guide[k] = (uint8_t)bin_search(s_intg, (double)k * (1.0 / kGuide));
@@ -289,6 +292,7 @@ __global__ void __launch_bounds__(kWalkThreads, kUniform ? kWalkMinBlocksW : kWa
     // queries so far of the lane's walk, also the Philox word of its next
     // point (word 0 places the start, word h the point after query h)
     int32_t hops = 0, bin1 = -1;
+    int32_t cvq = -1;  // control variate: the walk's (grid arc, first-hop bin) cell, -1 before its first hop
     int side = 0;
     double a0 = 0, perim = 0;
     // The rect the lane's next point is mapped on: the Gaussian surface of a
@@ -363,6 +367,7 @@ __global__ void __launch_bounds__(kWalkThreads, kUniform ? kWalkMinBlocksW : kWa
                     stream = J.stream_id;
                     hops = 0;
                     bin1 = -1;
+                    if (kCV) cvq = -1;
                     a0 = 0.0;
                     active = true;
                 }
@@ -405,7 +410,7 @@ __global__ void __launch_bounds__(kWalkThreads, kUniform ? kWalkMinBlocksW : kWa
                 if (P.start_grid) {  // midpoint of arc floor(u*Q) of Q equal arcs
                     const uint32_t q = (uint32_t)__dmul_rn(u, (double)P.start_grid);
                     u = __ddiv_rn(__dadd_rn((double)q, 0.5), (double)P.start_grid);
-                    if (kRec && P.rec_q) bin1 = -2 - (int)q;  // the arc rides in bin1 until the first hop
+                    if ((kRec && P.rec_q) || kCV) bin1 = -2 - (int)q;  // the arc rides in bin1 until the first hop
                 }
             }
             if (starting && uniform_start) {
@@ -415,6 +420,7 @@ __global__ void __launch_bounds__(kWalkThreads, kUniform ? kWalkMinBlocksW : kWa
                 point_from_index(sq, bin, exact, px, py);
                 if (hop == 1) {
                     if (kRec && P.rec_q) P.rec_q[walk_index()] = (-2 - bin1) * FRW_NSAMPLE + bin;
+                    if (kCV) cvq = (-2 - bin1) * FRW_NSAMPLE + bin;
                     bin1 = bin;
                     if (kUniform || kRec) a0 = __dsub_rn(sq[2], sq[0]);
                     if (kRec && P.rec_cv)
@@ -467,6 +473,13 @@ __global__ void __launch_bounds__(kWalkThreads, kUniform ? kWalkMinBlocksW : kWa
             }
             active = false;
             s_lhops[threadIdx.x] += (unsigned long long)hops;
+            if (kCV) {  // z = c (y - phi(q, first bin)), as the records-based gather computes it
+                const double yv = (int64_t)code == job_of<kMulti>(P, job).target ? 1.0 : 0.0;
+                const double f = cvq >= 0 ? (double)__ldg(P.cv_phi + cvq) : 0.0;
+                const double z = __dmul_rn(c, __dsub_rn(yv, f));
+                s_cvz[0][threadIdx.x] = __dadd_rn(s_cvz[0][threadIdx.x], z);
+                s_cvz[1][threadIdx.x] = __dadd_rn(s_cvz[1][threadIdx.x], __dmul_rn(z, z));
+            }
             if ((int64_t)code == job_of<kMulti>(P, job).target) {
                 pn++;
                 if (kUniform) {
@@ -484,6 +497,18 @@ __global__ void __launch_bounds__(kWalkThreads, kUniform ? kWalkMinBlocksW : kWa
     tab_round<kMulti, kUniform>(P, tab, lane, lt, pn > 0, target_key(pjob), pn, ps, ps2);
     if (s_lhops[threadIdx.x]) atomicAdd(P.job_stats + 4 * pjob + 2, s_lhops[threadIdx.x]);
     tab_flush<kMulti, kUniform>(P, tab, lane);
+    if (kCV) {
+        double z1 = s_cvz[0][threadIdx.x], z2 = s_cvz[1][threadIdx.x];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            z1 = __dadd_rn(z1, __shfl_xor_sync(kFull, z1, o));
+            z2 = __dadd_rn(z2, __shfl_xor_sync(kFull, z2, o));
+        }
+        if (lane == 0) {
+            atomicAdd(P.cv_sums, z1);
+            atomicAdd(P.cv_sums + 1, z2);
+        }
+    }
     if (st) atomicOr(P.status, st);
 }
 
@@ -532,6 +557,15 @@ frw_status launch_walk(const WalkParams &P, int threads, int blocks, cudaStream_
     const bool rec = P.rec_end || P.rec_hops || P.rec_bin || P.rec_w || P.rec_q || P.rec_cv;
     const bool uni = P.start_mode == FRW_START_UNIFORM;
     const dim3 g(blocks), b(threads);
+    if (P.cv_phi || P.cv_sums) {
+        if (!P.cv_phi || !P.cv_sums || P.njobs != 1 || rec || !uni || P.start_grid == 0) {
+            set_error("launch_walk: the control variate needs one job, no records and the uniform grid start");
+            return FRW_E_ARG;
+        }
+        k_walk<false, false, true, true><<<g, b, 0, stream>>>(P);
+        FRW_CK(cudaGetLastError());
+        return FRW_OK;
+    }
     if (P.njobs > 1) {
         if (rec) uni ? k_walk<true, true, true><<<g, b, 0, stream>>>(P) : k_walk<true, true, false><<<g, b, 0, stream>>>(P);
         else uni ? k_walk<true, false, true><<<g, b, 0, stream>>>(P) : k_walk<true, false, false><<<g, b, 0, stream>>>(P);

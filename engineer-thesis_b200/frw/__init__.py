@@ -235,6 +235,8 @@ _SIGS = {
     "frw_set_wait_limit": ([C.c_double], C.c_int),
     "frw_mlp_set_kernels": ([C.c_int], C.c_int),
     "frw_mlp_get_kernels": ([], C.c_int),
+    "frw_cv_set_walk_mode": ([C.c_int], C.c_int),
+    "frw_cv_get_walk_mode": ([], C.c_int),
     "frw_get_wait_limit": ([], C.c_double),
     "frw_parse_layout": ([C.c_char_p, C.c_int, _D, C.c_int64, _I64, _D, _I32], C.c_int),
     "frw_layout_create": ([_F, C.c_int64, _D, C.c_int, _VP, C.POINTER(_VP)], C.c_int),
@@ -339,6 +341,19 @@ def set_mlp_kernels(which: int) -> None:
 
 def mlp_kernels() -> int:
     return int(lib().frw_mlp_get_kernels())
+
+
+CV_WALK_FUSED, CV_WALK_RECORDS = 0, 1
+
+
+def set_cv_walk_mode(mode: int) -> None:
+    """CV_WALK_FUSED (phi looked up and z summed inside the walk kernel, the
+    default) or CV_WALK_RECORDS (per-walk records, then a summing kernel)."""
+    _check(lib().frw_cv_set_walk_mode(int(mode)))
+
+
+def cv_walk_mode() -> int:
+    return int(lib().frw_cv_get_walk_mode())
 
 
 def set_wait_limit(ms: float) -> None:

@@ -378,6 +378,15 @@ frw_status frw_cv_train(const frw_layout *layout, int64_t target, const frw_opts
 frw_status frw_cv_info_get(const frw_cv *cv, frw_cv_info *info);
 frw_status frw_cv_walk(const frw_cv *cv, uint64_t walks, uint64_t seed, frw_cv_result *result,
                        void *stream);
+/* How frw_cv_walk runs its walks (process-wide): FRW_CV_WALK_FUSED, the
+ * default -- one walk launch that looks phi up at every walk's end and keeps
+ * the sums of z = c (y - phi) beside the rows -- or FRW_CV_WALK_RECORDS,
+ * per-walk records in chunks of 2^23 walks summed by a second kernel.  Both
+ * give the same estimates up to the order of the FP64 sums. */
+#define FRW_CV_WALK_FUSED 0
+#define FRW_CV_WALK_RECORDS 1
+frw_status frw_cv_set_walk_mode(int mode);
+int frw_cv_get_walk_mode(void);
 frw_status frw_cv_destroy(frw_cv *cv);
 #define FRW_CV_PARAMS 5313 /* W1[64][16] b1[64] W2[64][64] b2[64] w3[64] b3 */
 frw_status frw_cv_params(const frw_cv *cv, float *out);

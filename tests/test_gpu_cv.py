@@ -123,6 +123,28 @@ def test_cv_unbiased_and_reduces_variance():
     assert info.quad_points == 4096 * 200 and info.train_loss > 0
 
 
+def test_cv_walk_fused_equals_records_path():
+    """The walk kernel's own control-variate sums give the estimates of the
+    per-walk records summed by a second kernel (same walks, sums in another
+    order)."""
+    o = frw.capacitance_opts(1.0, start_grid=1024)
+    with frw.Layout.from_rects(config1()) as L:
+        cv = frw.ControlVariate(L, 0, o, frw.cv_opts(train_walks=200_000))
+        assert frw.cv_walk_mode() == frw.CV_WALK_FUSED
+        a = cv.walk(3_000_000, seed=5)
+        try:
+            frw.set_cv_walk_mode(frw.CV_WALK_RECORDS)
+            b = cv.walk(3_000_000, seed=5)
+        finally:
+            frw.set_cv_walk_mode(frw.CV_WALK_FUSED)
+        cv.close()
+    for k in ("plain", "plain_se", "cv", "cv_se", "variance_ratio"):
+        assert getattr(a, k) == pytest.approx(getattr(b, k), rel=1e-10), k
+    assert a.walks == b.walks == 3_000_000
+    with pytest.raises(frw.FrwError):
+        frw.set_cv_walk_mode(7)
+
+
 def test_cv_mean_term_is_the_mean_of_f():
     """Unbiasedness of the re-added term: over many walks, mean(f) = E[f]."""
     rects = config1()
