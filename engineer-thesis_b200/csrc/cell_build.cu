@@ -14,8 +14,11 @@
 // clearance query at each cell centre and one box enumeration per cell (the
 // count pass), a scan, then the fill pass, which copies the rects the count
 // pass staged (the first kStage of each cell) and enumerates again only the
-// longer cells, from the radius the count pass kept.  Cells with more than
-// max_per_cell rects keep count -1 and their points use the tree.
+// longer cells, from the radius the count pass kept.  Large grids first
+// build coarse cells (4 x 4 cells each) that way and then answer each cell's
+// clearance and enumeration from its coarse cell's list instead of the tree.
+// Cells with more than max_per_cell rects keep count -1 and their points use
+// the tree.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -98,29 +101,56 @@ __device__ __forceinline__ void grown_box(const Grid &G, int64_t c, double r, do
     B[3] = (y0 + G.side) + r;
 }
 
-// The radius r_C of cell c: the tree's clearance at the cell centre.
-__device__ __forceinline__ double cell_radius(const DevLayout &L, const Grid &G, int64_t c) {
+// The radius r_C of cell c (plus `extra`) from the clearance at the cell
+// centre: the tree's, or, when L carries coarse cell lists, the coarse
+// list's (the same value: the list holds every rect the query can need).
+__device__ __forceinline__ double cell_radius(const DevLayout &L, const Grid &G, int64_t c, double extra) {
     const int ix = (int)(c % G.nx), iy = (int)(c / G.nx);
     const double x0 = G.gx0 + ix * G.side, y0 = G.gy0 + iy * G.side;
     Cands C;
     int hit;
     double best;
-    clearance(L, x0 + 0.5 * G.side, y0 + 0.5 * G.side, C, hit, best);  // L has no cells: the tree
-    return fmax(best, 0.0) + 0.5 * G.side + 2.0 * L.delta + G.margin;
+    clearance(L, x0 + 0.5 * G.side, y0 + 0.5 * G.side, C, hit, best);
+    return fmax(best, 0.0) + 0.5 * G.side + 2.0 * L.delta + G.margin + extra;
+}
+
+// Where cell c's rects come from: the entries of the coarse cell (of
+// factor x factor cells) that covers it, when L carries coarse lists and that
+// coarse cell did not overflow; else (count -1) the tree.
+__device__ __forceinline__ int2 coarse_range(const DevLayout &L, const Grid &G, int factor, int64_t c) {
+    if (!L.cells) return make_int2(0, -1);
+    const int ix = (int)(c % G.nx), iy = (int)(c / G.nx);
+    return __ldg(L.cells + (int64_t)(iy / factor) * L.gnx + ix / factor);
+}
+
+// Visits the rects touching B, from the coarse entries ce (positions into
+// L.crects) or from the tree (Morton positions) when ce.y < 0.  A fine
+// cell's grown box lies inside its coarse cell's grown box (the coarse radius
+// carries an extra margin over the Lipschitz bound r_fine <= r_coarse), so
+// the coarse list holds every rect touching it.
+template <typename F>
+__device__ __forceinline__ bool touching_from(const DevLayout &L, int2 ce, const double B[4], F &&visit) {
+    if (ce.y < 0) return touching(L, B, visit);
+    for (int k = ce.x; k < ce.x + ce.y; k++) {
+        const float4 r = __ldg(L.crects + k);
+        if ((double)r.z >= B[0] && B[2] >= (double)r.x && (double)r.w >= B[1] && B[3] >= (double)r.y)
+            if (!visit(k, r)) return true;
+    }
+    return true;
 }
 
 // Per cell: its list length, or -1 (in cells[c].y) when it exceeds cap or
 // the enumeration was incomplete; cnt[c] = entries to reserve; rad[c] its
-// radius and stage[kStage c ..] the (Morton) indices of its first kStage
+// radius and stage[kStage c ..] the source positions of its first kStage
 // rects, for the fill pass.
-__global__ void k_cell_count(DevLayout L, Grid G, int cap, int64_t *__restrict__ cnt, int2 *__restrict__ cells,
-                             float *__restrict__ crad, double *__restrict__ rad, int32_t *__restrict__ stage,
-                             unsigned long long *overflow, int64_t nthreads) {
+__global__ void k_cell_count(DevLayout L, Grid G, int factor, double extra, int cap, int64_t *__restrict__ cnt,
+                             int2 *__restrict__ cells, float *__restrict__ crad, double *__restrict__ rad,
+                             int32_t *__restrict__ stage, unsigned long long *overflow, int64_t nthreads) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nthreads) return;
     const int64_t c = tiled_cell(G, t);
     if (c < 0) return;
-    const double r = cell_radius(L, G, c);
+    const double r = cell_radius(L, G, c, extra);
     double B[4];
     grown_box(G, c, r, B);
     rad[c] = r;
@@ -129,7 +159,7 @@ __global__ void k_cell_count(DevLayout L, Grid G, int cap, int64_t *__restrict__
     crad[c] = __double2float_rd(r - G.margin);
     int n = 0;
     int32_t *sg = stage + kStage * c;
-    const bool complete = touching(L, B, [&](int k, float4) {
+    const bool complete = touching_from(L, coarse_range(L, G, factor, c), B, [&](int k, float4) {
         if (n < kStage) sg[n] = k;
         return ++n <= cap;
     });
@@ -140,30 +170,35 @@ __global__ void k_cell_count(DevLayout L, Grid G, int cap, int64_t *__restrict__
 }
 
 // Writes the lists of the cells that did not overflow: the staged rects, or
-// for longer lists the enumeration of the same grown box again (its order is
-// deterministic, so it meets the same rects as the count).
-__global__ void k_cell_fill(DevLayout L, Grid G, const int64_t *__restrict__ start, const double *__restrict__ rad,
-                            const int32_t *__restrict__ stage, int2 *__restrict__ cells, float4 *__restrict__ crects,
-                            int32_t *__restrict__ cids, int64_t ncells) {
+// for longer lists the enumeration of the same grown box from the same source
+// again (its order is deterministic, so it meets the same rects as the
+// count).
+__global__ void k_cell_fill(DevLayout L, Grid G, int factor, const int64_t *__restrict__ start,
+                            const double *__restrict__ rad, const int32_t *__restrict__ stage,
+                            int2 *__restrict__ cells, float4 *__restrict__ crects, int32_t *__restrict__ cids,
+                            int64_t ncells) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncells) return;
     const int m = cells[c].y;
     if (m < 0) return;
     const int64_t s = start[c];
+    const int2 ce = coarse_range(L, G, factor, c);
+    const float4 *src = ce.y < 0 ? L.rects : L.crects;
+    const int32_t *sid = ce.y < 0 ? L.ids : L.cids;
     if (m <= kStage) {
         for (int i = 0; i < m; i++) {
             const int k = stage[kStage * c + i];
-            crects[s + i] = __ldg(L.rects + k);
-            cids[s + i] = __ldg(L.ids + k);
+            crects[s + i] = __ldg(src + k);
+            cids[s + i] = __ldg(sid + k);
         }
     } else {
         double B[4];
         grown_box(G, c, rad[c], B);
         int n = 0;
-        touching(L, B, [&](int k, float4 r) {
+        touching_from(L, ce, B, [&](int k, float4 r) {
             if (n >= m) return false;
             crects[s + n] = r;
-            cids[s + n] = __ldg(L.ids + k);
+            cids[s + n] = __ldg(sid + k);
             return ++n < m;
         });
     }
@@ -262,6 +297,82 @@ void attach_cells(DevLayout &L, const CellBuffers &c) {
     L.gny = c.ny;
 }
 
+namespace {
+
+// Coarse cells, of kCoarse x kCoarse cells each, serve the fine build on
+// grids of at least kTwoLevelMin cells: their lists (from the tree, up to
+// kCoarseCap rects) answer the fine cells' clearance and enumeration, so the
+// tree is traversed once per coarse cell instead of once per cell.
+constexpr int kCoarse = 4;
+constexpr int64_t kTwoLevelMin = 1 << 16;
+constexpr int kCoarseCap = 64;
+
+// Count -> scan -> fill of the cells of grid G over L (with coarse lists of
+// factor `factor` attached, or the tree alone); the cell buffers in C.
+frw_status build_grid(const DevLayout &L, const Grid &G, int factor, double extra, int cap, cudaStream_t st,
+                      CellBuffers &C) {
+    const int64_t ncells = (int64_t)G.nx * G.ny;
+    C.ncells = ncells;
+    C.nx = G.nx;
+    C.ny = G.ny;
+    C.gx0 = G.gx0;
+    C.gy0 = G.gy0;
+    C.side = G.side;
+    C.ginv = 1.0 / G.side;
+    int64_t *cnt = nullptr, *start = nullptr, *sums = nullptr, *grand = nullptr;
+    double *rad = nullptr;
+    int32_t *stage = nullptr;
+    unsigned long long *ovf = nullptr;
+    const int64_t tiles = (ncells + kScanTile - 1) / kScanTile;
+    frw_status rc = FRW_OK;
+    auto ck = [&](cudaError_t e, const char *what) {
+        if (e != cudaSuccess && rc == FRW_OK) rc = cuda_fail(e, what);
+        return rc == FRW_OK;
+    };
+    do {
+        if (!ck(cudaMallocAsync(&C.cells, (size_t)ncells * sizeof(int2), st), "malloc cells")) break;
+        if (!ck(cudaMallocAsync(&C.crad, (size_t)ncells * sizeof(float), st), "malloc cell radii")) break;
+        if (!ck(cudaMallocAsync(&cnt, (size_t)ncells * 8, st), "malloc cell counts")) break;
+        if (!ck(cudaMallocAsync(&start, (size_t)ncells * 8, st), "malloc cell starts")) break;
+        if (!ck(cudaMallocAsync(&rad, (size_t)ncells * 8, st), "malloc cell radii (build)")) break;
+        if (!ck(cudaMallocAsync(&stage, (size_t)ncells * kStage * 4, st), "malloc staged rects")) break;
+        if (!ck(cudaMallocAsync(&sums, (size_t)tiles * 8, st), "malloc tile sums")) break;
+        if (!ck(cudaMallocAsync(&grand, 8, st), "malloc total")) break;
+        if (!ck(cudaMallocAsync(&ovf, 8, st), "malloc overflow count")) break;
+        if (!ck(cudaMemsetAsync(ovf, 0, 8, st), "memset")) break;
+        const unsigned blocks = (unsigned)((ncells + 127) / 128);
+        const int64_t nt = tiled_threads(G.nx, G.ny);
+        k_cell_count<<<(unsigned)((nt + 127) / 128), 128, 0, st>>>(L, G, factor, extra, cap, cnt, C.cells, C.crad,
+                                                                  rad, stage, ovf, nt);
+        k_tile_sums<<<(unsigned)tiles, kScanThreads, 0, st>>>(cnt, ncells, sums);
+        k_scan_sums<<<1, kScanThreads, 0, st>>>(sums, tiles, grand);
+        k_tile_scan<<<(unsigned)tiles, kScanThreads, 0, st>>>(cnt, ncells, sums, start);
+        if (!ck(cudaGetLastError(), "cell count")) break;
+        unsigned long long h[2] = {0, 0};  // list total, overflowed cells
+        if ((rc = read_back(&h[0], grand, 8, st, "build_cells: list total"))) break;
+        if ((rc = read_back(&h[1], ovf, 8, st, "build_cells: overflow count"))) break;
+        const int64_t total = (int64_t)h[0];
+        if (total > INT32_MAX) {
+            set_error("build_cells: more than 2^31 list entries; use fewer cells per rect");
+            rc = FRW_E_ARG;
+            break;
+        }
+        C.entries = total;
+        C.overflow = (int64_t)h[1];
+        if (!ck(cudaMallocAsync(&C.crects, (size_t)std::max<int64_t>(total, 1) * 16, st), "malloc cell rects")) break;
+        if (!ck(cudaMallocAsync(&C.cids, (size_t)std::max<int64_t>(total, 1) * 4, st), "malloc cell ids")) break;
+        if (total > 0)
+            k_cell_fill<<<blocks, 128, 0, st>>>(L, G, factor, start, rad, stage, C.cells, C.crects, C.cids, ncells);
+        if (!ck(cudaGetLastError(), "cell fill")) break;
+    } while (0);
+    for (void *p : {(void *)cnt, (void *)start, (void *)sums, (void *)grand, (void *)ovf, (void *)rad, (void *)stage})
+        if (p) cudaFreeAsync(p, st);
+    C.bytes = ncells * (int64_t)(sizeof(int2) + sizeof(float)) + C.entries * 20;
+    return rc;
+}
+
+}  // namespace
+
 frw_status build_cells(const DevLayout &Lin, double cells_per_rect, int cap, cudaStream_t st, CellBuffers *out) {
     *out = CellBuffers();
     if (!(cells_per_rect > 0) || cap < 1 || cap > (1 << 16)) {
@@ -269,7 +380,7 @@ frw_status build_cells(const DevLayout &Lin, double cells_per_rect, int cap, cud
         return FRW_E_ARG;
     }
     DevLayout L = Lin;
-    L.cells = nullptr;  // the build queries the tree
+    L.cells = nullptr;  // the build queries the tree (and coarse lists of its own)
     const double W = L.bx1 - L.bx0, H = L.by1 - L.by0;
     const double target = std::min((double)kMaxCells, std::max(1.0, cells_per_rect * (double)L.n));
     double side = std::sqrt(std::max(W * H, 1e-300) / target);
@@ -288,77 +399,45 @@ frw_status build_cells(const DevLayout &Lin, double cells_per_rect, int cap, cud
                                              std::max(std::fabs(L.bx1), std::fabs(L.by1))),
                                     std::max(W, H)) +
                      16.0;
-    Grid G{L.bx0, L.by0, side, std::ldexp(M, -30), (int)nx, (int)ny};
+    const double margin = std::ldexp(M, -30);
+    const Grid G{L.bx0, L.by0, side, margin, (int)nx, (int)ny};
 
     cudaEvent_t e0, e1;
     FRW_CK(cudaEventCreate(&e0));
     FRW_CK(cudaEventCreate(&e1));
-    CellBuffers C;
-    C.ncells = ncells;
-    C.nx = (int)nx;
-    C.ny = (int)ny;
-    C.gx0 = G.gx0;
-    C.gy0 = G.gy0;
-    C.side = side;
-    C.ginv = 1.0 / side;
-    int64_t *cnt = nullptr, *start = nullptr, *sums = nullptr, *grand = nullptr;
-    double *rad = nullptr;
-    int32_t *stage = nullptr;
-    unsigned long long *ovf = nullptr;
-    const int64_t tiles = (ncells + kScanTile - 1) / kScanTile;
+    CellBuffers C, K;  // the cells; coarse cells serving their build
     frw_status rc = FRW_OK;
-    auto ck = [&](cudaError_t e, const char *what) {
-        if (e != cudaSuccess && rc == FRW_OK) rc = cuda_fail(e, what);
-        return rc == FRW_OK;
-    };
     do {
-        if (!ck(cudaEventRecord(e0, st), "event")) break;
-        if (!ck(cudaMallocAsync(&C.cells, (size_t)ncells * sizeof(int2), st), "malloc cells")) break;
-        if (!ck(cudaMallocAsync(&C.crad, (size_t)ncells * sizeof(float), st), "malloc cell radii")) break;
-        if (!ck(cudaMallocAsync(&cnt, (size_t)ncells * 8, st), "malloc cell counts")) break;
-        if (!ck(cudaMallocAsync(&start, (size_t)ncells * 8, st), "malloc cell starts")) break;
-        if (!ck(cudaMallocAsync(&rad, (size_t)ncells * 8, st), "malloc cell radii (build)")) break;
-        if (!ck(cudaMallocAsync(&stage, (size_t)ncells * kStage * 4, st), "malloc staged rects")) break;
-        if (!ck(cudaMallocAsync(&sums, (size_t)tiles * 8, st), "malloc tile sums")) break;
-        if (!ck(cudaMallocAsync(&grand, 8, st), "malloc total")) break;
-        if (!ck(cudaMallocAsync(&ovf, 8, st), "malloc overflow count")) break;
-        if (!ck(cudaMemsetAsync(ovf, 0, 8, st), "memset")) break;
-        const unsigned blocks = (unsigned)((ncells + 127) / 128);
-        const int64_t nt = tiled_threads(nx, ny);
-        k_cell_count<<<(unsigned)((nt + 127) / 128), 128, 0, st>>>(L, G, cap, cnt, C.cells, C.crad, rad, stage, ovf,
-                                                                  nt);
-        k_tile_sums<<<(unsigned)tiles, kScanThreads, 0, st>>>(cnt, ncells, sums);
-        k_scan_sums<<<1, kScanThreads, 0, st>>>(sums, tiles, grand);
-        k_tile_scan<<<(unsigned)tiles, kScanThreads, 0, st>>>(cnt, ncells, sums, start);
-        if (!ck(cudaGetLastError(), "cell count")) break;
-        int64_t total = 0;
-        unsigned long long novf = 0;
-        if ((rc = read_back(&total, grand, 8, st, "build_cells: list total"))) break;
-        if ((rc = read_back(&novf, ovf, 8, st, "build_cells: overflow count"))) break;
-        if (total > INT32_MAX) {
-            set_error("build_cells: more than 2^31 list entries; use fewer cells per rect");
-            rc = FRW_E_ARG;
+        if (cudaEventRecord(e0, st) != cudaSuccess) {
+            rc = cuda_fail(cudaGetLastError(), "event");
             break;
         }
-        C.entries = total;
-        C.overflow = (int64_t)novf;
-        if (!ck(cudaMallocAsync(&C.crects, (size_t)std::max<int64_t>(total, 1) * 16, st), "malloc cell rects")) break;
-        if (!ck(cudaMallocAsync(&C.cids, (size_t)std::max<int64_t>(total, 1) * 4, st), "malloc cell ids")) break;
-        if (total > 0) k_cell_fill<<<blocks, 128, 0, st>>>(L, G, start, rad, stage, C.cells, C.crects, C.cids, ncells);
-        if (!ck(cudaGetLastError(), "cell fill")) break;
-        if (!ck(cudaEventRecord(e1, st), "event")) break;
+        if (ncells >= kTwoLevelMin) {
+            // coarse radius one margin above the Lipschitz bound r_cell <= r_coarse
+            const Grid Gk{L.bx0, L.by0, side * kCoarse, margin, (int)((nx + kCoarse - 1) / kCoarse),
+                          (int)((ny + kCoarse - 1) / kCoarse)};
+            if ((rc = build_grid(L, Gk, 1, margin, kCoarseCap, st, K))) break;
+            DevLayout Lk = L;
+            attach_cells(Lk, K);
+            rc = build_grid(Lk, G, kCoarse, 0.0, cap, st, C);
+        } else {
+            rc = build_grid(L, G, 1, 0.0, cap, st, C);
+        }
+        if (rc) break;
+        if (cudaEventRecord(e1, st) != cudaSuccess) {
+            rc = cuda_fail(cudaGetLastError(), "event");
+            break;
+        }
         if ((rc = wait_event(e1, "build_cells"))) break;
         cudaEventElapsedTime(&C.build_ms, e0, e1);
     } while (0);
-    for (void *p : {(void *)cnt, (void *)start, (void *)sums, (void *)grand, (void *)ovf, (void *)rad, (void *)stage})
-        if (p) cudaFreeAsync(p, st);
+    free_cells(&K, st);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc != FRW_OK) {
         free_cells(&C, st);
         return rc;
     }
-    C.bytes = ncells * (int64_t)(sizeof(int2) + sizeof(float)) + C.entries * 20;
     *out = C;
     return FRW_OK;
 }
