@@ -92,6 +92,21 @@ def test_bad_layout_arguments_rejected_before_device():
     with pytest.raises(frw.FrwError) as e:
         frw.Layout.from_file("/nonexistent/layout")
     assert e.value.status == frw.E_IO
+    import ctypes as C
+
+    one = np.array([[0, 0, 5, 5]], dtype=np.float32)
+    h = C.c_void_p()
+    ptr = one.ctypes.data_as(C.POINTER(C.c_float))
+    # empty layout; more than 2^26 - 1 rects (refused before the rects are read)
+    assert frw.lib().frw_layout_create(ptr, 0, None, 0, None, C.byref(h)) == frw.E_ARG
+    assert frw.lib().frw_layout_create(ptr, 1 << 26, None, 0, None, C.byref(h)) == frw.E_ARG
+    assert "2^26" in frw.lib().frw_last_error().decode()
+    # bounds that are not a box
+    bad = np.array([10.0, 0.0, 0.0, 10.0])
+    assert frw.lib().frw_layout_create(ptr, 1, bad.ctypes.data_as(C.POINTER(C.c_double)), 0, None,
+                                       C.byref(h)) == frw.E_ARG
+    assert "bounds invalid" in frw.lib().frw_last_error().decode()
+    assert not h.value
 
 
 @pytest.mark.parametrize("seed,n,domain", [(0xF4A7 + 1, 100, 1000.0), (0xF4A7 + 2, 10_000, 1e4),
