@@ -84,67 +84,28 @@ __device__ __forceinline__ void scan_rect(const float4 r, int k, const int32_t *
     }
 }
 
-// The clearance of p and its near-tie list.  With cell lists the list of
-// p's cell holds every rect that can come within 2*delta of the clearance of
-// any point of the cell (the cell's radius is bounded by the clearance of
-// its centre plus half a side, with a margin far above the rounding of the
-// cell index), so scanning it gives the same d*, the same containing rect and
-// a superset of the same ties as the whole tree; a list holds about two
-// rects, so every one gets the exact FP64 gap without an FP32 screen, and
-// the list itself stands for the ties.  Otherwise (no cell lists, or an
-// overflowed cell): one depth-first, nearest-child-first traversal.  Node
-// boxes and rect gaps are screened in FP32 (errors below L.slack); only
-// rects that can matter -- inside the current tie window or containing p --
-// get the exact FP64 gap.  Returns status bits.
-// kInside: the caller has checked that p lies inside the bounds.
-template <bool kInside = false>
-__device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, double py, Cands &C,
-                                              int &hit, double &best) {
+// The tree part of clearance (no cell lists, or an overflowed cell): one
+// depth-first, nearest-child-first traversal from the bounds distance in
+// `best`; FP32 screens (errors below slack), the exact FP64 gap only for
+// rects that can matter.
+__device__ __forceinline__ uint32_t tree_clearance(const float4 *nbox, const int4 *nref, const float4 *rects,
+                                                   const int32_t *ids, double px, double py, double r2, float slack,
+                                                   Cands &C, int &hit, double &best) {
     uint32_t st = 0;
-    const double r2 = 2.0 * L.delta;
-    best = fmin(fmin(px - L.bx0, L.bx1 - px), fmin(py - L.by0, L.by1 - py));
-    hit = kNoHit;
-    C.n = 0;
-    C.first = -1;
-    // outside the closed bounds no rect can contain p and p+-1 already
-    // leaves the bounds: nothing to look up
-    if (!kInside && !(px >= L.bx0 && py >= L.by0 && px <= L.bx1 && py <= L.by1)) return 0;
-    if (L.cells) {
-        int ix = (int)__dmul_rn(__dsub_rn(px, L.gx0), L.ginv);
-        int iy = (int)__dmul_rn(__dsub_rn(py, L.gy0), L.ginv);
-        ix = ix < 0 ? 0 : (ix >= L.gnx ? L.gnx - 1 : ix);
-        iy = iy < 0 ? 0 : (iy >= L.gny ? L.gny - 1 : iy);
-        const int2 ce = __ldg(L.cells + (int64_t)iy * L.gnx + ix);
-        if (ce.y >= 0) {
-            C.first = ce.x;
-            C.n = ce.y;
-            for (int k = ce.x; k < ce.x + ce.y; k++) {
-                const float4 r = __ldg(L.crects + k);
-                const double x0 = r.x, y0 = r.y, x1 = r.z, y1 = r.w;
-                const double g = fmax(fmax(x0 - px, px - x1), fmax(y0 - py, py - y1));
-                if (g <= 0.0 && px >= x0 && py >= y0 && px <= x1 && py <= y1) {
-                    const int id = __ldg(L.cids + k);
-                    hit = id < hit ? id : hit;
-                }
-                best = fmin(best, g);
-            }
-            return st;
-        }
-    }
-    const float pxf = (float)px, pyf = (float)py, slack = L.slack;
+    const float pxf = (float)px, pyf = (float)py;
     float limf = (float)(fmax(best, 0.0) + r2) + slack;  // screen: FP32 value > limf => exact > limit
     int stk_node[kStackMax];
     float stk_lb[kStackMax];
     int sp = 0;
     int nd = 0;  // node being visited; the nearest qualifying child is visited next directly
     for (;;) {
-        const float4 *bp = L.nbox + 4 * nd;
+        const float4 *bp = nbox + 4 * nd;
         float4 b[4];
         b[0] = __ldg(bp);
         b[1] = __ldg(bp + 1);
         b[2] = __ldg(bp + 2);
         b[3] = __ldg(bp + 3);
-        const int4 rf = __ldg(L.nref + nd);
+        const int4 rf = __ldg(nref + nd);
         const int ref[4] = {rf.x, rf.y, rf.z, rf.w};
         float lb[4];
 #pragma unroll
@@ -155,7 +116,7 @@ __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, dou
             if (ref[c] >= kRefEmpty || lb[c] > limf) continue;
             const int f = leaf_first(ref[c]), m = leaf_count(ref[c]);
             for (int k = f; k < f + m; k++)
-                scan_rect(__ldg(L.rects + k), k, L.ids, px, py, pxf, pyf, r2, slack, limf, best, hit, C, st);
+                scan_rect(__ldg(rects + k), k, ids, px, py, pxf, pyf, r2, slack, limf, best, hit, C, st);
         }
         // internal children within reach: visit the nearest next, stack the rest
         int next = -1;
@@ -191,6 +152,67 @@ __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, dou
         nd = stk_node[--sp];
     }
     return st;
+}
+
+// The same, out of line (a call: smaller code where the tree is rare).
+static __device__ __noinline__ uint32_t tree_clearance_call(const float4 *nbox, const int4 *nref,
+                                                            const float4 *rects, const int32_t *ids, double px,
+                                                            double py, double r2, float slack, Cands &C, int &hit,
+                                                            double &best) {
+    return tree_clearance(nbox, nref, rects, ids, px, py, r2, slack, C, hit, best);
+}
+
+// The clearance of p and its near-tie list.  With cell lists the list of
+// p's cell holds every rect that can come within 2*delta of the clearance of
+// any point of the cell (the cell's radius is bounded by the clearance of
+// its centre plus half a side, with a margin far above the rounding of the
+// cell index), so scanning it gives the same d*, the same containing rect and
+// a superset of the same ties as the whole tree; a list holds about two
+// rects, so every one gets the exact FP64 gap without an FP32 screen, and
+// the list itself stands for the ties.  Otherwise (no cell lists, or an
+// overflowed cell): one depth-first, nearest-child-first traversal.  Node
+// boxes and rect gaps are screened in FP32 (errors below L.slack); only
+// rects that can matter -- inside the current tie window or containing p --
+// get the exact FP64 gap.  Returns status bits.
+// kInside: the caller has checked that p lies inside the bounds.
+// kOutOfLineTree: the tree traversal is a call (smaller code at the caller).
+template <bool kInside = false, bool kOutOfLineTree = false>
+__device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, double py, Cands &C,
+                                              int &hit, double &best) {
+    uint32_t st = 0;
+    const double r2 = 2.0 * L.delta;
+    best = fmin(fmin(px - L.bx0, L.bx1 - px), fmin(py - L.by0, L.by1 - py));
+    hit = kNoHit;
+    C.n = 0;
+    C.first = -1;
+    // outside the closed bounds no rect can contain p and p+-1 already
+    // leaves the bounds: nothing to look up
+    if (!kInside && !(px >= L.bx0 && py >= L.by0 && px <= L.bx1 && py <= L.by1)) return 0;
+    if (L.cells) {
+        int ix = (int)__dmul_rn(__dsub_rn(px, L.gx0), L.ginv);
+        int iy = (int)__dmul_rn(__dsub_rn(py, L.gy0), L.ginv);
+        ix = ix < 0 ? 0 : (ix >= L.gnx ? L.gnx - 1 : ix);
+        iy = iy < 0 ? 0 : (iy >= L.gny ? L.gny - 1 : iy);
+        const int2 ce = __ldg(L.cells + (int64_t)iy * L.gnx + ix);
+        if (ce.y >= 0) {
+            C.first = ce.x;
+            C.n = ce.y;
+            for (int k = ce.x; k < ce.x + ce.y; k++) {
+                const float4 r = __ldg(L.crects + k);
+                const double x0 = r.x, y0 = r.y, x1 = r.z, y1 = r.w;
+                const double g = fmax(fmax(x0 - px, px - x1), fmax(y0 - py, py - y1));
+                if (g <= 0.0 && px >= x0 && py >= y0 && px <= x1 && py <= y1) {
+                    const int id = __ldg(L.cids + k);
+                    hit = id < hit ? id : hit;
+                }
+                best = fmin(best, g);
+            }
+            return st;
+        }
+    }
+    if (kOutOfLineTree)
+        return tree_clearance_call(L.nbox, L.nref, L.rects, L.ids, px, py, r2, L.slack, C, hit, best);
+    return tree_clearance(L.nbox, L.nref, L.rects, L.ids, px, py, r2, L.slack, C, hit, best);
 }
 
 // Tree::checkCollisions(box) restricted to the near-tie list (exact for the
@@ -328,12 +350,12 @@ __device__ __forceinline__ uint32_t replay_square(const DevLayout &L, const Cand
 }
 
 // drawBiggestSquareAtPoint + checkCollisons(point) for one point.
-template <bool kInside = false>
+template <bool kInside = false, bool kOutOfLineTree = false>
 __device__ __forceinline__ uint32_t query_point(const DevLayout &L, double px, double py, double sq[4],
                                                 int &hit) {
     Cands C;
     double best;
-    uint32_t st = clearance<kInside>(L, px, py, C, hit, best);
+    uint32_t st = clearance<kInside, kOutOfLineTree>(L, px, py, C, hit, best);
     st |= replay_square(L, C, px, py, best, sq);
     return st;
 }

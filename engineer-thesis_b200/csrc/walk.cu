@@ -438,7 +438,9 @@ __global__ void __launch_bounds__(kWalkThreads, kUniform ? kWalkMinBlocksW : kWa
                 code = -1;  // escaped: left the layer bounds
             } else {
                 int hit;
-                st |= query_point<true>(L, px, py, sq, hit);
+                // the rare tree traversal (overflowed cells) is a call in the
+                // 48-register kernel, whose code it would otherwise crowd
+                st |= query_point<true, !kUniform>(L, px, py, sq, hit);
                 hops++;
                 if (hit != kNoHit) code = hit;
                 else if (hops >= P.hop_cap) code = -2;
