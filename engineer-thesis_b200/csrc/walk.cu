@@ -66,12 +66,6 @@ __device__ __forceinline__ uint4 draw_block(uint64_t seed, uint32_t stream, uint
                     make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
 }
 
-__device__ __forceinline__ double word_u(const uint4 &b, uint32_t hop) {
-    const uint32_t k = hop & 3;
-    const uint32_t x = k == 0 ? b.x : (k == 1 ? b.y : (k == 2 ? b.z : b.w));
-    return (double)x * 0x1p-32;
-}
-
 // The last bin lo in [0, 200) with intg[lo] <= u (intg nondecreasing,
 // intg[0] = 0), by binary search.
 __device__ __forceinline__ int bin_search(const double *s_intg, double u) {
@@ -287,8 +281,9 @@ __global__ void __launch_bounds__(kWalkThreads, kUniform ? kWalkMinBlocksW : kWa
     bool active = false, exhausted = false;
     int job = 0;
     uint64_t pw = 0;
-    uint32_t stream = 0;
-    uint4 rnd = make_uint4(0, 0, 0, 0);  // uniforms of Philox words (hops & ~3) .. +3
+    // the lane's Philox block, words (hops & ~3) .. +3: in shared memory,
+    // which frees four registers (fewer spills), one load per hop
+    __shared__ uint32_t s_rnd[4][kWalkThreads];
     // queries so far of the lane's walk, also the Philox word of its next
     // point (word 0 places the start, word h the point after query h)
     int32_t hops = 0, bin1 = -1;
@@ -364,7 +359,6 @@ __global__ void __launch_bounds__(kWalkThreads, kUniform ? kWalkMinBlocksW : kWa
                     sq[2] = g4.z;
                     sq[3] = g4.w;
                     pw = J.first_walk + (gw - J.walk_begin);
-                    stream = J.stream_id;
                     hops = 0;
                     bin1 = -1;
                     if (kCV) cvq = -1;
@@ -398,8 +392,14 @@ __global__ void __launch_bounds__(kWalkThreads, kUniform ? kWalkMinBlocksW : kWa
         if (active) {
             const uint32_t hop = (uint32_t)hops;
             const bool starting = hops == 0;
-            if ((hop & 3) == 0) rnd = draw_block(seed, stream, pw, hop);
-            double u = word_u(rnd, hop);
+            if ((hop & 3) == 0) {
+                const uint4 b = draw_block(seed, job_of<kMulti>(P, job).stream_id, pw, hop);
+                s_rnd[0][threadIdx.x] = b.x;
+                s_rnd[1][threadIdx.x] = b.y;
+                s_rnd[2][threadIdx.x] = b.z;
+                s_rnd[3][threadIdx.x] = b.w;
+            }
+            double u = (double)s_rnd[hop & 3][threadIdx.x] * 0x1p-32;
             if (starting) {
                 if (kUniform)
                     perim = __dadd_rn(__dmul_rn(2.0, __dsub_rn(sq[2], sq[0])), __dmul_rn(2.0, __dsub_rn(sq[3], sq[1])));
