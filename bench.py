@@ -53,6 +53,7 @@ WORKLOAD = dict(workload="frw-c3-1e6-rects-1e8-walks", rects=1_000_000, domain=1
                    "between steps")
 METRIC = "walks/s (plain FRW, 10^6-rect layout, 1e8 walks/step, reference surface, start and estimator)"
 PROFILE = os.path.join(ROOT, "profiles", "walk_kernel_c3.md")
+PROFILE3 = os.path.join(ROOT, "profiles", "walk3d_kernel_1e4_boxes.md")
 
 
 def algorithmic_bytes_per_query(n_rects: int) -> int:
@@ -440,7 +441,7 @@ def _port3_worker(args):
     return done, time.perf_counter() - t0
 
 
-def walk3d_run(frw, device, stream, steps, cpu_seconds, cores):
+def walk3d_run(frw, device, stream, steps, cpu_seconds, cores, sm_mhz=None):
     """The 3-D walk (box conductors, cube transition domains from the
     reference's unit-cube Green's function): 10^4 boxes, 1e7 walks per step,
     capacitance row of box 0.  Per-walk records equal the FP64 oracle's
@@ -492,11 +493,18 @@ def walk3d_run(frw, device, stream, steps, cpu_seconds, cores):
     hops = r.hops_total
     peak, peak_kind = measured_peak_hbm()
     ach = hops * bh / (kms * 1e-3) / 1e9
+    prof3 = profile_figures(PROFILE3)
     roof3 = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-             "traffic": 1045248,
+             "traffic": prof3.get("dram_bytes_per_launch"),
              "note": f"k_walk3; algorithmic {bh:.0f} B/hop x {hops / W3D['walks']:.2f} hops/walk; peak {peak_kind}; "
-                     "traffic = DRAM bytes of one 1e6-walk launch under ncu (cold reads; the lists and tables "
-                     "are L2-resident, so HBM is an upper-bound denominator)"}
+                     "traffic = DRAM bytes of one 1e6-walk launch under ncu (cold reads of the lists and tables, "
+                     "which stay L2-resident: HBM is an upper-bound denominator, issue_frac the bound)"}
+    if "warp_instructions_per_walk" in prof3 and sm_mhz:
+        sms = torch.cuda.get_device_properties(device).multi_processor_count
+        roof3["issue_frac"] = (W3D["walks"] / (kms * 1e-3)) * prof3["warp_instructions_per_walk"] / (
+            sms * 4 * sm_mhz * 1e6)
+        roof3["warp_instructions_per_walk"] = prof3["warp_instructions_per_walk"]
+        roof3["threads_per_instruction"] = prof3.get("threads_per_instruction")
     out = {"workload": W3D["workload"], "config": W3D, "ms_per_step": ms, "walks_per_s": W3D["walks"] / (ms * 1e-3),
            "kernel_ms": kms, "kernel_walks_per_s": W3D["walks"] / (kms * 1e-3),
            "hops_per_s": r.hops_total / (kms * 1e-3), "mean_hops": r.hops_total / W3D["walks"],
@@ -727,7 +735,7 @@ def main():
         sub["batched"] = batched_run(frw, local, stream, 3)
     if solo and not args.no_3d:
         sub["walk3d"] = walk3d_run(frw, local, stream, 3, 0.0 if args.no_cpu_baseline else 2.0,
-                                   min(host_cores(), 16))
+                                   min(host_cores(), 16), clk.summary().get("sm_mhz"))
 
     if rank == 0:
         hbar = float(stats[2]) / float(stats[3])
