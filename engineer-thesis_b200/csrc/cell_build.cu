@@ -337,8 +337,9 @@ frw_status build_grid(const DevLayout &L, const Grid &G, int factor, double extr
         if (!ck(cudaMallocAsync(&rad, (size_t)ncells * 8, st), "malloc cell radii (build)")) break;
         if (!ck(cudaMallocAsync(&stage, (size_t)ncells * kStage * 4, st), "malloc staged rects")) break;
         if (!ck(cudaMallocAsync(&sums, (size_t)tiles * 8, st), "malloc tile sums")) break;
-        if (!ck(cudaMallocAsync(&grand, 8, st), "malloc total")) break;
-        if (!ck(cudaMallocAsync(&ovf, 8, st), "malloc overflow count")) break;
+        // the list total and the overflow count side by side: one read-back
+        if (!ck(cudaMallocAsync(&grand, 16, st), "malloc total")) break;
+        ovf = reinterpret_cast<unsigned long long *>(grand + 1);
         if (!ck(cudaMemsetAsync(ovf, 0, 8, st), "memset")) break;
         const unsigned blocks = (unsigned)((ncells + 127) / 128);
         const int64_t nt = tiled_threads(G.nx, G.ny);
@@ -349,8 +350,7 @@ frw_status build_grid(const DevLayout &L, const Grid &G, int factor, double extr
         k_tile_scan<<<(unsigned)tiles, kScanThreads, 0, st>>>(cnt, ncells, sums, start);
         if (!ck(cudaGetLastError(), "cell count")) break;
         unsigned long long h[2] = {0, 0};  // list total, overflowed cells
-        if ((rc = read_back(&h[0], grand, 8, st, "build_cells: list total"))) break;
-        if ((rc = read_back(&h[1], ovf, 8, st, "build_cells: overflow count"))) break;
+        if ((rc = read_back(h, grand, 16, st, "build_cells: list total"))) break;
         const int64_t total = (int64_t)h[0];
         if (total > INT32_MAX) {
             set_error("build_cells: more than 2^31 list entries; use fewer cells per rect");
@@ -365,7 +365,7 @@ frw_status build_grid(const DevLayout &L, const Grid &G, int factor, double extr
             k_cell_fill<<<blocks, 128, 0, st>>>(L, G, factor, start, rad, stage, C.cells, C.crects, C.cids, ncells);
         if (!ck(cudaGetLastError(), "cell fill")) break;
     } while (0);
-    for (void *p : {(void *)cnt, (void *)start, (void *)sums, (void *)grand, (void *)ovf, (void *)rad, (void *)stage})
+    for (void *p : {(void *)cnt, (void *)start, (void *)sums, (void *)grand, (void *)rad, (void *)stage})
         if (p) cudaFreeAsync(p, st);
     C.bytes = ncells * (int64_t)(sizeof(int2) + sizeof(float)) + C.entries * 20;
     return rc;

@@ -460,21 +460,27 @@ frw_status read_back(void *host, const void *dev, size_t bytes, cudaStream_t st,
     // wait; a copy whose wait gave up may still land, so its buffer is left
     // to it
     constexpr size_t kStage = 4096;
-    static thread_local void *stage = nullptr;
+    struct Stage {  // released when the thread ends
+        void *p = nullptr;
+        ~Stage() {
+            if (p) cudaFreeHost(p);
+        }
+    };
+    static thread_local Stage stage;
     if (staged && bytes <= kStage) {
-        if (!stage && cudaMallocHost(&stage, kStage) != cudaSuccess) {
-            stage = nullptr;
+        if (!stage.p && cudaMallocHost(&stage.p, kStage) != cudaSuccess) {
+            stage.p = nullptr;
             cudaGetLastError();
         }
-        if (stage) {
-            cudaError_t e = cudaMemcpyAsync(stage, dev, bytes, cudaMemcpyDeviceToHost, st);
+        if (stage.p) {
+            cudaError_t e = cudaMemcpyAsync(stage.p, dev, bytes, cudaMemcpyDeviceToHost, st);
             if (e != cudaSuccess) return cuda_fail(e, what);
             frw_status rc = wait_stream(st, what);
             if (rc) {
-                stage = nullptr;
+                stage.p = nullptr;  // the copy may still land there: the buffer is left to it
                 return rc;
             }
-            memcpy(host, stage, bytes);
+            memcpy(host, stage.p, bytes);
             return FRW_OK;
         }
     }
