@@ -197,11 +197,12 @@ __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, dou
         if (ce.y >= 0) {
             C.first = ce.x;
             C.n = ce.y;
+#pragma unroll 2
             for (int k = ce.x; k < ce.x + ce.y; k++) {
                 const float4 r = __ldg(L.crects + k);
                 const double x0 = r.x, y0 = r.y, x1 = r.z, y1 = r.w;
                 const double g = fmax(fmax(x0 - px, px - x1), fmax(y0 - py, py - y1));
-                if (g <= 0.0 && px >= x0 && py >= y0 && px <= x1 && py <= y1) {
+                if (g <= 0.0) {  // each difference is <= 0 exactly when p is on that side
                     const int id = __ldg(L.cids + k);
                     hit = id < hit ? id : hit;
                 }
