@@ -178,10 +178,11 @@ static __device__ __noinline__ uint32_t tree_clearance_call(const float4 *nbox, 
 // kOutOfLineTree: the tree traversal is a call (smaller code at the caller).
 template <bool kInside = false, bool kOutOfLineTree = false>
 __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, double py, Cands &C,
-                                              int &hit, double &best) {
+                                              int &hit, double &best, double bd = -1.0) {
     uint32_t st = 0;
     const double r2 = 2.0 * L.delta;
-    best = fmin(fmin(px - L.bx0, L.bx1 - px), fmin(py - L.by0, L.by1 - py));
+    // bd: the bounds distance, when the caller has it (kInside)
+    best = kInside ? bd : fmin(fmin(px - L.bx0, L.bx1 - px), fmin(py - L.by0, L.by1 - py));
     hit = kNoHit;
     C.n = 0;
     C.first = -1;
@@ -353,10 +354,10 @@ __device__ __forceinline__ uint32_t replay_square(const DevLayout &L, const Cand
 // drawBiggestSquareAtPoint + checkCollisons(point) for one point.
 template <bool kInside = false, bool kOutOfLineTree = false>
 __device__ __forceinline__ uint32_t query_point(const DevLayout &L, double px, double py, double sq[4],
-                                                int &hit) {
+                                                int &hit, double bd = -1.0) {
     Cands C;
     double best;
-    uint32_t st = clearance<kInside, kOutOfLineTree>(L, px, py, C, hit, best);
+    uint32_t st = clearance<kInside, kOutOfLineTree>(L, px, py, C, hit, best, bd);
     st |= replay_square(L, C, px, py, best, sq);
     return st;
 }

@@ -90,6 +90,15 @@ __device__ __forceinline__ int bin_of(const double *s_intg, const uint8_t *guide
     return lo;
 }
 
+// The same bin for u = word / 2^32, in integers: the guide entry of
+// floor(u * 256) = word >> 24, then word > thr[lo + 1] exactly when
+// intg[lo + 1] <= u.
+__device__ __forceinline__ int bin_of_word(const uint32_t *thr, const uint8_t *guide, uint32_t word) {
+    int lo = guide[word >> 24];
+    while (lo < FRW_NSAMPLE - 1 && word > thr[lo + 1]) lo++;
+    return lo;
+}
+
 __device__ __forceinline__ void kahan_add(double &s, double &c, double v) {
     const double y = __dsub_rn(v, c);
     const double t = __dadd_rn(s, y);
@@ -248,12 +257,17 @@ __global__ void __launch_bounds__(kWalkThreads, kUniform ? kWalkMinBlocksW : kWa
     __shared__ double s_wx[FRW_NSAMPLE], s_wy[FRW_NSAMPLE];
     __shared__ Slot s_tab[kWarpsPerBlock][kTabSlots];
     __shared__ uint8_t s_guide[kGuide];
+    __shared__ uint32_t s_thr[FRW_NSAMPLE + 1];  // ceil(intg[k] * 2^32) - 1: u >= intg[k] iff word > s_thr[k]
     __shared__ unsigned long long s_chunk[kWarpsPerBlock][2];  // per warp: unclaimed part of its walk chunk
     __shared__ unsigned long long s_lhops[kWalkThreads];       // per lane: hops of its walks (current job)
     __shared__ double s_cvz[kCV ? 2 : 1][kCV ? kWalkThreads : 1];  // per lane: sums of z and z^2
 
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    for (int i = threadIdx.x; i <= FRW_NSAMPLE; i += blockDim.x) s_intg[i] = P.intg[i];
+    for (int i = threadIdx.x; i <= FRW_NSAMPLE; i += blockDim.x) {
+        s_intg[i] = P.intg[i];
+        // intg[k] * 2^32 is exact; its ceiling is in [1, 2^32] for k >= 1
+        s_thr[i] = (uint32_t)((unsigned long long)ceil(P.intg[i] * 0x1p32) - 1ull);
+    }
     for (int i = threadIdx.x; i < FRW_NSAMPLE; i += blockDim.x) {
         s_wx[i] = P.wx[i];
         s_wy[i] = P.wy[i];
@@ -399,7 +413,8 @@ __global__ void __launch_bounds__(kWalkThreads, kUniform ? kWalkMinBlocksW : kWa
                 s_rnd[2][threadIdx.x] = b.z;
                 s_rnd[3][threadIdx.x] = b.w;
             }
-            double u = (double)s_rnd[hop & 3][threadIdx.x] * 0x1p-32;
+            const uint32_t word = s_rnd[hop & 3][threadIdx.x];
+            double u = (double)word * 0x1p-32;
             if (starting) {
                 if (kUniform)
                     perim = __dadd_rn(__dmul_rn(2.0, __dsub_rn(sq[2], sq[0])), __dmul_rn(2.0, __dsub_rn(sq[3], sq[1])));
@@ -416,7 +431,10 @@ __global__ void __launch_bounds__(kWalkThreads, kUniform ? kWalkMinBlocksW : kWa
             if (starting && uniform_start) {
                 side = perimeter_point(sq, u, px, py);
             } else {
-                const int bin = bin_of(s_intg, s_guide, u);
+                // the bin of the word itself (u = word / 2^32) unless a
+                // stratified or grid start moved u
+                const int bin = starting && (P.start_strata || P.start_grid) ? bin_of(s_intg, s_guide, u)
+                                                                            : bin_of_word(s_thr, s_guide, word);
                 point_from_index(sq, bin, exact, px, py);
                 if (hop == 1) {
                     if (kRec && P.rec_q) P.rec_q[walk_index()] = (-2 - bin1) * FRW_NSAMPLE + bin;
@@ -434,13 +452,16 @@ __global__ void __launch_bounds__(kWalkThreads, kUniform ? kWalkMinBlocksW : kWa
         if (active) {
             const WalkJob &J = job_of<kMulti>(P, job);
             const DevLayout &L = J.L;
-            if (!(px > L.bx0 && py > L.by0 && px < L.bx1 && py < L.by1)) {
+            // distance to the bounds: p is strictly inside exactly when it is
+            // > 0 (each difference is > 0 exactly when p is on that side)
+            const double bd = fmin(fmin(px - L.bx0, L.bx1 - px), fmin(py - L.by0, L.by1 - py));
+            if (!(bd > 0.0)) {
                 code = -1;  // escaped: left the layer bounds
             } else {
                 int hit;
                 // the rare tree traversal (overflowed cells) is a call in the
                 // 48-register kernel, whose code it would otherwise crowd
-                st |= query_point<true, !kUniform>(L, px, py, sq, hit);
+                st |= query_point<true, !kUniform>(L, px, py, sq, hit, bd);
                 hops++;
                 if (hit != kNoHit) code = hit;
                 else if (hops >= P.hop_cap) code = -2;
