@@ -13,16 +13,20 @@
 //     counter (hop/4, walk, stream), one 32-bit word per hop: a walk's
 //     trajectory depends only on its index, never on scheduling, so every
 //     walk can be replayed by the CPU oracle bit-for-bit;
-//   * the Green CDF (201 doubles), a 256-entry guide to it and the first-hop
-//     weight tables sit in shared memory; a bin is the guide's entry plus a
-//     step or two (the reference's linear scan, CPU/mainFunctions.cpp:40-46,
-//     returns the same index because the CDF is nondecreasing);
+//   * the Green CDF (201 doubles, and as integer thresholds on the Philox
+//     word), a 256-entry guide to it and the first-hop weight tables sit in
+//     shared memory; a bin is the guide's entry plus a step or two (the
+//     reference's linear scan, CPU/mainFunctions.cpp:40-46, returns the same
+//     index because the CDF is nondecreasing);
 //   * each hop is one clearance lookup + scalar replay (query.cuh);
 //   * walks ending on their job's target are summed in lane registers; other
 //     ends are accumulated per (job, conductor) in a per-warp shared-memory
-//     table with Kahan-compensated FP64 sums (single writer per update),
-//     flushed to global FP64 rows when full and at exit, where the lane sums
-//     join it.
+//     table, with Kahan-compensated FP64 sums (single writer per update) for
+//     weighted walks and counts alone (shared atomics) otherwise, flushed to
+//     the global rows when full and at exit, where the lane sums join it;
+//   * the kernel is compiled per launch configuration: one job or many,
+//     per-walk records or none, weighted (uniform) start or not, control-
+//     variate sums or not.
 #include "query.cuh"
 
 namespace frw {
