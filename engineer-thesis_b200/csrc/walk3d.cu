@@ -513,20 +513,21 @@ __global__ void __launch_bounds__(kW3Threads, kW3MinBlocks) k_walk3(const Walk3P
         if (__ballot_sync(kFull, active) == 0) break;
         if (!active) continue;
 
-        // one hop
+        // up to two hops per round of refills and walk ends
         int64_t end = -3;  // still walking
-        double d = 0.0;
-        if (!(W.px > P.L.b[0] && W.py > P.L.b[1] && W.pz > P.L.b[2] && W.px < P.L.b[3] && W.py < P.L.b[4] &&
-              W.pz < P.L.b[5])) {
-            end = -1;
-        } else {
-            int id;
-            nearest3(P.L, W.px, W.py, W.pz, d, id);
-            W.hops++;
-            if (d <= P.shell) end = id;
-            else if (W.hops >= P.hop_cap) end = -2;
-        }
-        if (end == -3) {
+        for (int pass = 0; pass < 2; pass++) {
+            double d = 0.0;
+            if (!(W.px > P.L.b[0] && W.py > P.L.b[1] && W.pz > P.L.b[2] && W.px < P.L.b[3] && W.py < P.L.b[4] &&
+                  W.pz < P.L.b[5])) {
+                end = -1;
+            } else {
+                int id;
+                nearest3(P.L, W.px, W.py, W.pz, d, id);
+                W.hops++;
+                if (d <= P.shell) end = id;
+                else if (W.hops >= P.hop_cap) end = -2;
+            }
+            if (end != -3) break;
             const uint32_t t = (uint32_t)W.hops + 1;
             if ((t >> 2) != W.rblk) {
                 W.rblk = t >> 2;
@@ -540,8 +541,8 @@ __global__ void __launch_bounds__(kW3Threads, kW3MinBlocks) k_walk3(const Walk3P
                 W.b1 = b;
                 W.a0 = __dmul_rn(2.0, d);
             }
-            continue;
         }
+        if (end == -3) continue;
         // the walk ended
         double c = 0.0;
         const double S = kMulti ? __ldg(&P.jobs[W.job].S) : P.S;
