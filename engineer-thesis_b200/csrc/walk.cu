@@ -34,10 +34,13 @@ namespace {
 
 constexpr int kWalkThreads = 256;
 constexpr int kHopsPerRound = 2;  // hops between refill / walk-end rounds (1: 5.8% slower, 3: 5.6%)
-// Resident blocks per SM: weighted walks (uniform start) keep more state, so
-// they run at 64 registers per thread (4 blocks of 256, 32 warps); walks
-// without weights fit 48 registers and run 5 blocks (40 warps).
-constexpr int kWalkMinBlocksW = 4;
+// Resident blocks per SM: 5 blocks of 256 (40 warps) at 48 registers per
+// thread, for weighted (uniform start) and unweighted walks alike (weighted
+// walks spill a little more there but gain from the extra warps since the
+// loop runs two hops per round; 4 blocks at 64 registers: 1.6% slower) --
+// except weighted walks of many jobs, whose per-job loads need the registers
+// (4 blocks at 64 registers: 6% faster than 5 at 48).
+constexpr int kWalkMinBlocksMultiW = 4;
 constexpr int kWalkMinBlocks = 5;
 constexpr int kWarpsPerBlock = kWalkThreads / 32;
 constexpr int kTabSlots = 32;  // per warp
@@ -257,7 +260,8 @@ __device__ __forceinline__ void tab_round(const WalkParams &P, Slot *tab, int la
 // weight sums are compiled out.  kCV: the control variate's sums (P.cv_phi,
 // P.cv_sums) are kept beside the rows.
 template <bool kMulti, bool kRec, bool kUniform, bool kCV = false>
-__global__ void __launch_bounds__(kWalkThreads, kUniform ? kWalkMinBlocksW : kWalkMinBlocks) k_walk(const WalkParams P) {
+__global__ void __launch_bounds__(kWalkThreads, kMulti && kUniform ? kWalkMinBlocksMultiW : kWalkMinBlocks)
+    k_walk(const WalkParams P) {
     __shared__ double s_intg[FRW_NSAMPLE + 1];
     __shared__ double s_wx[FRW_NSAMPLE], s_wy[FRW_NSAMPLE];
     __shared__ Slot s_tab[kWarpsPerBlock][kTabSlots];
