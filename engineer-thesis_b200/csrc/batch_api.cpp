@@ -86,6 +86,7 @@ WalkParams params_for(const frw_batch *B, const WalkJob *jobs, const WalkJob &jo
     P.wx = B->tables + FRW_NSAMPLE + 1;
     P.wy = B->tables + 2 * FRW_NSAMPLE + 1;
     P.job0 = job0;  // read by the single-job kernel when the batch has one job
+    for (int j = 0; j < B->njobs; j++) P.tree_points |= B->hjobs[j].L.tree_points;
     return P;
 }
 
@@ -199,7 +200,7 @@ frw_status frw_batch_create(const frw_layout *const *layouts, const int64_t *tar
     std::vector<double> tg(4 * (size_t)njobs);
     for (int j = 0; j < njobs; j++) {
         WalkJob &J = jobs[j];
-        memset(&J, 0, sizeof(J));
+        J = WalkJob{};
         J.L = B->views[j].dl;
         J.target = targets[j];
         J.walk_begin = B->begin[j];

@@ -295,6 +295,7 @@ void attach_cells(DevLayout &L, const CellBuffers &c) {
     L.ginv = c.ginv;
     L.gnx = c.nx;
     L.gny = c.ny;
+    L.tree_points = c.cells == nullptr || c.overflow > 0;
 }
 
 namespace {

@@ -815,6 +815,7 @@ frw_status frw_layout_set_cells(frw_layout *L, double cells_per_rect, int max_pe
     free_cells(&L->cells, nullptr);
     L->cells = c;
     L->dl.cells = nullptr;
+    L->dl.tree_points = 1;
     if (c.cells) attach_cells(L->dl, c);
     return FRW_OK;
 }

@@ -52,6 +52,10 @@ struct DevLayout {
     const float *crad;  // per cell: every rect within this L-inf distance of any point of the cell is listed
     double gx0, gy0, ginv;
     int32_t gnx, gny;
+    // 1 when the tree answers some points (no cell lists, or overflowed
+    // cells): only then can a point have more near ties than the tree's
+    // candidate list holds
+    int32_t tree_points = 1;
 };
 
 // ---- device status word (atomicOr'ed by kernels, read back by the host) ----
@@ -115,6 +119,9 @@ struct WalkParams {
     const double *intg;  // [201]
     const double *wx;    // [200]
     const double *wy;    // [200]
+    // 1 when some job's layout has tree_points set: the walk kernel then
+    // carries the whole-tree replay for points with many exact ties
+    int32_t tree_points;
 };
 
 // ---- host helpers ----------------------------------------------------------

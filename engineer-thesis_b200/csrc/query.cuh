@@ -34,8 +34,10 @@ constexpr double kMinDist = (double).095f;  // drawBiggestSquareAtPoint MIN_DIST
 // point answered by a cell list keeps its cell's whole list (first >= 0:
 // the cell-list entries first .. first + n - 1), a superset of the near
 // ties; a point answered by the tree keeps the near-tie list idx[0 .. n) of
-// tree rects (first < 0).  Testing more rects than the ties is as exact:
-// every listed rect is a real rect of the layout.
+// tree rects (first == -1).  Testing more rects than the ties is as exact:
+// every listed rect is a real rect of the layout.  More ties than kCandMax
+// (rects whose near sides line up tie exactly) set first = -2: the replay's
+// boxes near the clearance are then tested against the whole tree.
 struct Cands {
     int idx[kCandMax];  // tree: positions of the near-tied rects among the tree's rects
     float g[kCandMax];  // their gaps, rounded down (keeping extra entries is harmless)
@@ -50,6 +52,9 @@ __device__ __forceinline__ float lb_box_f(const float4 b, float px, float py) {
 
 // One rect of a leaf or a cell list: FP32 screen, then the exact FP64 gap;
 // tightens `best`, keeps the near-tie list and the containing rect.
+// kTies: a full list marks the point (C.first = -2) for the whole-tree
+// replay; otherwise a full list is an error.
+template <bool kTies>
 __device__ __forceinline__ void scan_rect(const float4 r, int k, const int32_t *ids, double px, double py,
                                           float pxf, float pyf, double r2, float slack, float &limf,
                                           double &best, int &hit, Cands &C, uint32_t &st) {
@@ -78,6 +83,11 @@ __device__ __forceinline__ void scan_rect(const float4 r, int k, const int32_t *
             C.idx[C.n] = k;
             C.g[C.n] = __double2float_rd(g);
             C.n++;
+        } else if (kTies) {
+            // more ties than the list holds (rects with aligned sides tie
+            // exactly: a column of equal x0 seen from its left): the replay's
+            // boxes near the clearance are then tested against the whole tree
+            C.first = -2;
         } else {
             st |= kStCandOverflow;
         }
@@ -88,6 +98,7 @@ __device__ __forceinline__ void scan_rect(const float4 r, int k, const int32_t *
 // depth-first, nearest-child-first traversal from the bounds distance in
 // `best`; FP32 screens (errors below slack), the exact FP64 gap only for
 // rects that can matter.
+template <bool kTies>
 __device__ __forceinline__ uint32_t tree_clearance(const float4 *nbox, const int4 *nref, const float4 *rects,
                                                    const int32_t *ids, double px, double py, double r2, float slack,
                                                    Cands &C, int &hit, double &best) {
@@ -116,7 +127,7 @@ __device__ __forceinline__ uint32_t tree_clearance(const float4 *nbox, const int
             if (ref[c] >= kRefEmpty || lb[c] > limf) continue;
             const int f = leaf_first(ref[c]), m = leaf_count(ref[c]);
             for (int k = f; k < f + m; k++)
-                scan_rect(__ldg(rects + k), k, ids, px, py, pxf, pyf, r2, slack, limf, best, hit, C, st);
+                scan_rect<kTies>(__ldg(rects + k), k, ids, px, py, pxf, pyf, r2, slack, limf, best, hit, C, st);
         }
         // internal children within reach: visit the nearest next, stack the rest
         int next = -1;
@@ -155,11 +166,12 @@ __device__ __forceinline__ uint32_t tree_clearance(const float4 *nbox, const int
 }
 
 // The same, out of line (a call: smaller code where the tree is rare).
+template <bool kTies>
 static __device__ __noinline__ uint32_t tree_clearance_call(const float4 *nbox, const int4 *nref,
                                                             const float4 *rects, const int32_t *ids, double px,
                                                             double py, double r2, float slack, Cands &C, int &hit,
                                                             double &best) {
-    return tree_clearance(nbox, nref, rects, ids, px, py, r2, slack, C, hit, best);
+    return tree_clearance<kTies>(nbox, nref, rects, ids, px, py, r2, slack, C, hit, best);
 }
 
 // The clearance of p and its near-tie list.  With cell lists the list of
@@ -176,7 +188,8 @@ static __device__ __noinline__ uint32_t tree_clearance_call(const float4 *nbox, 
 // get the exact FP64 gap.  Returns status bits.
 // kInside: the caller has checked that p lies inside the bounds.
 // kOutOfLineTree: the tree traversal is a call (smaller code at the caller).
-template <bool kInside = false, bool kOutOfLineTree = false>
+// kTies: see scan_rect.
+template <bool kInside = false, bool kOutOfLineTree = false, bool kTies = true>
 __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, double py, Cands &C,
                                               int &hit, double &best, double bd = -1.0) {
     uint32_t st = 0;
@@ -213,9 +226,12 @@ __device__ __forceinline__ uint32_t clearance(const DevLayout &L, double px, dou
         }
     }
     if (kOutOfLineTree)
-        return tree_clearance_call(L.nbox, L.nref, L.rects, L.ids, px, py, r2, L.slack, C, hit, best);
-    return tree_clearance(L.nbox, L.nref, L.rects, L.ids, px, py, r2, L.slack, C, hit, best);
+        return tree_clearance_call<kTies>(L.nbox, L.nref, L.rects, L.ids, px, py, r2, L.slack, C, hit, best);
+    return tree_clearance<kTies>(L.nbox, L.nref, L.rects, L.ids, px, py, r2, L.slack, C, hit, best);
 }
+
+__device__ __forceinline__ bool tree_box(const float4 *nbox, const int4 *nref, const float4 *rects,
+                                         const double B[4], bool has_ign, const double ign[4], uint32_t &st);
 
 // Tree::checkCollisions(box) restricted to the near-tie list (exact for the
 // boxes of the replay, see the file comment).  Only boxes within delta of the
@@ -247,10 +263,19 @@ __device__ __forceinline__ Window replay_window(const DevLayout &L, double px, d
     return Window{__dadd_rn(px, __dadd_rn(dstar, L.delta)), __dadd_rn(px, __dsub_rn(dstar, L.delta))};
 }
 
+// kTree: the near-tie list overflowed (C.first == -2) and the exact
+// predicate is the whole tree's checkCollisions(box).
+template <bool kTree>
 __device__ __forceinline__ bool collides_box(const DevLayout &L, const Cands &C, const double o[4],
-                                             const Window &W) {
+                                             const Window &W, uint32_t &st) {
     bool c = o[2] > W.hi;
-    if (!c && !(o[2] < W.lo)) c = collides_listed(L, C, o);  // rare: within delta of the clearance
+    if (!c && !(o[2] < W.lo)) {  // rare: within delta of the clearance
+        if (kTree)
+            c = !(o[1] >= L.by0 && o[0] >= L.bx0 && o[3] <= L.by1 && o[2] <= L.bx1) ||
+                tree_box(L.nbox, L.nref, L.rects, o, false, nullptr, st);
+        else
+            c = collides_listed(L, C, o);
+    }
     return c;
 }
 
@@ -274,22 +299,23 @@ __device__ __forceinline__ double signed_step(double d, bool shrink) {
 // drawBiggestSquareAtPoint replayed on scalars: same operations, same order,
 // explicit round-to-nearest intrinsics (no contraction); the halvings as
 // above.
+template <bool kTree = false>
 __device__ __forceinline__ uint32_t replay_square(const DevLayout &L, const Cands &C, double px,
                                                   double py, double dstar, double sq[4]) {
     const Window W = replay_window(L, px, dstar);
+    uint32_t st = 0;
     double o[4] = {__dsub_rn(px, 1.0), __dsub_rn(py, 1.0), __dadd_rn(px, 1.0), __dadd_rn(py, 1.0)};
-    if (collides_box(L, C, o, W)) {
+    if (collides_box<kTree>(L, C, o, W, st)) {
         sq[0] = o[0]; sq[1] = o[1]; sq[2] = o[2]; sq[3] = o[3];
-        return 0;
+        return st;
     }
     const double in2[4] = {__dsub_rn(px, 2.0), __dsub_rn(py, 2.0), __dadd_rn(px, 2.0),
                            __dadd_rn(py, 2.0)};
-    if (collides_box(L, C, in2, W)) {
+    if (collides_box<kTree>(L, C, in2, W, st)) {
         sq[0] = in2[0]; sq[1] = in2[1]; sq[2] = in2[2]; sq[3] = in2[3];
-        return 0;
+        return st;
     }
     double dist = L.dist0;
-    uint32_t st = 0;
     // the loop's first box is p +- 1 again, already found free: its step (grow
     // by dist, no halving before the first collision) is taken directly
     o[0] = __dsub_rn(o[0], dist);
@@ -299,7 +325,7 @@ __device__ __forceinline__ uint32_t replay_square(const DevLayout &L, const Cand
     int it = 1;
     // Growth (the reference's maxReached still false): grow by dist, without
     // halving, until a box collides.
-    bool isc = collides_box(L, C, o, W);
+    bool isc = collides_box<kTree>(L, C, o, W, st);
     while (!isc) {
         o[0] = __dsub_rn(o[0], dist);
         o[1] = __dsub_rn(o[1], dist);
@@ -310,7 +336,7 @@ __device__ __forceinline__ uint32_t replay_square(const DevLayout &L, const Cand
             sq[0] = o[0]; sq[1] = o[1]; sq[2] = o[2]; sq[3] = o[3];
             return st;
         }
-        isc = collides_box(L, C, o, W);
+        isc = collides_box<kTree>(L, C, o, W, st);
     }
     // Bisection (maxReached): the loop runs while the box collides or dist is
     // above MIN_DIST; a colliding box shrinks by dist, halved first while above
@@ -334,7 +360,7 @@ __device__ __forceinline__ uint32_t replay_square(const DevLayout &L, const Cand
         o[1] = __dadd_rn(o[1], sd);
         o[2] = __dsub_rn(o[2], sd);
         o[3] = __dsub_rn(o[3], sd);
-        isc = collides_box(L, C, o, W);
+        isc = collides_box<kTree>(L, C, o, W, st);
     }
     while (isc) {
         o[0] = __dadd_rn(o[0], dist);
@@ -345,37 +371,60 @@ __device__ __forceinline__ uint32_t replay_square(const DevLayout &L, const Cand
             st |= kStReplayCap;
             break;
         }
-        isc = collides_box(L, C, o, W);
+        isc = collides_box<kTree>(L, C, o, W, st);
     }
     sq[0] = o[0]; sq[1] = o[1]; sq[2] = o[2]; sq[3] = o[3];
     return st;
 }
 
-// drawBiggestSquareAtPoint + checkCollisons(point) for one point.
-template <bool kInside = false, bool kOutOfLineTree = false>
+// The replay against the whole tree, out of line: one call site per query,
+// taken only by points with more near ties than the list holds.
+struct ReplayOut {
+    double sq[4];
+    uint32_t st;
+};
+static __device__ __noinline__ ReplayOut replay_tree_call(const DevLayout L, double px, double py,
+                                                          double dstar) {
+    Cands C;
+    C.n = 0;
+    C.first = -2;
+    ReplayOut r;
+    r.st = replay_square<true>(L, C, px, py, dstar, r.sq);
+    return r;
+}
+
+// drawBiggestSquareAtPoint + checkCollisons(point) for one point.  kTies:
+// points with more near ties than the list holds take the whole-tree replay
+// (else they report kStCandOverflow).
+template <bool kInside = false, bool kOutOfLineTree = false, bool kTies = true>
 __device__ __forceinline__ uint32_t query_point(const DevLayout &L, double px, double py, double sq[4],
                                                 int &hit, double bd = -1.0) {
     Cands C;
     double best;
-    uint32_t st = clearance<kInside, kOutOfLineTree>(L, px, py, C, hit, best, bd);
-    st |= replay_square(L, C, px, py, best, sq);
+    uint32_t st = clearance<kInside, kOutOfLineTree, kTies>(L, px, py, C, hit, best, bd);
+    if (kTies && C.first == -2) {
+        const ReplayOut r = replay_tree_call(L, px, py, best);
+        sq[0] = r.sq[0]; sq[1] = r.sq[1]; sq[2] = r.sq[2]; sq[3] = r.sq[3];
+        st |= r.st;
+    } else {
+        st |= replay_square(L, C, px, py, best, sq);
+    }
     return st;
 }
 
 // Tree::checkCollisions(box, ignore) for an arbitrary box (complete DFS).
-__device__ __forceinline__ bool box_collides(const DevLayout &L, const double B[4], bool has_ign,
-                                             const double ign[4], uint32_t &st) {
-    if (!(B[1] >= L.by0 && B[0] >= L.bx0 && B[3] <= L.by1 && B[2] <= L.bx1)) return true;
+__device__ __forceinline__ bool tree_box(const float4 *nbox, const int4 *nref, const float4 *rects,
+                                         const double B[4], bool has_ign, const double ign[4], uint32_t &st) {
     int stk[kStackMax];
     int sp = 1;
     stk[0] = 0;
     while (sp > 0) {
         const int nd = stk[--sp];
-        const int4 rf = __ldg(L.nref + nd);
+        const int4 rf = __ldg(nref + nd);
         const int ref[4] = {rf.x, rf.y, rf.z, rf.w};
         for (int c = 0; c < 4; c++) {
             if (ref[c] == kRefEmpty) continue;
-            const float4 b = __ldg(L.nbox + 4 * nd + c);
+            const float4 b = __ldg(nbox + 4 * nd + c);
             if (!((double)b.z >= B[0] && B[2] >= (double)b.x && (double)b.w >= B[1] && B[3] >= (double)b.y))
                 continue;
             if (ref[c] >= 0) {
@@ -385,7 +434,7 @@ __device__ __forceinline__ bool box_collides(const DevLayout &L, const double B[
             }
             const int f = leaf_first(ref[c]), m = leaf_count(ref[c]);
             for (int k = f; k < f + m; k++) {
-                const float4 r = __ldg(L.rects + k);
+                const float4 r = __ldg(rects + k);
                 const double x0 = r.x, y0 = r.y, x1 = r.z, y1 = r.w;
                 if (has_ign && x0 == ign[0] && y0 == ign[1] && x1 == ign[2] && y1 == ign[3]) continue;
                 if (x1 >= B[0] && B[2] >= x0 && y1 >= B[1] && B[3] >= y0) return true;
@@ -393,6 +442,11 @@ __device__ __forceinline__ bool box_collides(const DevLayout &L, const double B[
         }
     }
     return false;
+}
+__device__ __forceinline__ bool box_collides(const DevLayout &L, const double B[4], bool has_ign,
+                                             const double ign[4], uint32_t &st) {
+    if (!(B[1] >= L.by0 && B[0] >= L.bx0 && B[3] <= L.by1 && B[2] <= L.bx1)) return true;
+    return tree_box(L.nbox, L.nref, L.rects, B, has_ign, ign, st);
 }
 
 // x / 200 for an integer-valued x in [0, 2^31), correctly rounded without the

@@ -258,8 +258,11 @@ __device__ __forceinline__ void tab_round(const WalkParams &P, Slot *tab, int la
 // on the Gaussian perimeter, whose walks carry the first-hop weight; with
 // the Green-CDF start every weight is 0, so the weight, its inputs and the
 // weight sums are compiled out.  kCV: the control variate's sums (P.cv_phi,
-// P.cv_sums) are kept beside the rows.
-template <bool kMulti, bool kRec, bool kUniform, bool kCV = false>
+// P.cv_sums) are kept beside the rows.  kTies: the tree answers some points
+// (P.tree_points), and those with more exact near ties than its candidate
+// list holds take the whole-tree replay; without it that code is compiled
+// out of the kernel.
+template <bool kMulti, bool kRec, bool kUniform, bool kCV = false, bool kTies = false>
 __global__ void __launch_bounds__(kWalkThreads, kMulti && kUniform ? kWalkMinBlocksMultiW : kWalkMinBlocks)
     k_walk(const WalkParams P) {
     __shared__ double s_intg[FRW_NSAMPLE + 1];
@@ -476,7 +479,7 @@ __global__ void __launch_bounds__(kWalkThreads, kMulti && kUniform ? kWalkMinBlo
                     int hit;
                     // the rare tree traversal (overflowed cells) is a call in the
                     // 48-register kernel, whose code it would otherwise crowd
-                    st |= query_point<true, !kUniform>(L, px, py, sq, hit, bd);
+                    st |= query_point<true, !kUniform, kTies>(L, px, py, sq, hit, bd);
                     hops++;
                     if (hit != kNoHit) code = hit;
                     else if (hops >= P.hop_cap) code = -2;
@@ -588,6 +591,22 @@ int walk_max_blocks_per_sm(int threads, bool multi, bool uniform) {
     return b;
 }
 
+namespace {
+template <bool kTies>
+void launch_variant(const WalkParams &P, bool multi, bool rec, bool uni, bool cv, dim3 g, dim3 b,
+                    cudaStream_t stream) {
+    if (cv) k_walk<false, false, true, true, kTies><<<g, b, 0, stream>>>(P);
+    else if (multi && rec && uni) k_walk<true, true, true, false, kTies><<<g, b, 0, stream>>>(P);
+    else if (multi && rec) k_walk<true, true, false, false, kTies><<<g, b, 0, stream>>>(P);
+    else if (multi && uni) k_walk<true, false, true, false, kTies><<<g, b, 0, stream>>>(P);
+    else if (multi) k_walk<true, false, false, false, kTies><<<g, b, 0, stream>>>(P);
+    else if (rec && uni) k_walk<false, true, true, false, kTies><<<g, b, 0, stream>>>(P);
+    else if (rec) k_walk<false, true, false, false, kTies><<<g, b, 0, stream>>>(P);
+    else if (uni) k_walk<false, false, true, false, kTies><<<g, b, 0, stream>>>(P);
+    else k_walk<false, false, false, false, kTies><<<g, b, 0, stream>>>(P);
+}
+}  // namespace
+
 frw_status launch_walk(const WalkParams &P, int threads, int blocks, cudaStream_t stream) {
     if (threads != kWalkThreads) {
         set_error("launch_walk: threads per block must be 256");
@@ -595,23 +614,16 @@ frw_status launch_walk(const WalkParams &P, int threads, int blocks, cudaStream_
     }
     const bool rec = P.rec_end || P.rec_hops || P.rec_bin || P.rec_w || P.rec_q || P.rec_cv;
     const bool uni = P.start_mode == FRW_START_UNIFORM;
+    const bool cv = P.cv_phi || P.cv_sums;
+    if (cv && (!P.cv_phi || !P.cv_sums || P.njobs != 1 || rec || !uni || P.start_grid == 0)) {
+        set_error("launch_walk: the control variate needs one job, no records and the uniform grid start");
+        return FRW_E_ARG;
+    }
     const dim3 g(blocks), b(threads);
-    if (P.cv_phi || P.cv_sums) {
-        if (!P.cv_phi || !P.cv_sums || P.njobs != 1 || rec || !uni || P.start_grid == 0) {
-            set_error("launch_walk: the control variate needs one job, no records and the uniform grid start");
-            return FRW_E_ARG;
-        }
-        k_walk<false, false, true, true><<<g, b, 0, stream>>>(P);
-        FRW_CK(cudaGetLastError());
-        return FRW_OK;
-    }
-    if (P.njobs > 1) {
-        if (rec) uni ? k_walk<true, true, true><<<g, b, 0, stream>>>(P) : k_walk<true, true, false><<<g, b, 0, stream>>>(P);
-        else uni ? k_walk<true, false, true><<<g, b, 0, stream>>>(P) : k_walk<true, false, false><<<g, b, 0, stream>>>(P);
-    } else {
-        if (rec) uni ? k_walk<false, true, true><<<g, b, 0, stream>>>(P) : k_walk<false, true, false><<<g, b, 0, stream>>>(P);
-        else uni ? k_walk<false, false, true><<<g, b, 0, stream>>>(P) : k_walk<false, false, false><<<g, b, 0, stream>>>(P);
-    }
+    if (P.tree_points || P.job0.L.tree_points)
+        launch_variant<true>(P, P.njobs > 1, rec, uni, cv, g, b, stream);
+    else
+        launch_variant<false>(P, P.njobs > 1, rec, uni, cv, g, b, stream);
     FRW_CK(cudaGetLastError());
     return FRW_OK;
 }

@@ -71,6 +71,89 @@ def test_cells_any_resolution_and_overflow(cells_per_rect, max_per_cell):
     assert np.array_equal(sq_c2, sq_t2) and np.array_equal(hit_c2, hit_t2)
 
 
+def test_two_level_build_with_overflowing_coarse_cells():
+    """Large grids build their cells from coarse cells of 4 x 4 cells; a dense
+    cluster of small rects in a sparse layout overflows its coarse cell (over
+    64 rects), whose cells then enumerate the tree.  Queries from the cells
+    equal the tree's on uniform points and on points in and around the
+    cluster."""
+    rng = np.random.default_rng(0x2C0)
+    sparse = frw.generate_layout(0xF4A7 + 9, 70_000, 1e5)
+    # 20 x 20 rects of side 1, two apart, in an empty patch
+    gx, gy = np.meshgrid(np.arange(20) * 3.0, np.arange(20) * 3.0)
+    x0, y0 = 50_000.0 + gx.ravel(), 50_000.0 + gy.ravel()
+    cluster = np.stack([x0, y0, x0 + 1, y0 + 1], 1).astype(np.float32)
+    keep = ~((sparse[:, 2] >= 49_900) & (sparse[:, 0] <= 50_200) & (sparse[:, 3] >= 49_900) & (sparse[:, 1] <= 50_200))
+    rects = np.concatenate([sparse[keep], cluster]).astype(np.float32)
+    with frw.Layout.from_rects(rects) as L:
+        ci = L.cells
+        assert ci.cells >= 1 << 16 and ci.overflow_cells > 0
+        b = L.bounds
+        near = np.stack([50_000 + rng.uniform(-200, 260, 20_000), 50_000 + rng.uniform(-200, 260, 20_000)], 1)
+        pts = np.concatenate([_points(rects.astype(np.float64), b, 40_000, 13, ci.cell_side), near])
+        sq_c, hit_c = L.query(pts)
+        L.set_cells(0)
+        sq_t, hit_t = L.query(pts)
+    assert np.array_equal(sq_c, sq_t) and np.array_equal(hit_c, hit_t)
+    assert np.any(hit_c[-20_000:] >= len(rects) - 400)  # some points hit the cluster
+
+
+def _aligned_array(nx=30, ny=30, pitch=3.0):
+    """nx x ny rects of side 1 on a pitch-3 grid: seen from beside a column
+    (or a row), every rect of it within the L-inf cone ties exactly."""
+    gx, gy = np.meshgrid(np.arange(nx) * pitch, np.arange(ny) * pitch)
+    x0, y0 = 100.0 + gx.ravel(), 100.0 + gy.ravel()
+    return np.stack([x0, y0, x0 + 1, y0 + 1], 1).astype(np.float32)
+
+
+def test_tree_query_with_many_exact_ties_equals_oracle():
+    """Points beside the array see up to ~25 rects at one exact gap, more than
+    the tree's near-tie list holds: those points take the whole-tree replay.
+    Squares and hits equal the oracle's, from the tree and from the cells."""
+    rects = _aligned_array()
+    b = np.array([0.0, 0.0, 300.0, 300.0])
+    rng = np.random.default_rng(0x71E5)
+    far = np.stack([rng.uniform(0, 300, 30_000), rng.uniform(0, 300, 30_000)], 1)
+    side = np.stack([rng.uniform(20, 99, 10_000), rng.uniform(100, 190, 10_000)], 1)  # left of column 0
+    below = np.stack([rng.uniform(100, 190, 10_000), rng.uniform(20, 99, 10_000)], 1)  # under row 0
+    pts = np.concatenate([far, side, below])
+    G = O.Grid(rects.astype(np.float64), b)
+    sq_o, hit_o = G.query_batch(pts)
+    with frw.Layout.from_rects(rects, b) as L:
+        sq_c, hit_c = L.query(pts)
+        L.set_cells(0)
+        sq_t, hit_t = L.query(pts)
+    assert np.array_equal(sq_t, sq_o) and np.array_equal(hit_t, hit_o)
+    assert np.array_equal(sq_c, sq_o) and np.array_equal(hit_c, hit_o)
+
+
+def test_tree_walks_with_many_exact_ties_equal_oracle():
+    """The walk kernel answers tree points with many exact ties by the
+    whole-tree replay (the layout has no cell lists): per-walk records equal
+    the oracle's, and the estimator rows equal those of the cell-list walks
+    (a kernel built without the whole-tree replay, the cells leaving no point
+    to the tree)."""
+    rects = _aligned_array()
+    b = np.array([0.0, 0.0, 300.0, 300.0])
+    target = 15 * 30 + 0  # a rect of column 0
+    o = frw.opts(gauss_mode=frw.GAUSS_OFFSET, gauss_param=4.0, start_mode=frw.START_UNIFORM)
+    G = O.Grid(rects.astype(np.float64), b)
+    n = 4000
+    end_o, hops_o, b1_o, w_o = G.walks(G.walk_cfg(target=target, gauss_mode=o.gauss_mode, gauss_param=o.gauss_param,
+                                                  start_mode=o.start_mode, hop_cap=o.hop_cap, seed=77,
+                                                  stream=o.stream_id), 0, n)
+    with frw.Layout.from_rects(rects, b) as L:
+        rows_c = L.walk(target, 200_000, seed=78, o=o)
+        L.set_cells(0)
+        end, hops, b1, w = L.walk_trace(target, 0, n, seed=77, o=o)
+        rows_t = L.walk(target, 200_000, seed=78, o=o)
+    assert np.array_equal(end, end_o) and np.array_equal(hops, hops_o)
+    assert np.array_equal(b1, b1_o) and np.array_equal(w, w_o)
+    # same walks: equal counts; the weight sums differ only in summation order
+    assert np.array_equal(rows_c.conductor, rows_t.conductor) and np.array_equal(rows_c.hits, rows_t.hits)
+    assert np.allclose(rows_c.sum_w, rows_t.sum_w, rtol=1e-12, atol=1e-300)
+
+
 def test_cells_c2_lists_are_short():
     """10^4 rects: 16 cells per rect, a handful of rects per list, no overflow."""
     rects = frw.generate_layout(0xF4A7 + 2, 10_000, 1e4)
