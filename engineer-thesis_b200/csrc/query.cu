@@ -6,7 +6,9 @@ namespace {
 
 // One point per thread: drawBiggestSquareAtPoint + checkCollisons(point),
 // batched (the reference issues them one walk hop at a time,
-// Cuda/randomwalk.cu:102-103).
+// Cuda/randomwalk.cu:102-103).  kTies: L.tree_points is set, so points with
+// many exact ties can reach the whole-tree replay (compiled out otherwise).
+template <bool kTies>
 __global__ void __launch_bounds__(128) k_query(DevLayout L, const double2 *__restrict__ pts, int64_t n,
                                                double4 *__restrict__ sq, int64_t *__restrict__ hit,
                                                uint32_t *status) {
@@ -16,7 +18,7 @@ __global__ void __launch_bounds__(128) k_query(DevLayout L, const double2 *__res
         const double2 p = pts[i];
         double s[4];
         int h;
-        st = query_point(L, p.x, p.y, s, h);
+        st = query_point<false, false, kTies>(L, p.x, p.y, s, h);
         sq[i] = make_double4(s[0], s[1], s[2], s[3]);
         hit[i] = h == kNoHit ? -1 : (int64_t)h;
     }
@@ -126,8 +128,11 @@ frw_status launch_query(const DevLayout &L, const double *d_pts, int64_t n, doub
                         uint32_t *d_status, cudaStream_t stream) {
     if (n <= 0) return FRW_OK;
     const int T = 128;
-    k_query<<<(unsigned)((n + T - 1) / T), T, 0, stream>>>(L, (const double2 *)d_pts, n, (double4 *)d_sq,
-                                                           d_hit, d_status);
+    const unsigned g = (unsigned)((n + T - 1) / T);
+    if (L.tree_points)
+        k_query<true><<<g, T, 0, stream>>>(L, (const double2 *)d_pts, n, (double4 *)d_sq, d_hit, d_status);
+    else
+        k_query<false><<<g, T, 0, stream>>>(L, (const double2 *)d_pts, n, (double4 *)d_sq, d_hit, d_status);
     FRW_CK(cudaGetLastError());
     return FRW_OK;
 }
