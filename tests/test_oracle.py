@@ -125,3 +125,34 @@ def test_oracle_walks_deterministic():
     assert ((end >= -2) & (end < 3)).all() and (hops >= 0).all() and (end >= 0).mean() > 0.5
     # the weight factor is defined by the first hop; walks without one carry 0
     assert (w[b1 < 0] == 0).all() and (w[end >= 0] != 0).mean() > 0.5
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="compiled reference not present")
+def test_aligned_ties_oracle_pinned_to_reference():
+    """Points beside an aligned array of rects see up to ~30 rects at one
+    exact L-inf gap.  On them the restated reference tree (defect mode)
+    equals the compiled reference, and the brute-force complete predicate
+    equals the restated tree with a complete traversal: the oracle the
+    device's tie handling is checked against is pinned on such points."""
+    gx, gy = np.meshgrid(np.arange(30) * 3.0, np.arange(30) * 3.0)
+    x0, y0 = 100.0 + gx.ravel(), 100.0 + gy.ravel()
+    rects = np.stack([x0, y0, x0 + 1, y0 + 1], 1)
+    bounds = np.array([0.0, 0.0, 300.0, 300.0])
+    rng = np.random.default_rng(0x71E6)
+    pts = np.concatenate([np.stack([rng.uniform(20, 99, 1500), rng.uniform(100, 190, 1500)], 1),
+                          np.stack([rng.uniform(100, 190, 1500), rng.uniform(20, 99, 1500)], 1),
+                          np.stack([rng.uniform(0, 300, 1000), rng.uniform(0, 300, 1000)], 1)])
+    R = O.Ref(rects=rects, bounds=bounds)
+    sq_r, hit_r = R.query_batch(pts)
+    T = O.RefTree(rects, bounds)
+    sq_d = np.array([T.biggest_square(x, y, True) for x, y in pts])
+    hit_d = np.array([T.point_hit(x, y) for x, y in pts])
+    assert np.array_equal(sq_d, sq_r) and np.array_equal(hit_d, hit_r)
+    G = O.Grid(rects, bounds)
+    sq_g, _ = G.query_batch(pts)
+    sq_c = np.array([T.biggest_square(x, y, False) for x, y in pts])
+    assert np.array_equal(sq_g, sq_c)
+    # the points beside the array do tie: many rects at the minimum gap
+    px, py = pts[:1500, :1], pts[:1500, 1:]
+    g = np.maximum(np.maximum(rects[:, 0] - px, px - rects[:, 2]), np.maximum(rects[:, 1] - py, py - rects[:, 3]))
+    assert ((g == g.min(1, keepdims=True)).sum(1) > 8).mean() > 0.3
